@@ -1,0 +1,140 @@
+"""Synthetic input decks for the benchmark workloads.
+
+Each generator writes a complete PIAFS input deck (solver.inp, boundary.inp,
+physics.inp, optional chemistry.inp / weno.inp, binary initial.inp and
+imap.inp) into a directory, in the reference's formats, so that the same
+directory runs unchanged through the reference CPU binary and through this
+package.  All inputs are synthetic and seeded (numpy ``default_rng``):
+seed 0 drives field noise and beam amplitude, seed 1 ensemble parameters,
+seed 2 serving arrivals, seed 3 serving request parameters.
+
+Workloads:
+
+* ``euler1d_density_wave`` -- 1D Euler, gamma 1.4, periodic [0,1) with
+  x_i = i/N, rho = 1 + a sin(2 pi x), u = 1, p = 1; WENO5 (components), Roe,
+  SSPRK3 with a fixed dt.
+* ``ns2d_photochem_beam`` -- 2D Navier-Stokes with the O2/O3 photochemical
+  heating source, periodic in x and slip walls in y, on [0,1]^2 with
+  x_i = (i+1/2)/N; quiescent gas rho = 1 + U(-1e-6, 1e-6), u = v = 0,
+  p = 1/gamma_chem; species O2 = 1, O3 = f_O3/f_O2, others 0; a Gaussian beam
+  map A exp(-((x-1/2)^2+(y-1/2)^2)/r^2).  With chemistry on, the reference
+  derives gamma, Re and Pr from chemistry.inp (NavierStokes2DInitialize.c:196-215);
+  Re ~ 1e4 is realised through the beam half-angle theta (Re is proportional
+  to 1/sin(theta): theta = 4.2117e-5 rad gives Re = 1.0e4).  dt is fixed from
+  CFL 0.4 at t = 0 because the reference takes a fixed dt.
+"""
+from __future__ import annotations
+
+import math
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import deck
+
+# Default chemistry gas properties (ChemistryInitialize.c: defaults), used to
+# compute gamma_chem for the initial pressure and the CFL-based dt.
+_CP_O2, _CV_O2 = 918.45, 650.0
+THETA_RE_1E4 = 4.2117e-5
+
+
+def chem_gamma(f_CO2: float = 0.0) -> float:
+    """Specific-heat ratio of the O2/CO2 mixture (ChemistryInitialize.c:263-266)."""
+    f_O2 = 1.0 - f_CO2
+    cp = f_O2 * _CP_O2 + f_CO2 * 842.86
+    cv = f_O2 * _CV_O2 + f_CO2 * 654.5
+    return cp / cv
+
+
+def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float = 1e-4,
+                         amp: float = 0.2, scheme: str = "weno5", upwinding: str = "roe",
+                         time_scheme_type: str = "ssprk3", file_op_iter: Optional[int] = None,
+                         op_file_format: str = "binary", weno: Optional[Dict] = None,
+                         screen_op_iter: int = 0) -> Dict:
+    os.makedirs(path, exist_ok=True)
+    gamma = 1.4
+    x = np.arange(N, dtype=np.float64) / N
+    rho = 1.0 + amp * np.sin(2.0 * np.pi * x)
+    uvel, p = 1.0, 1.0
+    e = p / (gamma - 1.0) + 0.5 * rho * uvel * uvel
+    u = np.stack([rho, rho * uvel, e], axis=1)
+    deck.write_keyfile(os.path.join(path, "solver.inp"), {
+        "ndims": 1, "nvars": 3, "size": N, "ghost": 3, "n_iter": n_iter,
+        "time_scheme": "rk", "time_scheme_type": time_scheme_type,
+        "hyp_space_scheme": scheme, "hyp_interp_type": "components", "dt": dt,
+        "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
+        "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
+        "model": "euler1d",
+    })
+    deck.write_boundary(os.path.join(path, "boundary.inp"), [
+        deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0]),
+        deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0]),
+    ])
+    deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding})
+    if weno:
+        deck.write_keyfile(os.path.join(path, "weno.inp"), weno)
+    deck.write_array_binary(os.path.join(path, "initial.inp"), [x], u)
+    return {"ndims": 1, "nvars": 3, "size": [N], "n_iter": n_iter, "dt": dt}
+
+
+def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_iter: int = 200,
+                        scheme: str = "crweno5", upwinding: str = "llf-char",
+                        time_scheme_type: str = "ssprk3", seed: int = 0, beam_amp: Optional[float] = None,
+                        beam_radius: float = 0.05, theta: float = THETA_RE_1E4, Re: float = 1e4,
+                        cfl: float = 0.4, dt: Optional[float] = None, file_op_iter: Optional[int] = None,
+                        op_file_format: str = "binary", chemistry: bool = True,
+                        noise: float = 1e-6, weno: Optional[Dict] = None, extra_chem: Optional[Dict] = None,
+                        screen_op_iter: int = 0, write_output: str = "no") -> Dict:
+    os.makedirs(path, exist_ok=True)
+    NX = N
+    NY = NY or N
+    rng = np.random.default_rng(seed)
+    gamma = chem_gamma() if chemistry else 1.4
+    nvars = 11 if chemistry else 4
+    x = (np.arange(NX, dtype=np.float64) + 0.5) / NX
+    y = (np.arange(NY, dtype=np.float64) + 0.5) / NY
+    rho = 1.0 + rng.uniform(-noise, noise, size=(NY, NX))
+    p = 1.0 / gamma
+    u = np.zeros((NY, NX, nvars))
+    u[..., 0] = rho
+    u[..., 3] = p / (gamma - 1.0)
+    if chemistry:
+        u[..., 4] = 1.0            # O2 (normalised by n_O2)
+        u[..., 5] = 0.005 / 1.0    # O3 = f_O3 / f_O2
+    A = float(rng.uniform(0.5, 1.5)) if beam_amp is None else float(beam_amp)
+    X, Y = np.meshgrid(x, y)
+    imap = A * np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / beam_radius ** 2)
+    c0 = math.sqrt(gamma * p / (1.0 + noise))
+    if dt is None:
+        dt = cfl * (1.0 / max(NX, NY)) / c0
+    deck.write_keyfile(os.path.join(path, "solver.inp"), {
+        "ndims": 2, "nvars": nvars, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
+        "time_scheme": "rk", "time_scheme_type": time_scheme_type,
+        "hyp_space_scheme": scheme, "hyp_interp_type": "components",
+        "par_space_scheme": "2", "dt": dt,
+        "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
+        "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
+        "model": "navierstokes2d",
+    })
+    big = 1e99
+    deck.write_boundary(os.path.join(path, "boundary.inp"), [
+        deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0, -big, big]),
+        deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0, -big, big]),
+        deck.BoundaryZone("slip-wall", 1, 1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
+        deck.BoundaryZone("slip-wall", 1, -1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
+    ])
+    phys = {"gamma": 1.4, "upwinding": upwinding, "Pr": 0.72, "Re": Re,
+            "include_chemistry": "yes" if chemistry else "no", "write_output": write_output}
+    deck.write_keyfile(os.path.join(path, "physics.inp"), phys)
+    if chemistry:
+        chem = {"theta": theta}
+        if extra_chem:
+            chem.update(extra_chem)
+        deck.write_keyfile(os.path.join(path, "chemistry.inp"), chem)
+        deck.write_array_binary(os.path.join(path, "imap.inp"), [x, y], imap.reshape(-1, 1))
+    if weno:
+        deck.write_keyfile(os.path.join(path, "weno.inp"), weno)
+    deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, nvars))
+    return {"ndims": 2, "nvars": nvars, "size": [NX, NY], "n_iter": n_iter, "dt": dt,
+            "beam_amp": A, "gamma": gamma}
