@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the PIAFS per-stage RHS + explicit RK path on B200.
+
+Metric: grid-point RK-stage updates per second (one unit = one interior grid
+point advanced through one Runge-Kutta stage).  Default workload: the 2D
+Navier-Stokes photochemical case on a 2048 x 2048 grid (11 conserved
+variables, CRWENO5 components, LLF upwinding, SSPRK3, FP64), synthetic seeded
+inputs of that shape.  A "step" is one SSPRK3 time step over the whole grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own
+independent replica of the workload (a single grid does not shard without a
+halo exchange; replicas are the weakly scaled unit) and the timed region is
+bracketed by barriers with the max over ranks taken on the device clocks.
+
+--impl reference times the reference's own CPU implementation (the
+llnl/piafs binary built from source by oracle/Makefile, OpenMP on all host
+threads) on a bounded sample of the same workload; under torchrun only rank 0
+runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_UNIT = {11: 264, 4: 96, 3: 72}   # 3 * nvars * 8: read U_s, read u_n, write (FP64 state)
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+CPU_SAMPLE_N = 512                          # sample grid of the CPU arms
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="ns2d_photochem", choices=["ns2d_photochem", "euler1d"])
+    ap.add_argument("--n", type=int, default=None, help="grid size (default 2048 / 1024)")
+    ap.add_argument("--scheme", default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+def make_deck(path, a, n_iter, n=None):
+    from piafs_b200 import cases
+    if a.workload == "euler1d":
+        N = n or a.n or 1024
+        return cases.euler1d_density_wave(path, N=N, n_iter=n_iter, dt=1e-4, scheme=a.scheme or "weno5",
+                                          op_file_format="none")
+    N = n or a.n or 2048
+    return cases.ns2d_photochem_beam(path, N=N, n_iter=n_iter, scheme=a.scheme or "crweno5",
+                                     op_file_format="none", dt=0.4 / 2048)
+
+
+def workload_config(a, meta, n_gpus):
+    sz = meta["size"]
+    name = ("ns2d_photochem_crweno5_llf_ssprk3" if a.workload == "ns2d_photochem" else "euler1d_weno5_roe_ssprk3")
+    if a.scheme:
+        name = name.replace("crweno5", a.scheme).replace("weno5", a.scheme)
+    return {"workload": f"{name}_{'x'.join(map(str, sz))}", "grid": sz, "nvars": meta["nvars"],
+            "time_scheme": "ssprk3", "dt": meta["dt"], "replicas": n_gpus, "parallelism": f"replicas{n_gpus}",
+            "step": "one SSPRK3 time step (3 RK stages) over the whole grid",
+            "l2": "state arrays (%.0f MB each) exceed the 126 MB L2; no flush" % (
+                8 * meta["nvars"] * (sz[0] + 6) * ((sz[1] + 6) if len(sz) > 1 else 1) / 1e6)}
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ CPU baselines
+def ref_binary():
+    for b in ("PIAFS_omp", "PIAFS"):
+        p = os.path.join(REF_DIR, b)
+        if os.access(p, os.X_OK):
+            return p, b == "PIAFS_omp"
+    return None, False
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def sample_size(nsteps, warm):
+    """Grid side of the CPU sample: the whole reference run should take about
+    two minutes at ~0.2 M updates/s (the reference's rate on this workload)."""
+    budget = 120.0 / max(nsteps + warm, 1)
+    n = int((budget * 0.2e6 / 3) ** 0.5) // 32 * 32
+    return max(128, min(CPU_SAMPLE_N, n))
+
+
+def run_reference_steps(a, nsteps, warm):
+    """Run the reference binary on the CPU sample deck; returns (per-step
+    seconds of the timed steps, cores, kind, sample description)."""
+    binary, omp = ref_binary()
+    cores = host_threads() if omp else 1
+    with tempfile.TemporaryDirectory() as d:
+        n = sample_size(nsteps, warm) if a.workload == "ns2d_photochem" else (a.n or 1024)
+        meta = make_deck(d, a, warm + nsteps, n=n)
+        # per-step wall time lines: "iter= ... wctime: X (s)" (TimePrintStep.c)
+        from piafs_b200 import deck
+        kv = deck.read_keyfile(os.path.join(d, "solver.inp"))
+        txt = open(os.path.join(d, "solver.inp")).read()
+        txt = re.sub(r"screen_op_iter\s+\d+", "screen_op_iter 1", txt)
+        open(os.path.join(d, "solver.inp"), "w").write(txt)
+        if binary:
+            env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+            out = subprocess.run([binary], cwd=d, env=env, capture_output=True, text=True, check=True).stdout
+            w = [float(x) for x in re.findall(r"wctime:\s*([0-9.Ee+-]+)", out)]
+            kind = "reference"
+        else:
+            # the reference binary was not built here: time the oracle port
+            from oracle import oracle
+            case = oracle.load(d)
+            w = []
+            u = case.u0.copy()
+            for k in range(warm + nsteps):
+                t0 = time.perf_counter()
+                u = case.run(nsteps=1, u=u, t0=k * case.dt)
+                w.append(time.perf_counter() - t0)
+            kind, cores = "port", 1
+        units = 3 * meta["size"][0] * (meta["size"][1] if len(meta["size"]) > 1 else 1)
+        sample = (f"{'x'.join(map(str, meta['size']))} grid of the same workload, {nsteps} timed SSPRK3 steps "
+                  f"after {warm} warm-up, per-step wall time printed by the reference")
+        return w[warm:warm + nsteps], units, cores, kind, sample
+
+
+def cpu_baseline(a):
+    steps = 3 if a.workload == "ns2d_photochem" else 200
+    w, units, cores, kind, sample = run_reference_steps(a, steps, 1)
+    v = units * len(w) / sum(w)
+    return {"value": v, "unit": "pt-stage updates/s", "cores": cores, "kind": kind, "sample": sample}
+
+
+# --------------------------------------------------------------------- main
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    n_gpus = max(world, 1)
+    metric = "pt-stage updates/s"
+
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        w, units, cores, kind, sample = run_reference_steps(a, a.steps, a.warmup)
+        total = sum(w)
+        v = units * len(w) / total
+        meta_n = sample_size(a.steps, a.warmup) if a.workload == "ns2d_photochem" else (a.n or 1024)
+        line = {"impl": "reference", "metric": metric, "value": v, "unit": metric, "n_gpus": a.gpus,
+                "steps": len(w), "warmup": a.warmup, "ms_per_step": 1e3 * total / max(len(w), 1),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded decks of the workload's shape)",
+                "config": {"workload": ("ns2d_photochem_crweno5_llf_ssprk3" if a.workload == "ns2d_photochem"
+                                        else "euler1d_weno5_roe_ssprk3") + f"_sample_{meta_n}",
+                           "sample_of": "2048x2048" if a.workload == "ns2d_photochem" else str(meta_n)},
+                "cpu_baseline": {"value": v, "unit": metric, "cores": cores, "kind": kind, "sample": sample},
+                "e2e": {"value": v, "unit": metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import numpy as np
+    import torch
+    import piafs_b200
+    from piafs_b200 import Simulation
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world <= 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    tmp = tempfile.mkdtemp(prefix=f"piafs_bench_r{rank}_")
+    try:
+        meta = make_deck(tmp, a, a.warmup + a.steps)
+        sim = Simulation(tmp)
+        info = sim.info
+        npts = info["dim"][0] * info["dim"][1]
+        units_per_step = info["nstages"] * npts
+        stream = torch.cuda.ExternalStream(sim.stream)
+
+        # warm-up (also instantiates the CUDA graph of a step)
+        sim.time_rk(a.warmup)
+        with ClockSampler(local) as clk:
+            time.sleep(0.3)
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.time_rk_async(a.steps)
+            e1.record(stream)
+            sim.synchronize()
+            torch.cuda.synchronize()
+            barrier()
+            ms = e0.elapsed_time(e1)
+        ms_max = max_over_ranks(ms)
+        assert sim.info["singular"] == 0, "zero pivot during the benchmark"
+        sol_ok = bool(np.isfinite(sim.solution()).all())
+        value = units_per_step * a.steps * n_gpus / (ms_max / 1e3)
+
+        # dominant kernel: per-phase device time of one RHS evaluation
+        phases = sim.profile_rhs(reps=3)
+        dom = max(phases, key=phases.get)
+        nv = info["nvars"]
+        bpu = BYTES_PER_UNIT.get(nv, 3 * nv * 8)
+        peaks = {}
+        pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(pk):
+            peaks = json.load(open(pk))
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = bpu * npts / (phases[dom] / 1e3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+        if os.path.exists(tf):
+            tj = json.load(open(tf))
+            ent = tj.get(dom)
+            if ent and ent.get("grid") == info["dim"][:info["ndims"]]:
+                traffic = ent["bytes"]
+        step_ms = ms_max / a.steps
+        path_gbs = bpu * units_per_step / (step_ms / 1e3) / 1e9 / 1.0
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                    "units_per_launch": npts, "bytes_per_unit": bpu,
+                    "phase_ms": {k: round(v, 4) for k, v in phases.items()},
+                    "path_gbs": path_gbs, "path_frac": path_gbs / peak}
+
+        # end to end through the C ABI with host buffers: H2D of the state,
+        # one step, D2H of the state, every step
+        ne = max(1, min(a.e2e_steps, a.steps))
+        shape = sim.shape_ghosted
+        pinned = torch.empty(shape[0] * shape[1], dtype=torch.float64, pin_memory=True)
+        uh = pinned.numpy()
+        uh[:] = sim.state()
+        t = sim.info["t"]
+        barrier()
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        for _ in range(ne):
+            sim.time_rk_host(uh, t)
+            t += info["dt"]
+        h1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(h0.elapsed_time(h1))
+        e2e = {"value": units_per_step * ne * n_gpus / (e2e_ms / 1e3), "unit": metric,
+               "h2d_bytes_per_step": int(uh.nbytes), "d2h_bytes_per_step": int(uh.nbytes),
+               "steps": ne, "ms_per_step": e2e_ms / ne,
+               "api": "piafs_gpu_TimeRK_host (pinned host state in, one step, state out)"}
+        launches = info["launches_per_step"] * a.steps
+        sim.close()
+
+        base = None
+        if rank == 0 and world == 1 and not a.no_cpu_baseline:
+            try:
+                base = cpu_baseline(a)
+            except Exception as ex:  # reported, not fatal
+                base = {"value": None, "error": str(ex)[:200]}
+        if rank == 0:
+            line = {"metric": metric, "value": value, "unit": metric, "n_gpus": n_gpus, "steps": a.steps,
+                    "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded decks of the workload's shape)",
+                    "config": workload_config(a, meta, n_gpus), "roofline": roofline, "cpu_baseline": base,
+                    "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(), "finite": sol_ok,
+                    "precision": "fp64"}
+            print(json.dumps(line))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

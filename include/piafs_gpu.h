@@ -1,0 +1,157 @@
+/* piafs_gpu.h -- C ABI of the B200 (sm_100a) implementation of PIAFS's
+ * per-stage right-hand side and explicit Runge-Kutta time step.
+ *
+ * The library replaces the hot path behind the reference's function-pointer
+ * interface on HyPar (include/hypar.h:204-290 in llnl/piafs): TimeIntegrate,
+ * HyperbolicFunction, InterpolateInterfacesHyp, Upwind, FFunction,
+ * ParabolicFunction, FirstDerivativePar, SourceFunction and
+ * ApplyBoundaryConditions.  It reads the reference's input deck (solver.inp,
+ * boundary.inp, physics.inp, chemistry.inp, weno.inp, initial.inp, imap.inp)
+ * and writes the reference's binary output files, so a deck runs unchanged on
+ * either implementation.
+ *
+ * Conventions
+ *   - Every function returns PIAFS_OK (0) or a PIAFS_ERR_* code; the message
+ *     of the last failure on the calling thread is piafs_gpu_last_error().
+ *     No function aborts the process.
+ *   - Host arrays use the reference layout: array of structures, variable
+ *     index fastest, then dim0, then dim1, ghost points included
+ *     (include/arrayfunctions.h:43-50).  Interface arrays have no ghosts and
+ *     dim_d + 1 entries along the reconstruction direction
+ *     (src/Simulation/Initialize.c:165-174).
+ *   - "Device" arguments are CUDA device pointers in that same layout.
+ *   - A simulation object is used by one host thread at a time; every call is
+ *     complete (synchronised) when it returns.
+ */
+#ifndef PIAFS_GPU_H
+#define PIAFS_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PIAFS_OK = 0,
+  PIAFS_ERR_ARGUMENT = 1,     /* bad argument or call sequence            */
+  PIAFS_ERR_INPUT = 2,        /* missing or malformed input deck          */
+  PIAFS_ERR_UNSUPPORTED = 3,  /* option outside the GPU path              */
+  PIAFS_ERR_CUDA = 4,         /* CUDA runtime failure                     */
+  PIAFS_ERR_SINGULAR = 5,     /* zero pivot in a tridiagonal solve        */
+  PIAFS_ERR_IO = 6,           /* output file could not be written         */
+  PIAFS_ERR_MEMORY = 7        /* device allocation failed                 */
+};
+
+enum { PIAFS_PRECISION_FP64 = 0, PIAFS_PRECISION_MIXED = 1 };
+
+typedef struct piafs_gpu_sim piafs_gpu_sim;
+
+typedef struct {
+  int ndims, nvars, ghosts;
+  int dim[2];                 /* interior points per dimension (dim[1] = 1 in 1D) */
+  int n_iter, restart_iter, screen_op_iter, file_op_iter;
+  int iter;                   /* completed time steps                     */
+  int nstages;
+  double dt, t;               /* time step, current simulation time        */
+  double gamma, Re, Pr;       /* values in effect (chemistry may override) */
+  long long npoints_ghosted;  /* points of a ghosted array                 */
+  long long ninterfaces[2];   /* points of an interface array per dir      */
+  double cfl, norm;           /* last diagnostics (TimePreStep/PostStep)   */
+  int singular;               /* zero pivots seen since creation           */
+  int launches_per_step;      /* kernels one time step launches            */
+} piafs_gpu_info;
+
+/* Message of the last failure on this thread ("" if none). */
+const char* piafs_gpu_last_error(void);
+
+/* Set up a simulation from the input deck in `deck_dir` and upload it to the
+ * current CUDA device.  Replaces the reference's ReadInputs, Initialize,
+ * InitialSolution, InitializeBoundaries, InitializeSolvers and
+ * InitializePhysics (src/main.cpp:126-212).  `precision` is one of
+ * PIAFS_PRECISION_*. */
+int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** sim);
+void piafs_gpu_destroy(piafs_gpu_sim* sim);
+int piafs_gpu_get_info(piafs_gpu_sim* sim, piafs_gpu_info* info);
+
+/* State transfer with host arrays in the reference layout (ghosts included).
+ * set_state also sets the simulation time. */
+int piafs_gpu_set_state(piafs_gpu_sim* sim, const double* u_host, double t);
+int piafs_gpu_get_state(piafs_gpu_sim* sim, double* u_host);
+/* Interior points only, in output-file order (npoints x nvars). */
+int piafs_gpu_get_solution(piafs_gpu_sim* sim, double* u_interior_host);
+
+/* Advance the device-resident state by `nsteps` time steps: per step the
+ * boundary conditions on u (TimePreStep.c:36-41), the explicit RK stages
+ * (TimeRK.c:34-102) and t += dt (TimePostStep.c:31).  Replaces
+ * TS->TimeIntegrate = TimeRK (src/TimeIntegration/TimeRK.c:34). */
+int piafs_gpu_TimeRK(piafs_gpu_sim* sim, int nsteps);
+
+/* One time step on a host array, the drop-in form of TimeIntegrate when the
+ * caller owns solver->u: copies u_host (ghosted, reference layout) to the
+ * device, advances one step from time t and copies the result back. */
+int piafs_gpu_TimeRK_host(piafs_gpu_sim* sim, double* u_host, double t);
+
+/* The reference's Solve() loop (src/Simulation/Solve.cpp:29-123): n_iter
+ * steps from the initial solution with op_NNNNN.bin written to `output_dir`
+ * at iteration 0, every file_op_iter steps and at the end (binary output
+ * format only). */
+int piafs_gpu_Solve(piafs_gpu_sim* sim, const char* output_dir);
+
+/* Asynchronous form of piafs_gpu_TimeRK: enqueues nsteps steps on the
+ * simulation's CUDA stream and returns without waiting (diagnostics and the
+ * singular-pivot count are updated at the next synchronising call). */
+int piafs_gpu_TimeRK_async(piafs_gpu_sim* sim, int nsteps);
+/* The simulation's CUDA stream (a cudaStream_t), for callers that order
+ * their own work or timing events after it. */
+int piafs_gpu_get_stream(piafs_gpu_sim* sim, void** stream);
+int piafs_gpu_synchronize(piafs_gpu_sim* sim);
+
+/* Time each kernel phase of one right-hand-side evaluation on the current
+ * state with CUDA events on the simulation's stream, averaged over `reps`
+ * evaluations.  ms[k] receives the mean duration of phase k; phases are, per
+ * direction d = 0..ndims-1, [3d] flux, [3d+1] interface reconstruction
+ * (WENO5 or the CRWENO5 line solve), [3d+2] upwinding + divergence, then
+ * [3 ndims] viscous + source.  nphases (in/out) is the capacity / count. */
+int piafs_gpu_profile_rhs(piafs_gpu_sim* sim, int reps, double* ms, int* nphases);
+
+/* max CFL of the current state (NavierStokes2DComputeCFL.c /
+ * Euler1DComputeCFL.c). */
+int piafs_gpu_ComputeCFL(piafs_gpu_sim* sim, double* cfl);
+
+/* ---- operator-level entry points (device pointers, reference layout) ----
+ * These mirror the HyPar function pointers one to one and exist so that each
+ * operator can be checked on its own.  Time-dependent operators take t. */
+
+/* TS->RHSFunction = TimeRHSFunctionExplicit (TimeRHSFunctionExplicit.c:29);
+ * fills the ghosts of u (boundary conditions) like the reference does. */
+int piafs_gpu_RHSFunction(piafs_gpu_sim* sim, double* rhs, double* u, double t);
+/* solver->HyperbolicFunction (HyperbolicFunction.c:34) */
+int piafs_gpu_HyperbolicFunction(piafs_gpu_sim* sim, double* hyp, const double* u, double t);
+/* solver->ParabolicFunction = NavierStokes2DParabolicFunction (:41) */
+int piafs_gpu_ParabolicFunction(piafs_gpu_sim* sim, double* par, const double* u, double t);
+/* solver->SourceFunction (SourceFunction.c:21) */
+int piafs_gpu_SourceFunction(piafs_gpu_sim* sim, double* source, const double* u, double t);
+/* solver->ApplyBoundaryConditions (ApplyBoundaryConditions.c:31) */
+int piafs_gpu_ApplyBoundaryConditions(piafs_gpu_sim* sim, double* u, double t);
+/* solver->FFunction (NavierStokes2DFlux.c:24 / Euler1DFlux.c:19) */
+int piafs_gpu_FFunction(piafs_gpu_sim* sim, double* f, const double* u, int dir, double t);
+/* solver->SetInterpLimiterVar + solver->InterpolateInterfacesHyp
+ * (WENOFifthOrderCalculateWeights.c:41 + Interp1PrimFifthOrderWENO.c:77 /
+ * Interp1PrimFifthOrderCRWENO.c:81): the interface values of fC (uflag = 0)
+ * or of u (uflag = 1), left-biased for upw > 0, right-biased for upw < 0. */
+int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* sim, double* fI, const double* fC, const double* u,
+                                       int upw, int dir, int uflag);
+/* solver->Upwind (NavierStokes2DUpwind.c / Euler1DUpwind.c) */
+int piafs_gpu_Upwind(piafs_gpu_sim* sim, double* fI, const double* fL, const double* fR, const double* uL,
+                     const double* uR, const double* u, int dir, double t);
+/* solver->FirstDerivativePar = FirstDerivativeFirstOrder
+ * (FirstDerivativeFirstOrder.c:40) on an array with `nv` values per point */
+int piafs_gpu_FirstDerivativePar(piafs_gpu_sim* sim, double* Df, const double* f, int dir, int bias, int nv);
+/* tridiagLU (tridiagLU.c:86), serial semantics: ns independent systems of n
+ * rows, layout [row * ns + system], solved in place into x.  Returns
+ * PIAFS_ERR_SINGULAR on a zero pivot like the reference's -1. */
+int piafs_gpu_tridiagLU(double* a, double* b, double* c, double* x, int n, int ns);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PIAFS_GPU_H */

@@ -203,7 +203,9 @@ class Case:
         # physics.inp
         ph = _keyfile(os.path.join(path, "physics.inp")) or {}
         gamma = float(ph.get("gamma", 1.4))
-        P.bc_gamma = gamma      # wall BCs keep the physics.inp gamma
+        # wall BCs keep the physics.inp gamma (set before chemistry overrides
+        # it, NavierStokes2DInitialize.c:172-174); Euler1D never sets it (0)
+        P.bc_gamma = gamma if self.model == "navierstokes2d" else 0.0
         upw = ph.get("upwinding", "roe")
         P.upwind = {"roe": 0, "rf-char": 1, "llf-char": 2, "rusanov": 3}[upw]
         include_chem = ph.get("include_chemistry", "no") == "yes"

@@ -1,0 +1,278 @@
+"""piafs_b200 -- B200 (sm_100a) implementation of PIAFS's per-stage
+right-hand side and explicit Runge-Kutta time step.
+
+The compute path is the native library ``libpiafs_gpu.so`` (hand-written CUDA
+kernels behind the C ABI of ``include/piafs_gpu.h``); this module is a thin
+ctypes host binding.  It mirrors the reference's simulation flow
+(ReadInputs/Initialize -> Solve, src/main.cpp:68-247) and the HyPar operator
+function pointers (include/hypar.h:204-290):
+
+    sim = Simulation("path/to/deck")     # the reference's input deck
+    sim.solve("path/to/deck")            # op_NNNNN.bin like the CPU code
+    sim.time_rk(10)                      # TimeIntegrate, device-resident
+    u = sim.solution()                   # (npoints, nvars), output order
+
+Operator-level calls take CUDA device pointers (or torch CUDA tensors) in the
+reference's array-of-structures layout.  There is no CPU fallback: if the
+library or a CUDA device is missing, these calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import cases, deck  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpiafs_gpu.so")
+CLI_PATH = os.path.join(HERE, "bin", "piafs-gpu")
+
+PIAFS_OK = 0
+ERRORS = {1: "argument", 2: "input", 3: "unsupported", 4: "cuda", 5: "singular", 6: "io", 7: "memory"}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+# Every entry point of include/piafs_gpu.h with its ctypes signature.
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+SIGNATURES = {
+    "piafs_gpu_last_error": (C.c_char_p, []),
+    "piafs_gpu_create": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(_vp)]),
+    "piafs_gpu_destroy": (None, [_vp]),
+    "piafs_gpu_get_info": (C.c_int, [_vp, _vp]),
+    "piafs_gpu_set_state": (C.c_int, [_vp, _dp, C.c_double]),
+    "piafs_gpu_get_state": (C.c_int, [_vp, _dp]),
+    "piafs_gpu_get_solution": (C.c_int, [_vp, _dp]),
+    "piafs_gpu_TimeRK": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_TimeRK_host": (C.c_int, [_vp, _dp, C.c_double]),
+    "piafs_gpu_Solve": (C.c_int, [_vp, C.c_char_p]),
+    "piafs_gpu_ComputeCFL": (C.c_int, [_vp, _dp]),
+    "piafs_gpu_TimeRK_async": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "piafs_gpu_synchronize": (C.c_int, [_vp]),
+    "piafs_gpu_profile_rhs": (C.c_int, [_vp, C.c_int, _dp, C.POINTER(C.c_int)]),
+    "piafs_gpu_RHSFunction": (C.c_int, [_vp, _vp, _vp, C.c_double]),
+    "piafs_gpu_HyperbolicFunction": (C.c_int, [_vp, _vp, _vp, C.c_double]),
+    "piafs_gpu_ParabolicFunction": (C.c_int, [_vp, _vp, _vp, C.c_double]),
+    "piafs_gpu_SourceFunction": (C.c_int, [_vp, _vp, _vp, C.c_double]),
+    "piafs_gpu_ApplyBoundaryConditions": (C.c_int, [_vp, _vp, C.c_double]),
+    "piafs_gpu_FFunction": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_double]),
+    "piafs_gpu_InterpolateInterfacesHyp": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_int]),
+    "piafs_gpu_Upwind": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double]),
+    "piafs_gpu_FirstDerivativePar": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int]),
+    "piafs_gpu_tridiagLU": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
+}
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("ndims", C.c_int), ("nvars", C.c_int), ("ghosts", C.c_int), ("dim", C.c_int * 2),
+        ("n_iter", C.c_int), ("restart_iter", C.c_int), ("screen_op_iter", C.c_int),
+        ("file_op_iter", C.c_int), ("iter", C.c_int), ("nstages", C.c_int),
+        ("dt", C.c_double), ("t", C.c_double), ("gamma", C.c_double), ("Re", C.c_double),
+        ("Pr", C.c_double), ("npoints_ghosted", C.c_longlong), ("ninterfaces", C.c_longlong * 2),
+        ("cfl", C.c_double), ("norm", C.c_double), ("singular", C.c_int),
+        ("launches_per_step", C.c_int),
+    ]
+
+    def asdict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class PiafsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"piafs_gpu error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libpiafs_gpu.so (building it first if this is a source tree with
+    nvcc but no library).  Raises if it cannot be had: there is no fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    L = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(code: int):
+    if code != PIAFS_OK:
+        raise PiafsError(code, _lib.piafs_gpu_last_error().decode())
+
+
+def _ptr(x) -> int:
+    """Device pointer of a torch CUDA tensor, or an int pointer as is."""
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if not x.is_cuda or x.dtype.__str__() != "torch.float64" or not x.is_contiguous():
+            raise ValueError("expected a contiguous float64 CUDA tensor")
+        return x.data_ptr()
+    raise TypeError(f"cannot take a device pointer of {type(x)}")
+
+
+def _hp(a: np.ndarray):
+    if a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("expected a C-contiguous float64 array")
+    return a.ctypes.data_as(_dp)
+
+
+class Simulation:
+    """One PIAFS simulation resident on the current CUDA device."""
+
+    def __init__(self, deck_dir: str, precision: str = "fp64"):
+        L = load_library()
+        h = _vp()
+        _check(L.piafs_gpu_create(os.fsencode(deck_dir), PRECISION[precision], C.byref(h)))
+        self._h = h
+        self.deck_dir = deck_dir
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.piafs_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---------------------------------------------------------------- info
+    @property
+    def info(self) -> dict:
+        inf = Info()
+        _check(_lib.piafs_gpu_get_info(self._h, C.byref(inf)))
+        return inf.asdict()
+
+    @property
+    def shape_ghosted(self):
+        i = self.info
+        return (i["npoints_ghosted"], i["nvars"])
+
+    @property
+    def shape_interior(self):
+        i = self.info
+        return (i["dim"][0] * i["dim"][1], i["nvars"])
+
+    # --------------------------------------------------------------- state
+    def set_state(self, u: np.ndarray, t: float = 0.0):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.size != int(np.prod(self.shape_ghosted)):
+            raise ValueError("state must be a ghosted array in the reference layout")
+        _check(_lib.piafs_gpu_set_state(self._h, _hp(u), float(t)))
+
+    def state(self) -> np.ndarray:
+        u = np.empty(self.shape_ghosted)
+        _check(_lib.piafs_gpu_get_state(self._h, _hp(u)))
+        return u.reshape(-1)
+
+    def solution(self) -> np.ndarray:
+        u = np.empty(self.shape_interior)
+        _check(_lib.piafs_gpu_get_solution(self._h, _hp(u)))
+        return u
+
+    # ------------------------------------------------------------ stepping
+    def time_rk(self, nsteps: int = 1):
+        """TimeIntegrate on the device-resident state (TimeRK.c:34)."""
+        _check(_lib.piafs_gpu_TimeRK(self._h, int(nsteps)))
+
+    def time_rk_host(self, u: np.ndarray, t: float) -> np.ndarray:
+        """One step on a host array in the reference layout, in place."""
+        _check(_lib.piafs_gpu_TimeRK_host(self._h, _hp(u), float(t)))
+        return u
+
+    def time_rk_async(self, nsteps: int = 1):
+        """Enqueue nsteps steps on the simulation's stream without waiting."""
+        _check(_lib.piafs_gpu_TimeRK_async(self._h, int(nsteps)))
+
+    def synchronize(self):
+        _check(_lib.piafs_gpu_synchronize(self._h))
+
+    @property
+    def stream(self) -> int:
+        """The simulation's cudaStream_t as an integer handle."""
+        p = _vp()
+        _check(_lib.piafs_gpu_get_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def profile_rhs(self, reps: int = 3):
+        """Per-phase device time (ms) of one RHS evaluation (see piafs_gpu.h)."""
+        ms = (C.c_double * 16)()
+        n = C.c_int(16)
+        _check(_lib.piafs_gpu_profile_rhs(self._h, int(reps), ms, C.byref(n)))
+        names = []
+        for d in range(self.info["ndims"]):
+            names += [f"flux_{'xy'[d]}", f"reconstruct_{'xy'[d]}", f"upwind_div_{'xy'[d]}"]
+        names.append("viscous_source")
+        return dict(zip(names, list(ms)[: n.value]))
+
+    def solve(self, output_dir: Optional[str] = None):
+        """The reference's Solve() loop with op_NNNNN.bin output."""
+        _check(_lib.piafs_gpu_Solve(self._h, os.fsencode(output_dir or self.deck_dir)))
+
+    def cfl(self) -> float:
+        c = C.c_double()
+        _check(_lib.piafs_gpu_ComputeCFL(self._h, C.byref(c)))
+        return c.value
+
+    # ------------------------------------------------ operator-level calls
+    def RHSFunction(self, rhs, u, t=0.0):
+        _check(_lib.piafs_gpu_RHSFunction(self._h, _ptr(rhs), _ptr(u), float(t)))
+
+    def HyperbolicFunction(self, hyp, u, t=0.0):
+        _check(_lib.piafs_gpu_HyperbolicFunction(self._h, _ptr(hyp), _ptr(u), float(t)))
+
+    def ParabolicFunction(self, par, u, t=0.0):
+        _check(_lib.piafs_gpu_ParabolicFunction(self._h, _ptr(par), _ptr(u), float(t)))
+
+    def SourceFunction(self, src, u, t=0.0):
+        _check(_lib.piafs_gpu_SourceFunction(self._h, _ptr(src), _ptr(u), float(t)))
+
+    def ApplyBoundaryConditions(self, u, t=0.0):
+        _check(_lib.piafs_gpu_ApplyBoundaryConditions(self._h, _ptr(u), float(t)))
+
+    def FFunction(self, f, u, dir, t=0.0):
+        _check(_lib.piafs_gpu_FFunction(self._h, _ptr(f), _ptr(u), int(dir), float(t)))
+
+    def InterpolateInterfacesHyp(self, fI, fC, u, upw, dir, uflag):
+        _check(_lib.piafs_gpu_InterpolateInterfacesHyp(self._h, _ptr(fI), _ptr(fC), _ptr(u), int(upw), int(dir),
+                                                       int(uflag)))
+
+    def Upwind(self, fI, fL, fR, uL, uR, u, dir, t=0.0):
+        _check(_lib.piafs_gpu_Upwind(self._h, _ptr(fI), _ptr(fL), _ptr(fR), _ptr(uL), _ptr(uR), _ptr(u), int(dir),
+                                     float(t)))
+
+    def FirstDerivativePar(self, Df, f, dir, bias, nv):
+        _check(_lib.piafs_gpu_FirstDerivativePar(self._h, _ptr(Df), _ptr(f), int(dir), int(bias), int(nv)))
+
+
+def tridiagLU(a, b, c, x, n: int, ns: int):
+    """Batched tridiagonal solve, reference layout [row * ns + system]."""
+    L = load_library()
+    code = L.piafs_gpu_tridiagLU(_ptr(a), _ptr(b), _ptr(c), _ptr(x), int(n), int(ns))
+    if code != PIAFS_OK:
+        raise PiafsError(code, L.piafs_gpu_last_error().decode())

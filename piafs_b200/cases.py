@@ -85,13 +85,16 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
                         cfl: float = 0.4, dt: Optional[float] = None, file_op_iter: Optional[int] = None,
                         op_file_format: str = "binary", chemistry: bool = True,
                         noise: float = 1e-6, weno: Optional[Dict] = None, extra_chem: Optional[Dict] = None,
-                        screen_op_iter: int = 0, write_output: str = "no") -> Dict:
+                        screen_op_iter: int = 0, write_output: str = "no", layers: int = 1) -> Dict:
+    """``layers`` is the number of simulated z-layers, z_i + 1 with
+    z_i = ceil(z_mm 1e-3 nz / Lz) from chemistry.inp (ChemistryInitialize.c:353);
+    each layer carries its own 7 species."""
     os.makedirs(path, exist_ok=True)
     NX = N
     NY = NY or N
     rng = np.random.default_rng(seed)
     gamma = chem_gamma() if chemistry else 1.4
-    nvars = 11 if chemistry else 4
+    nvars = 4 + 7 * layers if chemistry else 4
     x = (np.arange(NX, dtype=np.float64) + 0.5) / NX
     y = (np.arange(NY, dtype=np.float64) + 0.5) / NY
     rho = 1.0 + rng.uniform(-noise, noise, size=(NY, NX))
@@ -100,8 +103,9 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
     u[..., 0] = rho
     u[..., 3] = p / (gamma - 1.0)
     if chemistry:
-        u[..., 4] = 1.0            # O2 (normalised by n_O2)
-        u[..., 5] = 0.005 / 1.0    # O3 = f_O3 / f_O2
+        for iz in range(layers):
+            u[..., 4 + 7 * iz] = 1.0            # O2 (normalised by n_O2)
+            u[..., 5 + 7 * iz] = 0.005 / 1.0    # O3 = f_O3 / f_O2
     A = float(rng.uniform(0.5, 1.5)) if beam_amp is None else float(beam_amp)
     X, Y = np.meshgrid(x, y)
     imap = A * np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / beam_radius ** 2)
@@ -138,3 +142,49 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
     deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, nvars))
     return {"ndims": 2, "nvars": nvars, "size": [NX, NY], "n_iter": n_iter, "dt": dt,
             "beam_amp": A, "gamma": gamma}
+
+
+def ns2d_shear_layer(path: str, N: int = 64, NY: Optional[int] = None, n_iter: int = 20, dt: float = 2e-3,
+                     scheme: str = "crweno5", upwinding: str = "llf-char", Re: float = 200.0,
+                     time_scheme_type: str = "ssprk3", weno: Optional[Dict] = None, delta: float = 0.05,
+                     amp: float = 0.05, file_op_iter: Optional[int] = None, op_file_format: str = "binary",
+                     screen_op_iter: int = 0) -> Dict:
+    """2D Navier-Stokes (no chemistry) double shear layer, periodic in x, slip
+    walls in y: u = tanh((y-1/4)/delta) - tanh((y-3/4)/delta) - 1,
+    v = amp sin(2 pi x), rho = 1, p = 1/gamma; Re from physics.inp."""
+    os.makedirs(path, exist_ok=True)
+    NX, NY = N, NY or N
+    gamma = 1.4
+    x = (np.arange(NX, dtype=np.float64) + 0.5) / NX
+    y = (np.arange(NY, dtype=np.float64) + 0.5) / NY
+    X, Y = np.meshgrid(x, y)
+    uu = np.tanh((Y - 0.25) / delta) - np.tanh((Y - 0.75) / delta) - 1.0
+    vv = amp * np.sin(2 * np.pi * X)
+    rho = np.ones_like(X)
+    p = 1.0 / gamma
+    u = np.zeros((NY, NX, 4))
+    u[..., 0] = rho
+    u[..., 1] = rho * uu
+    u[..., 2] = rho * vv
+    u[..., 3] = p / (gamma - 1.0) + 0.5 * rho * (uu * uu + vv * vv)
+    deck.write_keyfile(os.path.join(path, "solver.inp"), {
+        "ndims": 2, "nvars": 4, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
+        "time_scheme": "rk", "time_scheme_type": time_scheme_type,
+        "hyp_space_scheme": scheme, "hyp_interp_type": "components", "par_space_scheme": "2",
+        "dt": dt, "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
+        "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
+        "model": "navierstokes2d",
+    })
+    big = 1e99
+    deck.write_boundary(os.path.join(path, "boundary.inp"), [
+        deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0, -big, big]),
+        deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0, -big, big]),
+        deck.BoundaryZone("slip-wall", 1, 1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
+        deck.BoundaryZone("slip-wall", 1, -1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
+    ])
+    deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding, "Re": Re,
+                                                           "Pr": 0.72})
+    if weno:
+        deck.write_keyfile(os.path.join(path, "weno.inp"), weno)
+    deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, 4))
+    return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}

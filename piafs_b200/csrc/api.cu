@@ -1,0 +1,565 @@
+// C ABI of the PIAFS GPU path (include/piafs_gpu.h): simulation object,
+// time stepping with CUDA-graph replay, Solve() loop with reference-format
+// output, and the operator-level entry points.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/piafs_gpu.h"
+#include "deck.h"
+#include "kernels.h"
+
+using namespace piafs;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? PIAFS_ERR_MEMORY : PIAFS_ERR_CUDA,             \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                             \
+  } while (0)
+
+struct piafs_gpu_sim {
+  Deck deck;
+  DevParams P;
+  int precision = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // device state (structure of arrays)
+  double* u = nullptr;
+  double* U[MAX_STAGES] = {nullptr};       // U[0] aliases u
+  double* Ud[MAX_STAGES] = {nullptr};
+  double* fC = nullptr;
+  double* iface[5] = {nullptr};            // uL, uR, fL, fR, operator scratch
+  double* scratch = nullptr;               // ghosted plane set for operator calls
+  double* dxinv = nullptr;
+  double* imap = nullptr;
+  double* tdev = nullptr;                  // simulation time on the device
+  double* top_t = nullptr;                 // time for operator calls
+  double* norm_acc = nullptr;
+  unsigned long long* cfl_acc = nullptr;
+  int* err = nullptr;
+  double* aos = nullptr;                   // ghosted AoS staging (host transfers)
+  size_t aos_bytes = 0;
+  // host mirror of the clock
+  double t = 0.0;
+  int iter = 0;
+  double last_cfl = -1.0, last_norm = 0.0;
+  int singular = 0;
+  // CUDA graphs of one step: [0] plain, [1] with residual norm
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool use_graph = true;
+};
+
+static void free_sim(piafs_gpu_sim* s) {
+  if (!s) return;
+  for (auto& g : s->graph) if (g) cudaGraphExecDestroy(g);
+  cudaFree(s->u);
+  for (int k = 1; k < MAX_STAGES; k++) cudaFree(s->U[k]);
+  for (auto p : s->Ud) cudaFree(p);
+  cudaFree(s->fC);
+  for (auto p : s->iface) cudaFree(p);
+  cudaFree(s->scratch);
+  cudaFree(s->dxinv);
+  cudaFree(s->imap);
+  cudaFree(s->tdev);
+  cudaFree(s->top_t);
+  cudaFree(s->norm_acc);
+  cudaFree(s->cfl_acc);
+  cudaFree(s->err);
+  cudaFree(s->aos);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+// -------------------------------------------------------------- the RHS
+// TimeRHSFunctionExplicit (TimeRHSFunctionExplicit.c:29-77) on SoA arrays:
+// rhs = -hyp + par + source; U must have its ghosts filled.
+static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const double* tdev, double cstage) {
+  const DevParams& P = s->P;
+  for (int d = 0; d < P.ndims; d++) {
+    launch_flux(P, U, s->fC, d, s->stream);
+    if (P.scheme == WENO5)
+      launch_weno5(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->stream);
+    else
+      launch_crweno(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->err, s->stream);
+    launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, rhs, d, d == 0 ? 0 : 1,
+                      s->stream);
+  }
+  launch_visc_source(P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream);
+}
+
+static void enqueue_bc(piafs_gpu_sim* s, double* u) {
+  for (const Zone& z : s->deck.zones) launch_bc(s->P, u, z, s->stream);
+}
+
+// One time step: TimePreStep's boundary conditions on u, TimeRK's stages and
+// step completion, t += dt.  U[0] aliases u: the reference copies u into
+// U[0] and re-applies the (idempotent) boundary conditions to it.
+static void enqueue_step(piafs_gpu_sim* s, bool with_norm) {
+  const DevParams& P = s->P;
+  const Deck& d = s->deck;
+  const int ns = d.nstages;
+  const long long n = (long long)P.nvars * P.ps;
+  enqueue_bc(s, s->u);
+  for (int st = 0; st < ns; st++) {
+    double* Us = st == 0 ? s->u : s->U[st];
+    if (st > 0) {
+      const double* dd[MAX_STAGES];
+      double a[MAX_STAGES];
+      for (int j = 0; j < st; j++) { dd[j] = s->Ud[j]; a[j] = d.dt * d.A[st * MAX_STAGES + j]; }
+      launch_stage(n, Us, s->u, dd, a, st, s->stream);
+      enqueue_bc(s, Us);
+    }
+    enqueue_rhs(s, s->Ud[st], Us, s->tdev, d.c[st]);
+  }
+  const double* dd[MAX_STAGES];
+  double b[MAX_STAGES];
+  for (int j = 0; j < ns; j++) { dd[j] = s->Ud[j]; b[j] = d.dt * d.b[j]; }
+  if (with_norm) cudaMemsetAsync(s->norm_acc, 0, sizeof(double), s->stream);
+  launch_update(P, s->u, dd, b, ns, with_norm ? s->norm_acc : nullptr, s->stream);
+  launch_advance_time(s->tdev, d.dt, s->stream);
+}
+
+static int run_steps(piafs_gpu_sim* s, int nsteps, bool norm_last) {
+  for (int k = 0; k < nsteps; k++) {
+    const bool with_norm = norm_last && (k == nsteps - 1);
+    const int gi = with_norm ? 1 : 0;
+    if (s->use_graph) {
+      if (!s->graph[gi]) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(s, with_norm);
+        CK(cudaStreamEndCapture(s->stream, &g));
+        CK(cudaGraphInstantiate(&s->graph[gi], g, 0));
+        cudaGraphDestroy(g);
+      }
+      CK(cudaGraphLaunch(s->graph[gi], s->stream));
+    } else {
+      enqueue_step(s, with_norm);
+    }
+    s->t += s->deck.dt;   // same accumulation as the device clock (TimePostStep.c:31)
+    s->iter++;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->stream));
+  int e = 0;
+  CK(cudaMemcpy(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    s->singular++;
+    cudaMemset(s->err, 0, sizeof(int));
+  }
+  if (norm_last) {
+    double sum = 0.0;
+    CK(cudaMemcpy(&sum, s->norm_acc, sizeof(double), cudaMemcpyDeviceToHost));
+    double npts = (double)s->P.N0 * (double)s->P.N1;
+    s->last_norm = std::sqrt(sum / npts);
+  }
+  return PIAFS_OK;
+}
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* piafs_gpu_last_error(void) { return g_err.c_str(); }
+
+int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
+  if (!deck_dir || !out) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (precision != PIAFS_PRECISION_FP64)
+    return fail(PIAFS_ERR_UNSUPPORTED, "only the FP64 path is available in this build");
+  auto* s = new piafs_gpu_sim();
+  std::string err;
+  int r = read_deck(deck_dir, s->deck, err);
+  if (!r) r = make_params(s->deck, s->P, err);
+  if (r) { delete s; return fail(r, err); }
+  s->precision = precision;
+  const char* ng = std::getenv("PIAFS_GPU_NO_GRAPH");
+  s->use_graph = !(ng && ng[0] == '1');
+  const DevParams& P = s->P;
+  const Deck& d = s->deck;
+  auto alloc = [&](double** p, size_t n) -> cudaError_t {
+    cudaError_t e = cudaMalloc(p, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, n * sizeof(double));
+    return e;
+  };
+  cudaError_t e = cudaGetDevice(&s->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  const size_t planes = (size_t)P.nvars * P.ps, iplanes = (size_t)P.nvars * P.pis;
+  if (e == cudaSuccess) e = alloc(&s->u, planes);
+  for (int k = 1; k < d.nstages && e == cudaSuccess; k++) e = alloc(&s->U[k], planes);
+  for (int k = 0; k < d.nstages && e == cudaSuccess; k++) e = alloc(&s->Ud[k], planes);
+  if (e == cudaSuccess) e = alloc(&s->fC, planes);
+  for (int k = 0; k < 5 && e == cudaSuccess; k++) e = alloc(&s->iface[k], iplanes);
+  if (e == cudaSuccess) e = alloc(&s->scratch, planes);
+  if (e == cudaSuccess) e = alloc(&s->dxinv, d.dxinv.size());
+  if (e == cudaSuccess) e = alloc(&s->imap, d.imap.size());
+  if (e == cudaSuccess) e = alloc(&s->tdev, 1);
+  if (e == cudaSuccess) e = alloc(&s->top_t, 1);
+  if (e == cudaSuccess) e = alloc(&s->norm_acc, 1);
+  if (e == cudaSuccess) e = cudaMalloc(&s->cfl_acc, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&s->err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(s->err, 0, sizeof(int));
+  s->aos_bytes = (size_t)P.npg * P.nvars * sizeof(double);
+  if (e == cudaSuccess) e = cudaMalloc(&s->aos, s->aos_bytes);
+  if (e == cudaSuccess) e = cudaMemcpy(s->dxinv, d.dxinv.data(), d.dxinv.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->imap, d.imap.data(), d.imap.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    int code = e == cudaErrorMemoryAllocation ? PIAFS_ERR_MEMORY : PIAFS_ERR_CUDA;
+    std::string msg = std::string("device set-up failed: ") + cudaGetErrorString(e);
+    free_sim(s);
+    return fail(code, msg);
+  }
+  s->U[0] = s->u;
+  // initial solution; restart time waqt = restart_iter * dt (TimeInitialize.c:51)
+  int rr = piafs_gpu_set_state(s, d.u0.data(), d.restart_iter * d.dt);
+  if (rr) { free_sim(s); return rr; }
+  s->iter = d.restart_iter;
+  *out = s;
+  return PIAFS_OK;
+}
+
+void piafs_gpu_destroy(piafs_gpu_sim* s) { free_sim(s); }
+
+int piafs_gpu_get_info(piafs_gpu_sim* s, piafs_gpu_info* info) {
+  if (!s || !info) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  const Deck& d = s->deck;
+  std::memset(info, 0, sizeof(*info));
+  info->ndims = d.ndims; info->nvars = d.nvars; info->ghosts = d.ghosts;
+  info->dim[0] = s->P.N0; info->dim[1] = s->P.N1;
+  info->n_iter = d.n_iter; info->restart_iter = d.restart_iter;
+  info->screen_op_iter = d.screen_op_iter; info->file_op_iter = d.file_op_iter;
+  info->iter = s->iter; info->nstages = d.nstages;
+  info->dt = d.dt; info->t = s->t;
+  info->gamma = d.gamma; info->Re = d.Re; info->Pr = d.Pr;
+  info->npoints_ghosted = s->P.npg;
+  info->ninterfaces[0] = s->P.nint[0]; info->ninterfaces[1] = s->P.nint[1];
+  info->cfl = s->last_cfl; info->norm = s->last_norm; info->singular = s->singular;
+  // kernels per step: prestep BCs, per stage (combine + BCs for s > 0, three
+  // per direction, viscous/source), update, clock
+  const int nz = (int)d.zones.size();
+  const int vs = ((s->P.ndims == 2 && s->P.viscous) || s->P.chem) ? 1 : 0;
+  info->launches_per_step = nz + d.nstages * (3 * s->P.ndims + vs) + (d.nstages - 1) * (1 + nz) + 2;
+  return PIAFS_OK;
+}
+
+int piafs_gpu_set_state(piafs_gpu_sim* s, const double* u_host, double t) {
+  if (!s || !u_host) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  CK(cudaMemcpyAsync(s->aos, u_host, s->aos_bytes, cudaMemcpyHostToDevice, s->stream));
+  launch_aos_to_soa(s->aos, s->u, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  CK(cudaMemcpyAsync(s->tdev, &t, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->t = t;
+  return PIAFS_OK;
+}
+
+int piafs_gpu_get_state(piafs_gpu_sim* s, double* u_host) {
+  if (!s || !u_host) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  launch_soa_to_aos(s->u, s->aos, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  CK(cudaMemcpyAsync(u_host, s->aos, s->aos_bytes, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return PIAFS_OK;
+}
+
+int piafs_gpu_get_solution(piafs_gpu_sim* s, double* out) {
+  if (!s || !out) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  launch_soa_to_interior(s->P, s->u, s->aos, s->stream);
+  CK(cudaMemcpyAsync(out, s->aos, (size_t)s->P.N0 * s->P.N1 * s->P.nvars * sizeof(double), cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return PIAFS_OK;
+}
+
+int piafs_gpu_TimeRK(piafs_gpu_sim* s, int nsteps) {
+  if (!s || nsteps < 0) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  return run_steps(s, nsteps, false);
+}
+
+int piafs_gpu_TimeRK_async(piafs_gpu_sim* s, int nsteps) {
+  if (!s || nsteps < 0) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  for (int k = 0; k < nsteps; k++) {
+    if (s->use_graph) {
+      if (!s->graph[0]) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(s, false);
+        CK(cudaStreamEndCapture(s->stream, &g));
+        CK(cudaGraphInstantiate(&s->graph[0], g, 0));
+        cudaGraphDestroy(g);
+      }
+      CK(cudaGraphLaunch(s->graph[0], s->stream));
+    } else {
+      enqueue_step(s, false);
+    }
+    s->t += s->deck.dt;
+    s->iter++;
+  }
+  CK(cudaGetLastError());
+  return PIAFS_OK;
+}
+
+int piafs_gpu_get_stream(piafs_gpu_sim* s, void** stream) {
+  if (!s || !stream) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  *stream = (void*)s->stream;
+  return PIAFS_OK;
+}
+
+int piafs_gpu_synchronize(piafs_gpu_sim* s) {
+  if (!s) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  CK(cudaStreamSynchronize(s->stream));
+  int e = 0;
+  CK(cudaMemcpy(&e, s->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) { s->singular++; cudaMemset(s->err, 0, sizeof(int)); }
+  return PIAFS_OK;
+}
+
+int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) {
+  if (!s || !ms || !nphases || reps < 1) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  const DevParams& P = s->P;
+  const int np = 3 * P.ndims + 1;
+  if (*nphases < np) return fail(PIAFS_ERR_ARGUMENT, "ms[] too small");
+  *nphases = np;
+  std::vector<cudaEvent_t> ev(np + 1);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(np, 0.0);
+  double* U = s->u;
+  double* R = s->Ud[0];
+  for (int r = 0; r < reps; r++) {
+    enqueue_bc(s, U);
+    int k = 0;
+    CK(cudaEventRecord(ev[0], s->stream));
+    for (int d = 0; d < P.ndims; d++) {
+      launch_flux(P, U, s->fC, d, s->stream);
+      CK(cudaEventRecord(ev[++k], s->stream));
+      if (P.scheme == WENO5)
+        launch_weno5(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->stream);
+      else
+        launch_crweno(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->err, s->stream);
+      CK(cudaEventRecord(ev[++k], s->stream));
+      launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, R, d, d == 0 ? 0 : 1,
+                        s->stream);
+      CK(cudaEventRecord(ev[++k], s->stream));
+    }
+    launch_visc_source(P, U, s->dxinv, s->imap, s->tdev, 0.0, R, 1, 1, s->stream);
+    CK(cudaEventRecord(ev[++k], s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < np; i++) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      acc[i] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int i = 0; i < np; i++) ms[i] = acc[i] / reps;
+  CK(cudaGetLastError());
+  return PIAFS_OK;
+}
+
+int piafs_gpu_TimeRK_host(piafs_gpu_sim* s, double* u_host, double t) {
+  if (int r = piafs_gpu_set_state(s, u_host, t)) return r;
+  if (int r = run_steps(s, 1, false)) return r;
+  return piafs_gpu_get_state(s, u_host);
+}
+
+int piafs_gpu_ComputeCFL(piafs_gpu_sim* s, double* cfl) {
+  if (!s || !cfl) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  CK(cudaMemsetAsync(s->cfl_acc, 0, sizeof(unsigned long long), s->stream));
+  launch_cfl(s->P, s->u, s->dxinv, s->cfl_acc, s->stream);
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, s->cfl_acc, sizeof(bits), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  std::memcpy(cfl, &bits, sizeof(double));
+  s->last_cfl = *cfl;
+  return PIAFS_OK;
+}
+
+int piafs_gpu_Solve(piafs_gpu_sim* s, const char* output_dir) {
+  if (!s || !output_dir) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  const Deck& d = s->deck;
+  const bool write = d.op_file_format == "binary" || d.op_file_format == "bin";
+  if (!write && d.op_file_format != "none")
+    return fail(PIAFS_ERR_UNSUPPORTED, "op_file_format " + d.op_file_format + " is not supported (binary, none)");
+  const bool overwrite = d.op_overwrite != "no";
+  int index = 0;
+  // a restart fast-forwards the output index (InitializeSolvers.c:240-245)
+  if (!overwrite)
+    for (int t = 0; t < d.restart_iter; t++)
+      if ((t + 1) % d.file_op_iter == 0) index++;
+  std::vector<double> host((size_t)s->P.N0 * s->P.N1 * d.nvars);
+  auto output = [&]() -> int {
+    if (!write) return PIAFS_OK;
+    if (int r = piafs_gpu_get_solution(s, host.data())) return r;
+    char name[64];
+    if (overwrite) std::snprintf(name, sizeof(name), "op.bin");
+    else std::snprintf(name, sizeof(name), "op_%05d.bin", index);
+    std::string err;
+    if (int r = write_binary(std::string(output_dir) + "/" + name, d, host.data(), err)) return fail(r, err);
+    if (!overwrite) index++;
+    return PIAFS_OK;
+  };
+  // Solve.cpp:54-95
+  for (int it = s->iter; it < d.n_iter; it++) {
+    if (it == 0) if (int r = output()) return r;
+    const bool screen = ((it + 1) % d.screen_op_iter) == 0;
+    if (screen) {
+      double c;
+      if (int r = piafs_gpu_ComputeCFL(s, &c)) return r;
+    }
+    if (int r = run_steps(s, 1, screen)) return r;
+    if (((it + 1) % d.file_op_iter == 0) && (it + 1 < d.n_iter))
+      if (int r = output()) return r;
+  }
+  return output();
+}
+
+// ------------------------------------------------- operator-level calls
+static int to_soa(piafs_gpu_sim* s, const double* aos, double* soa) {
+  launch_aos_to_soa(aos, soa, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  return PIAFS_OK;
+}
+static int set_top_t(piafs_gpu_sim* s, double t) {
+  CK(cudaMemcpyAsync(s->top_t, &t, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+  return PIAFS_OK;
+}
+static int finish(piafs_gpu_sim* s) {
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->stream));
+  return PIAFS_OK;
+}
+
+int piafs_gpu_RHSFunction(piafs_gpu_sim* s, double* rhs, double* u, double t) {
+  if (!s || !rhs || !u) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  const size_t planes = (size_t)s->P.nvars * s->P.ps * sizeof(double);
+  double* U = s->scratch;
+  double* R = s->Ud[0];
+  to_soa(s, u, U);
+  enqueue_bc(s, U);
+  CK(cudaMemsetAsync(R, 0, planes, s->stream));
+  if (int r = set_top_t(s, t)) return r;
+  enqueue_rhs(s, R, U, s->top_t, 0.0);
+  launch_soa_to_aos(U, u, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  launch_soa_to_aos(R, rhs, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  return finish(s);
+}
+
+int piafs_gpu_HyperbolicFunction(piafs_gpu_sim* s, double* hyp, const double* u, double t) {
+  if (!s || !hyp || !u) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  const DevParams& P = s->P;
+  double* U = s->scratch;
+  double* H = s->Ud[0];
+  to_soa(s, u, U);
+  CK(cudaMemsetAsync(H, 0, (size_t)P.nvars * P.ps * sizeof(double), s->stream));
+  for (int d = 0; d < P.ndims; d++) {
+    launch_flux(P, U, s->fC, d, s->stream);
+    if (P.scheme == WENO5)
+      launch_weno5(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->stream);
+    else
+      launch_crweno(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->err, s->stream);
+    launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, H, d, d == 0 ? 2 : 3,
+                      s->stream);
+  }
+  launch_soa_to_aos(H, hyp, P.npg, P.nvars, P.ps, s->stream);
+  return finish(s);
+}
+
+static int visc_or_source(piafs_gpu_sim* s, double* out, const double* u, double t, int visc, int chem) {
+  if (!s || !out || !u) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  const DevParams& P = s->P;
+  double* U = s->scratch;
+  double* R = s->Ud[0];
+  to_soa(s, u, U);
+  CK(cudaMemsetAsync(R, 0, (size_t)P.nvars * P.ps * sizeof(double), s->stream));
+  if (int r = set_top_t(s, t)) return r;
+  launch_visc_source(P, U, s->dxinv, s->imap, s->top_t, 0.0, R, visc, chem, s->stream);
+  launch_soa_to_aos(R, out, P.npg, P.nvars, P.ps, s->stream);
+  return finish(s);
+}
+int piafs_gpu_ParabolicFunction(piafs_gpu_sim* s, double* par, const double* u, double t) {
+  return visc_or_source(s, par, u, t, 1, 0);
+}
+int piafs_gpu_SourceFunction(piafs_gpu_sim* s, double* src, const double* u, double t) {
+  return visc_or_source(s, src, u, t, 0, 1);
+}
+
+int piafs_gpu_ApplyBoundaryConditions(piafs_gpu_sim* s, double* u, double) {
+  if (!s || !u) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  to_soa(s, u, s->scratch);
+  enqueue_bc(s, s->scratch);
+  launch_soa_to_aos(s->scratch, u, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  return finish(s);
+}
+
+int piafs_gpu_FFunction(piafs_gpu_sim* s, double* f, const double* u, int dir, double) {
+  if (!s || !f || !u || dir < 0 || dir >= s->P.ndims) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  to_soa(s, u, s->scratch);
+  launch_flux(s->P, s->scratch, s->fC, dir, s->stream);
+  launch_soa_to_aos(s->fC, f, s->P.npg, s->P.nvars, s->P.ps, s->stream);
+  return finish(s);
+}
+
+int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* s, double* fI, const double* fC, const double* u, int upw,
+                                       int dir, int uflag) {
+  if (!s || !fI || !fC || !u || dir < 0 || dir >= s->P.ndims) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  const DevParams& P = s->P;
+  to_soa(s, u, s->scratch);
+  to_soa(s, fC, s->fC);
+  if (P.scheme == WENO5)
+    launch_weno5(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);
+  else
+    launch_crweno(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->err, s->stream);
+  const double* src = s->iface[(uflag ? 0 : 2) + (upw > 0 ? 0 : 1)];
+  launch_iface_soa_to_aos(src, fI, P.nint[dir], P.nvars, P.pis, s->stream);
+  return finish(s);
+}
+
+int piafs_gpu_Upwind(piafs_gpu_sim* s, double* fI, const double* fL, const double* fR, const double* uL,
+                     const double* uR, const double* u, int dir, double) {
+  if (!s || !fI || !fL || !fR || !uL || !uR || !u || dir < 0 || dir >= s->P.ndims)
+    return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  const DevParams& P = s->P;
+  const long long ni = P.nint[dir];
+  to_soa(s, u, s->scratch);
+  launch_iface_aos_to_soa(uL, s->iface[0], ni, P.nvars, P.pis, s->stream);
+  launch_iface_aos_to_soa(uR, s->iface[1], ni, P.nvars, P.pis, s->stream);
+  launch_iface_aos_to_soa(fL, s->iface[2], ni, P.nvars, P.pis, s->stream);
+  launch_iface_aos_to_soa(fR, s->iface[3], ni, P.nvars, P.pis, s->stream);
+  launch_upwind_iface(P, s->scratch, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->iface[4], dir, s->stream);
+  launch_iface_soa_to_aos(s->iface[4], fI, ni, P.nvars, P.pis, s->stream);
+  return finish(s);
+}
+
+int piafs_gpu_FirstDerivativePar(piafs_gpu_sim* s, double* Df, const double* f, int dir, int bias, int nv) {
+  if (!s || !Df || !f || dir < 0 || dir >= s->P.ndims || nv < 1) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  launch_first_deriv(s->P, Df, f, dir, bias, nv, s->stream);
+  return finish(s);
+}
+
+int piafs_gpu_tridiagLU(double* a, double* b, double* c, double* x, int n, int ns) {
+  if (!a || !b || !c || !x || n < 0 || ns < 0) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  if (n == 0 || ns == 0) return PIAFS_OK;
+  int* err = nullptr;
+  CK(cudaMalloc(&err, sizeof(int)));
+  CK(cudaMemset(err, 0, sizeof(int)));
+  launch_tridiag(a, b, c, x, n, ns, err, 0);
+  int h = 0;
+  cudaError_t e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(err);
+  CK(e);
+  CK(cudaGetLastError());
+  if (h) return fail(PIAFS_ERR_SINGULAR, "zero pivot in tridiagLU");
+  return PIAFS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// Shared device-side definitions for the PIAFS GPU path.
+//
+// Device layout (structure of arrays): variable v of point p lives at
+// u[v * ps + p], where p = (i + g) + W0 * (j + g) is the reference's point
+// index (include/arrayfunctions.h:43-50) and ps is the plane stride (the
+// ghosted point count rounded up to 32 doubles so every plane starts on a
+// 256-byte boundary).  Interface arrays use the same scheme with the
+// reference's interface index (bounds_inter, HyperbolicFunction.c:64-66):
+// q = i + (N0+1) * j along x, q = i + N0 * j along y.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace piafs {
+
+enum Model { EULER1D = 0, NS2D = 1 };
+enum Scheme { WENO5 = 0, CRWENO5 = 1 };
+enum Upwind { UPW_ROE = 0, UPW_RF = 1, UPW_LLF = 2, UPW_RUSANOV = 3 };
+enum WenoType { W_JS = 0, W_MAPPED = 1, W_BORGES = 2, W_YC = 3 };
+enum BcType { BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_SLIPWALL = 2 };
+
+constexpr int MAX_ZONES = 16;
+constexpr int MAX_STAGES = 4;
+
+// Everything a kernel needs to know about one simulation; passed by value.
+struct DevParams {
+  int ndims, nvars, ghosts;
+  int N0, N1;            // interior sizes (N1 = 1 in 1D)
+  int W0, W1;            // ghosted sizes (W1 = 1 in 1D)
+  int g1;                // ghosts along dim 1 (0 in 1D)
+  long long npg;         // ghosted points
+  long long ps;          // plane stride (points)
+  long long nint[2];     // interfaces per direction
+  long long pis;         // interface plane stride
+  int model, scheme, upwind, weno_type, no_limiting;
+  double eps;
+  double gamma, bc_gamma, Re, Pr, Tref, T0, TS, TA, TB;
+  int viscous;
+  // photochemistry (normalised, ChemistryInitialize.c:267-353)
+  int chem, nflow, nz, zstride;
+  double k[11], q[11];
+  double chem_gamma, I0, ch_c, ch_h, ch_nu, n_O2, t_start_norm, t_pulse_norm, sO3, dz;
+  double dt;
+};
+
+__host__ __device__ inline long long pidx(const DevParams& P, int i, int j) {
+  return (long long)(i + P.ghosts) + (long long)P.W0 * (long long)(j + P.g1);
+}
+
+// ------------------------------------------------------------ flow variables
+// _NavierStokes2DGetFlowVar_ (navierstokes2d.h:70-80)
+template <typename T>
+__device__ __forceinline__ void ns_flowvar(T rho_in, T ru, T rv, T e_in, T gamma, T& rho, T& vx,
+                                           T& vy, T& e, T& P) {
+  rho = rho_in;
+  vx = (rho == T(0)) ? T(0) : ru / rho;
+  vy = (rho == T(0)) ? T(0) : rv / rho;
+  e = e_in;
+  T vsq = (vx * vx) + (vy * vy);
+  P = (e - T(0.5) * rho * vsq) * (gamma - T(1));
+}
+// _Euler1DGetFlowVar_ (euler1d.h:61-69)
+template <typename T>
+__device__ __forceinline__ void eu_flowvar(T rho_in, T ru, T e_in, T gamma, T& rho, T& v, T& e, T& P) {
+  rho = rho_in;
+  v = ru / rho;
+  e = e_in;
+  P = (e - T(0.5) * rho * v * v) * (gamma - T(1));
+}
+
+// --------------------------------------------------------------- WENO weights
+// Nonlinear weights of the fifth-order WENO family for one stencil
+// (m3,m2,m1,p1,p2) and optimal weights (c1,c2,c3).  Jiang-Shu, mapped
+// (Henrick-Aslam-Powers), Borges (WENO-Z) and Yamaleev-Carpenter variants as
+// selected in weno.inp (interpolation.h:255-545).  The Jiang-Shu weights are
+// normalised with a single reciprocal: w_k = c_k prod_{m!=k} q_m / sum, with
+// q_m = (beta_m + eps)^2, which equals c_k/q_k / sum_m c_m/q_m.
+template <typename T>
+__device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T m2, T m1, T p1,
+                                             T p2, T eps, T& w1, T& w2, T& w3) {
+  const T t1312 = T(13.0 / 12.0), q4 = T(0.25);
+  T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
+  T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
+  T d3 = m1 - T(2) * p1 + p2, e3 = T(3) * m1 - T(4) * p1 + p2;
+  T b1 = t1312 * d1 * d1 + q4 * e1 * e1;
+  T b2 = t1312 * d2 * d2 + q4 * e2 * e2;
+  T b3 = t1312 * d3 * d3 + q4 * e3 * e3;
+  if (type == W_JS || type == W_MAPPED) {
+    T s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
+    T q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
+    T a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
+    T inv = T(1) / (a1 + a2 + a3);
+    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+    if (type == W_MAPPED) {
+      T x1 = w1, x2 = w2, x3 = w3;
+      T n1 = x1 * (c1 + c1 * c1 - T(3) * c1 * x1 + x1 * x1), d1m = (c1 * c1 + x1 * (T(1) - T(2) * c1));
+      T n2 = x2 * (c2 + c2 * c2 - T(3) * c2 * x2 + x2 * x2), d2m = (c2 * c2 + x2 * (T(1) - T(2) * c2));
+      T n3 = x3 * (c3 + c3 * c3 - T(3) * c3 * x3 + x3 * x3), d3m = (c3 * c3 + x3 * (T(1) - T(2) * c3));
+      T A1 = n1 / d1m, A2 = n2 / d2m, A3 = n3 / d3m;
+      T inv2 = T(1) / (A1 + A2 + A3);
+      w1 = A1 * inv2; w2 = A2 * inv2; w3 = A3 * inv2;
+    }
+    return;
+  }
+  T tau;
+  if (type == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
+  else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = t * t; }
+  T r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
+  T a1 = c1 * (T(1) + r1 * r1), a2 = c2 * (T(1) + r2 * r2), a3 = c3 * (T(1) + r3 * r3);
+  T inv = T(1) / (a1 + a2 + a3);
+  w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+}
+
+// 3-point candidate values of explicit WENO5 (Interp1PrimFifthOrderWENO.c:144-146)
+template <typename T>
+__device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p1, T p2) {
+  const T s = T(1.0 / 6.0);
+  T f1 = (T(2) * s) * m3 + (T(-7) * s) * m2 + (T(11) * s) * m1;
+  T f2 = (-s) * m2 + (T(5) * s) * m1 + (T(2) * s) * p1;
+  T f3 = (T(2) * s) * m1 + (T(5) * s) * p1 + (-s) * p2;
+  return w1 * f1 + w2 * f2 + w3 * f3;
+}
+
+}  // namespace piafs

@@ -1,0 +1,58 @@
+// Host-side set-up of a PIAFS simulation from its input deck.
+//
+// Mirrors the reference's initialisation sequence for the hot path
+// (src/Simulation/ReadInputs.c, Initialize.c, InitialSolution.c,
+// InitializeBoundaries.c, InitializeSolvers.c, InitializePhysics.c and the
+// model/chemistry initialisers) and produces the flat parameters, grid,
+// initial state and boundary zones the device path consumes.
+#pragma once
+#include <string>
+#include <vector>
+#include "common.cuh"
+#include "kernels.h"
+
+namespace piafs {
+
+struct Deck {
+  // solver.inp (ReadInputs.c:202-229 defaults)
+  int ndims = 1, nvars = 1, ghosts = 1;
+  std::vector<int> size;
+  int n_iter = 0, restart_iter = 0, screen_op_iter = 1, file_op_iter = 1000;
+  double dt = 0.0;
+  std::string time_scheme = "euler", time_scheme_type = " ", hyp_space_scheme = "1", hyp_interp_type = "characteristic";
+  std::string par_space_scheme = "2", ip_file_type = "ascii", op_file_format = "text", op_overwrite = "no";
+  std::string model = "none", input_mode = "serial", output_mode = "serial", conservation_check = "no";
+  // physics.inp
+  double gamma = 1.4, Pr = 0.72, Re = -1.0, Tref = 273.15, T0 = 275.0, TS = 110.4, TA = 245.4, TB = 27.6;
+  std::string upwinding = "roe", include_chem = "no", write_output = "yes";
+  // weno.inp
+  int mapped = 0, borges = 0, yc = 0, no_limiting = 0;
+  double weno_eps = 1e-6;
+  // derived
+  double bc_gamma = 1.4;      // wall BCs keep the physics.inp gamma
+  int nstages = 1;
+  double A[MAX_STAGES * MAX_STAGES] = {0}, b[MAX_STAGES] = {0}, c[MAX_STAGES] = {0};
+  // chemistry (normalised), valid if chem
+  bool chem = false;
+  int nz = 1;
+  double chem_gamma = 0, kn[11] = {0}, qn[11] = {0}, I0 = 0, ch_c = 0, ch_h = 0, ch_nu = 0, n_O2 = 0;
+  double t_start_norm = 0, t_pulse_norm = 0, sO3 = 0, dz = 0;
+  double L_ref = 0, kg = 0, IA = 1, IB = 1, IC = 0;
+  // grid and fields (host, reference layout)
+  std::vector<double> x;        // ghosted coordinates, dims concatenated
+  std::vector<double> dxinv;    // ghosted 1/dx, dims concatenated
+  std::vector<double> grid;     // interior coordinates, dims concatenated (for output)
+  std::vector<double> u0;       // AoS with ghosts
+  std::vector<double> imap;     // ghosted (chemistry only)
+  std::vector<Zone> zones;
+};
+
+// Parse the deck in `dir`.  Returns 0 on success, otherwise a PIAFS_ERR_*
+// code with a message in `err`.
+int read_deck(const std::string& dir, Deck& d, std::string& err);
+// Flat device parameters from a parsed deck.
+int make_params(const Deck& d, DevParams& P, std::string& err);
+// Write an op_*.bin file (WriteBinary.c:37-93) from the interior AoS field.
+int write_binary(const std::string& path, const Deck& d, const double* u_interior, std::string& err);
+
+}  // namespace piafs

@@ -1,0 +1,919 @@
+// Hot-path kernels of the PIAFS GPU path (sm_100a).
+//
+// Per RK stage the host enqueues, for each direction d:
+//   k_flux          cell-centred flux F_d(U) at every point (FFunction)
+//   k_weno5 or      interface values uL,uR,fL,fR (InterpolateInterfacesHyp
+//   k_crweno_line     with the weights of SetInterpLimiterVar fused in)
+//   k_upwind_div    upwind flux at interfaces + conservative difference,
+//                   accumulated into the stage derivative (Upwind +
+//                   HyperbolicFunction's dxinv*(fI[j+1]-fI[j]))
+// then k_visc_source (ParabolicFunction + SourceFunction) and the RK
+// kernels k_stage / k_update (TimeRK).  All state is FP64.
+#include <cstdio>
+#include "kernels.h"
+#include "physics.cuh"
+
+namespace piafs {
+
+// ============================================================ layout helpers
+__global__ void k_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long long npg,
+                             int nv, long long ps) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= npg * nv) return;
+  long long p = idx / nv;
+  int v = (int)(idx - p * nv);
+  soa[v * ps + p] = aos[idx];
+}
+__global__ void k_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, long long npg,
+                             int nv, long long ps) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= npg * nv) return;
+  long long p = idx / nv;
+  int v = (int)(idx - p * nv);
+  aos[idx] = soa[v * ps + p];
+}
+// interior points only, op-file order (point-major, dim0 fastest)
+__global__ void k_soa_to_interior(DevParams P, const double* __restrict__ soa, double* __restrict__ out) {
+  long long n = (long long)P.N0 * P.N1 * P.nvars;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  long long pt = idx / P.nvars;
+  int v = (int)(idx - pt * P.nvars);
+  int i = (int)(pt % P.N0), j = (int)(pt / P.N0);
+  out[idx] = soa[v * P.ps + pidx(P, i, j)];
+}
+__global__ void k_interior_to_soa(DevParams P, const double* __restrict__ in, double* __restrict__ soa) {
+  long long n = (long long)P.N0 * P.N1 * P.nvars;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  long long pt = idx / P.nvars;
+  int v = (int)(idx - pt * P.nvars);
+  int i = (int)(pt % P.N0), j = (int)(pt / P.N0);
+  soa[v * P.ps + pidx(P, i, j)] = in[idx];
+}
+// interface arrays: AoS (reference) <-> SoA (device)
+__global__ void k_iface_aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, long long ni,
+                                   int nv, long long pis) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= ni * nv) return;
+  long long q = idx / nv;
+  int v = (int)(idx - q * nv);
+  soa[v * pis + q] = aos[idx];
+}
+__global__ void k_iface_soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, long long ni,
+                                   int nv, long long pis) {
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= ni * nv) return;
+  long long q = idx / nv;
+  int v = (int)(idx - q * nv);
+  aos[idx] = soa[v * pis + q];
+}
+
+// ================================================================ boundaries
+// One zone of ApplyBoundaryConditions: BCPeriodicU (BCPeriodic.c:22-62),
+// BCExtrapolateU (BCExtrapolate.c:16-50), BCSlipWallU (BCSlipWall.c:24-136).
+// Only the ghost slab of the zone is written; corner ghosts are never touched.
+__global__ void k_bc_zone(DevParams P, double* __restrict__ u, Zone z) {
+  int ni = z.ie[0] - z.is[0], nj = z.ie[1] - z.is[1];
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)ni * nj) return;
+  int gi[2] = {z.is[0] + (int)(idx % ni), z.is[1] + (int)(idx / ni)};
+  int d = z.dim, b = gi[d] - z.is[d];
+  int src[2] = {gi[0], gi[1]};
+  int Nd = d == 0 ? P.N0 : P.N1;
+  if (z.type == BC_PERIODIC) {
+    // source keeps the zone-relative index in the other dimension
+    if (P.ndims == 2) src[1 - d] = gi[1 - d] - z.is[1 - d];
+    src[d] = z.face == 1 ? b + Nd - P.ghosts : b;
+  } else {
+    src[d] = z.face == 1 ? P.ghosts - 1 - b : Nd - b - 1;
+  }
+  long long p1 = pidx(P, gi[0], gi[1]), p2 = pidx(P, src[0], src[1]);
+  if (z.type == BC_SLIPWALL) {
+    double g = P.bc_gamma, igm1 = 1.0 / (g - 1.0);
+    if (P.ndims == 1) {
+      double rho, uv, e, pr;
+      eu_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], g, rho, uv, e, pr);
+      double ug = 2.0 * z.vel[0] - uv;
+      u[p1] = rho;
+      u[P.ps + p1] = rho * ug;
+      u[2 * P.ps + p1] = igm1 * pr + 0.5 * rho * ug * ug;
+    } else {
+      double rho, uv, vv, e, pr, ug, vg;
+      ns_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], u[3 * P.ps + p2], g, rho, uv, vv, e, pr);
+      if (d == 0) { ug = 2.0 * z.vel[0] - uv; vg = vv; }
+      else        { ug = uv; vg = 2.0 * z.vel[1] - vv; }
+      u[p1] = rho;
+      u[P.ps + p1] = rho * ug;
+      u[2 * P.ps + p1] = rho * vg;
+      u[3 * P.ps + p1] = igm1 * pr + 0.5 * rho * (ug * ug + vg * vg);
+    }
+  } else {
+    for (int v = 0; v < P.nvars; v++) u[v * P.ps + p1] = u[v * P.ps + p2];
+  }
+}
+
+// ======================================================================= RK
+// U_s = u + sum_{j<s} (dt a_sj) Udot_j at every point (TimeRK.c:46-57)
+__global__ void k_stage(long long n, double* __restrict__ Us, const double* __restrict__ u,
+                        const double* __restrict__ d0, double a0, const double* __restrict__ d1, double a1,
+                        const double* __restrict__ d2, double a2, int nterms) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x = u[i];
+  if (nterms > 0) x += a0 * d0[i];
+  if (nterms > 1) x += a1 * d1[i];
+  if (nterms > 2) x += a2 * d2[i];
+  Us[i] = x;
+}
+
+// u += sum_s (dt b_s) Udot_s (TimeRK.c:86-99); optionally accumulates
+// sum (u_old - u_new)^2 over interior points (TimePostStep.c:36-54)
+__global__ void k_update(DevParams P, double* __restrict__ u, const double* __restrict__ d0, double b0,
+                         const double* __restrict__ d1, double b1, const double* __restrict__ d2, double b2,
+                         const double* __restrict__ d3, double b3, int ns, double* __restrict__ norm_acc) {
+  long long n = (long long)P.nvars * P.ps;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double sq = 0.0;
+  if (i < n) {
+    double old = u[i], x = old;
+    if (ns > 0) x += b0 * d0[i];
+    if (ns > 1) x += b1 * d1[i];
+    if (ns > 2) x += b2 * d2[i];
+    if (ns > 3) x += b3 * d3[i];
+    u[i] = x;
+    if (norm_acc) {
+      long long p = i % P.ps;
+      if (p < P.npg) {
+        int ii = (int)(p % P.W0) - P.ghosts, jj = (int)(p / P.W0) - P.g1;
+        if (ii >= 0 && ii < P.N0 && jj >= 0 && jj < P.N1) { double d = old - x; sq = d * d; }
+      }
+    }
+  }
+  if (norm_acc) {
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    __shared__ double ws[32];
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = sq;
+    __syncthreads();
+    if (w == 0) {
+      sq = lane < (blockDim.x >> 5) ? ws[lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+      if (lane == 0) atomicAdd(norm_acc, sq);
+    }
+  }
+}
+
+// max local CFL over interior points (NavierStokes2DComputeCFL.c:19-56,
+// Euler1DComputeCFL.c).  Non-negative doubles order like their bit patterns.
+__global__ void k_cfl(DevParams P, const double* __restrict__ u, const double* __restrict__ dxinv,
+                      unsigned long long* __restrict__ out) {
+  long long n = (long long)P.N0 * P.N1;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double m = 0.0;
+  if (idx < n) {
+    int i = (int)(idx % P.N0), j = (int)(idx / P.N0);
+    long long p = pidx(P, i, j);
+    if (P.model == NS2D) {
+      double rho, vx, vy, e, pr;
+      ns_flowvar(u[p], u[P.ps + p], u[2 * P.ps + p], u[3 * P.ps + p], P.gamma, rho, vx, vy, e, pr);
+      double c = sqrt(P.gamma * pr / rho);
+      double lx = (absv(vx) + c) * P.dt * dxinv[P.ghosts + i];
+      double ly = (absv(vy) + c) * P.dt * dxinv[P.W0 + P.ghosts + j];
+      m = maxv(lx, ly);
+    } else {
+      double rho, v, e, pr;
+      eu_flowvar(u[p], u[P.ps + p], u[2 * P.ps + p], P.gamma, rho, v, e, pr);
+      double c = sqrt(P.gamma * pr / rho);
+      m = (absv(v) + c) * P.dt * dxinv[P.ghosts + i];
+    }
+    if (!(m >= 0.0)) m = 0.0;
+  }
+  for (int o = 16; o > 0; o >>= 1) m = maxv(m, __shfl_down_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// ===================================================================== flux
+// NavierStokes2DFlux (NavierStokes2DFlux.c:24-52) / Euler1DFlux, every point
+template <int MODEL, int DIR>
+__global__ void k_flux(DevParams P, const double* __restrict__ U, double* __restrict__ F) {
+  long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (p >= P.npg) return;
+  const long long ps = P.ps;
+  if (MODEL == NS2D) {
+    double rho, vx, vy, e, pr;
+    ns_flowvar(U[p], U[ps + p], U[2 * ps + p], U[3 * ps + p], P.gamma, rho, vx, vy, e, pr);
+    double vn = DIR == 0 ? vx : vy;
+    F[p] = rho * vn;
+    if (DIR == 0) { F[ps + p] = rho * vx * vx + pr; F[2 * ps + p] = rho * vx * vy; }
+    else          { F[ps + p] = rho * vy * vx; F[2 * ps + p] = rho * vy * vy + pr; }
+    F[3 * ps + p] = (e + pr) * vn;
+    for (int m = 4; m < P.nvars; m++) F[m * ps + p] = vn * U[m * ps + p];
+  } else {
+    double rho, v, e, pr;
+    eu_flowvar(U[p], U[ps + p], U[2 * ps + p], P.gamma, rho, v, e, pr);
+    F[p] = rho * v;
+    F[ps + p] = rho * v * v + pr;
+    F[2 * ps + p] = (e + pr) * v;
+    for (int m = 3; m < P.nvars; m++) F[m * ps + p] = v * U[m * ps + p];
+  }
+}
+
+// decode interface index q of direction DIR into (position along dir, line)
+template <int DIR>
+__device__ __forceinline__ void iface_decode(const DevParams& P, long long q, int& i, int& l) {
+  if (DIR == 0) { i = (int)(q % (P.N0 + 1)); l = (int)(q / (P.N0 + 1)); }
+  else          { l = (int)(q % P.N0);       i = (int)(q / P.N0); }
+}
+template <int DIR>
+__device__ __forceinline__ long long cell_of(const DevParams& P, int i, int l) {
+  return DIR == 0 ? pidx(P, i, l) : pidx(P, l, i);
+}
+
+// ==================================================================== WENO5
+// Interp1PrimFifthOrderWENO (Interp1PrimFifthOrderWENO.c:77-171) for the four
+// (upw, uflag) combinations with the weights of
+// WENOFifthOrderCalculateWeights fused in; one thread per (interface, var).
+template <int DIR>
+__global__ void k_weno5(DevParams P, const double* __restrict__ U, const double* __restrict__ F,
+                        double* __restrict__ uL, double* __restrict__ uR, double* __restrict__ fL,
+                        double* __restrict__ fR) {
+  const long long ni = P.nint[DIR];
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= ni * P.nvars) return;
+  int v = (int)(idx / ni);
+  long long q = idx - (long long)v * ni;
+  int i, l;
+  iface_decode<DIR>(P, q, i, l);
+  const long long st = DIR == 0 ? 1 : P.W0;
+  const long long c0 = cell_of<DIR>(P, i, l);    // cell i (right of the interface)
+  const double* u = U + (long long)v * P.ps + c0;
+  const double* f = F + (long long)v * P.ps + c0;
+  double a[6], b[6];     // cells i-3 .. i+2
+#pragma unroll
+  for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * st]; b[r] = f[(r - 3) * st]; }
+  const double c1 = 0.1, c2 = 0.6, c3 = 0.3, eps = P.eps;
+  double w1, w2, w3;
+  const long long o = (long long)v * P.pis + q;
+  // left-biased: (m3..p2) = cells i-3..i+1 ; right-biased: cells i+2..i-2
+  if (P.no_limiting) { w1 = c1; w2 = c2; w3 = c3; }
+  else weno_weights(P.weno_type, c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
+  uL[o] = weno5_value(w1, w2, w3, a[0], a[1], a[2], a[3], a[4]);
+  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, w1, w2, w3);
+  uR[o] = weno5_value(w1, w2, w3, a[5], a[4], a[3], a[2], a[1]);
+  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, w1, w2, w3);
+  fL[o] = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
+  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
+  fR[o] = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
+}
+
+// ================================================================== CRWENO5
+// Interp1PrimFifthOrderCRWENO (Interp1PrimFifthOrderCRWENO.c:81-240) with the
+// tridiagonal solve of tridiagLU (tridiagLU.c:86-277) replaced by a
+// partitioned solve in the spirit of tridiagLU's own substructuring (its
+// stages 1-4 with "ranks" = threads): one CTA per line, each thread owns M
+// consecutive rows in registers.  The first row of each chunk is a separator;
+// the chunk's other rows are eliminated down and up so that each is
+// x_i = rho_i - alpha_i X_k - gamma_i X_{k+1} in the separators X.  The
+// separator equations form a tridiagonal system with one unknown per thread,
+// solved by parallel cyclic reduction in shared memory; then every row is
+// recovered from its two separators.
+//
+// Rows 0 and N are the WENO5 rows with B = 1 (physical boundaries, also on
+// periodic domains, :164-175); they are solved directly and folded into rows 1
+// and N-1.  Rows past N-1 are identity rows.
+__device__ __forceinline__ void crweno_row(const DevParams& P, const double* fv, int r, int upw,
+                                           double& A, double& B, double& C, double& R) {
+  double m3, m2, m1, p1, p2;
+  if (upw > 0) { m3 = fv[r]; m2 = fv[r + 1]; m1 = fv[r + 2]; p1 = fv[r + 3]; p2 = fv[r + 4]; }
+  else         { m3 = fv[r + 5]; m2 = fv[r + 4]; m1 = fv[r + 3]; p1 = fv[r + 2]; p2 = fv[r + 1]; }
+  double w1, w2, w3;
+  if (P.no_limiting) { w1 = 0.2; w2 = 0.5; w3 = 0.3; }
+  else weno_weights(P.weno_type, 0.2, 0.5, 0.3, m3, m2, m1, p1, p2, P.eps, w1, w2, w3);
+  const double s6 = 1.0 / 6.0, t3 = 1.0 / 3.0;
+  double f1 = s6 * m2 + (5.0 * s6) * m1;
+  double f2 = (5.0 * s6) * m1 + s6 * p1;
+  double f3 = s6 * m1 + (5.0 * s6) * p1;
+  double lo = (2.0 * t3) * w1 + t3 * w2, hi = t3 * w3;
+  B = t3 * w1 + (2.0 * t3) * w2 + (2.0 * t3) * w3;
+  if (upw > 0) { A = lo; C = hi; } else { C = lo; A = hi; }
+  R = w1 * f1 + w2 * f2 + w3 * f3;
+}
+
+// WENO5 boundary row value at interface i (WENO optimal weights)
+__device__ __forceinline__ double crweno_edge(const DevParams& P, const double* src, long long st, int i, int upw) {
+  double m3, m2, m1, p1, p2;
+  if (upw > 0) { m3 = src[(i - 3) * st]; m2 = src[(i - 2) * st]; m1 = src[(i - 1) * st]; p1 = src[i * st]; p2 = src[(i + 1) * st]; }
+  else         { m3 = src[(i + 2) * st]; m2 = src[(i + 1) * st]; m1 = src[i * st]; p1 = src[(i - 1) * st]; p2 = src[(i - 2) * st]; }
+  double w1, w2, w3;
+  if (P.no_limiting) { w1 = 0.1; w2 = 0.6; w3 = 0.3; }
+  else weno_weights(P.weno_type, 0.1, 0.6, 0.3, m3, m2, m1, p1, p2, P.eps, w1, w2, w3);
+  return weno5_value(w1, w2, w3, m3, m2, m1, p1, p2);
+}
+
+template <int M, int DIR>
+__global__ void __launch_bounds__(256) k_crweno_line(DevParams P, const double* __restrict__ U,
+                                                      const double* __restrict__ F, double* __restrict__ uL,
+                                                      double* __restrict__ uR, double* __restrict__ fL,
+                                                      double* __restrict__ fR, int lines_per_block,
+                                                      int* __restrict__ err) {
+  static_assert(M >= 2, "a chunk needs a separator and at least one interior row");
+  extern __shared__ double sm[];
+  const int Pt = blockDim.x, k = threadIdx.x;
+  double* pa = sm;            // PCR buffers [2][4][Pt]
+  double* tp = sm + 8 * Pt;   // last-row spikes published per chunk [3][Pt]
+  double* sy = sm + 11 * Pt;  // separator values [Pt]
+  const int v = blockIdx.y;
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const int nlines = DIR == 0 ? P.N1 : P.N0;
+  const long long st = DIR == 0 ? 1 : P.W0;
+  const long long ist = DIR == 0 ? 1 : P.N0;
+  const int s = 1 + k * M;                       // separator row of this thread
+  const int kN = (N - 2) / M;                    // thread owning row N-1
+  for (int lc = 0; lc < lines_per_block; lc++) {
+    const int line = blockIdx.x * lines_per_block + lc;
+    if (line >= nlines) break;
+    const long long base = DIR == 0 ? pidx(P, 0, line) : pidx(P, line, 0);
+    const long long ibase = DIR == 0 ? (long long)(P.N0 + 1) * line : line;
+    for (int sys = 0; sys < 4; sys++) {
+      const int upw = (sys & 1) ? -1 : 1;
+      const double* src = (sys < 2 ? U : F) + (long long)v * P.ps + base;
+      double* out = (sys == 0 ? uL : sys == 1 ? uR : sys == 2 ? fL : fR) + (long long)v * P.pis + ibase;
+      double fv[M + 5];
+#pragma unroll
+      for (int r = 0; r < M + 5; r++) {
+        const int c = s - 3 + r;
+        fv[r] = (c <= N + 2) ? src[c * st] : 0.0;
+      }
+      double x0 = 0.0, xN = 0.0;
+      if (k == 0) x0 = crweno_edge(P, src, st, 0, upw);
+      if (k == kN) xN = crweno_edge(P, src, st, N, upw);
+      // ---- rows; the separator row r = 0 is kept as built
+      double As = 0.0, Bs = 1.0, Cs = 0.0, Rs = 0.0;
+      double al[M], be[M], cc[M], rh[M], rb[M];
+      int bad = 0;
+#pragma unroll
+      for (int r = 0; r < M; r++) {
+        const int i = s + r;
+        double A = 0.0, B = 1.0, C = 0.0, R = 0.0;
+        if (i <= N - 1) {
+          crweno_row(P, fv, r, upw, A, B, C, R);
+          if (i == 1) { R -= A * x0; A = 0.0; }
+          if (i == N - 1) { R -= C * xN; C = 0.0; }
+        }
+        if (r == 0) { As = A; Bs = B; Cs = C; Rs = R; continue; }
+        // downward elimination of the interior rows, spike on the separator X_k
+        if (r == 1) { al[1] = A; be[1] = B; rh[1] = R; }
+        else {
+          const double f = A * rb[r - 1];
+          be[r] = B - f * cc[r - 1];
+          al[r] = -f * al[r - 1];
+          rh[r] = R - f * rh[r - 1];
+        }
+        cc[r] = C;
+        bad |= (be[r] == 0.0);
+        rb[r] = 1.0 / be[r];
+      }
+      // ---- upward elimination, normalised: x_{s+r} = rh - al X_k - cc X_{k+1}
+      al[M - 1] *= rb[M - 1]; rh[M - 1] *= rb[M - 1]; cc[M - 1] *= rb[M - 1];
+#pragma unroll
+      for (int r = M - 2; r >= 1; r--) {
+        const double c = cc[r];
+        al[r] = (al[r] - c * al[r + 1]) * rb[r];
+        rh[r] = (rh[r] - c * rh[r + 1]) * rb[r];
+        cc[r] = -(c * cc[r + 1]) * rb[r];
+      }
+      if (bad) atomicOr(err, 1);
+      tp[k] = al[M - 1]; tp[Pt + k] = cc[M - 1]; tp[2 * Pt + k] = rh[M - 1];
+      __syncthreads();
+      // ---- separator equation: As x_{s-1} + Bs X_k + Cs x_{s+1} = Rs with
+      //      x_{s-1} = rho_p - alpha_p X_{k-1} - gamma_p X_k (previous chunk's
+      //      last row) and x_{s+1} = rh[1] - al[1] X_k - cc[1] X_{k+1}
+      double alp = 0.0, gap = 0.0, rhp = 0.0;
+      if (k > 0) { alp = tp[k - 1]; gap = tp[Pt + k - 1]; rhp = tp[2 * Pt + k - 1]; }
+      {
+        double a = -(As * alp);
+        double b = Bs - As * gap - Cs * al[1];
+        double c = -(Cs * cc[1]);
+        double d = Rs - As * rhp - Cs * rh[1];
+        int buf = 0;
+        pa[k] = a; pa[Pt + k] = b; pa[2 * Pt + k] = c; pa[3 * Pt + k] = d;
+        __syncthreads();
+        for (int dl = 1; dl < Pt; dl <<= 1) {
+          const double* cur = pa + buf * 4 * Pt;
+          double* nxt = pa + (buf ^ 1) * 4 * Pt;
+          double am = 0.0, bm = 1.0, cm = 0.0, dm = 0.0, ap = 0.0, bp = 1.0, cp = 0.0, dp = 0.0;
+          if (k - dl >= 0) { am = cur[k - dl]; bm = cur[Pt + k - dl]; cm = cur[2 * Pt + k - dl]; dm = cur[3 * Pt + k - dl]; }
+          if (k + dl < Pt) { ap = cur[k + dl]; bp = cur[Pt + k + dl]; cp = cur[2 * Pt + k + dl]; dp = cur[3 * Pt + k + dl]; }
+          const double alpha = -a / bm, gamma = -c / bp;
+          a = alpha * am;
+          c = gamma * cp;
+          b = b + alpha * cm + gamma * ap;
+          d = d + alpha * dm + gamma * dp;
+          nxt[k] = a; nxt[Pt + k] = b; nxt[2 * Pt + k] = c; nxt[3 * Pt + k] = d;
+          buf ^= 1;
+          __syncthreads();
+        }
+        sy[k] = d / b;
+      }
+      __syncthreads();
+      // ---- recover every row
+      const double Xk = sy[k];
+      const double Xn = k + 1 < Pt ? sy[k + 1] : 0.0;
+      if (s <= N - 1) out[s * ist] = Xk;
+#pragma unroll
+      for (int r = 1; r < M; r++) {
+        const int i = s + r;
+        if (i <= N - 1) out[i * ist] = rh[r] - al[r] * Xk - cc[r] * Xn;
+      }
+      if (k == 0) out[0] = x0;
+      if (k == kN) out[(long long)N * ist] = xN;
+      __syncthreads();   // shared buffers are reused by the next system
+    }
+  }
+}
+
+// ============================================================ upwind + div
+// Upwind (NavierStokes2DUpwind*/Euler1DUpwind*) at the interfaces of a tile,
+// then hyp += dxinv (fI[j+1] - fI[j]) (HyperbolicFunction.c:97-112) and the
+// stage derivative rhs = -hyp (TimeRHSFunctionExplicit.c:64-66).
+// mode 0: rhs = -hyp_x (first direction); 1: rhs <- -((-rhs) + hyp_y);
+// mode 2: out = hyp_x; 3: out <- out + hyp_y (the hyperbolic term alone).
+// Tile: DIR 0: 128 cells of one row; DIR 1: 32 columns x 8 rows.
+template <int MODEL, int UPW, int DIR>
+__global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* __restrict__ U,
+                                                    const double* __restrict__ uL, const double* __restrict__ uR,
+                                                    const double* __restrict__ fL, const double* __restrict__ fR,
+                                                    const double* __restrict__ dxinv, double* __restrict__ rhs,
+                                                    int mode) {
+  extern __shared__ double sfi[];
+  constexpr int NF = Flow<MODEL>::NF;
+  const int TX = DIR == 0 ? 128 : 32, TY = DIR == 0 ? 1 : 8;
+  const int TL = DIR == 0 ? TX : TY;             // cells along the line in the tile
+  const int TW = DIR == 0 ? 1 : TX;              // lines in the tile
+  const int nvars = P.nvars;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const int nl = DIR == 0 ? P.N1 : P.N0;
+  // tile origin
+  const int i0 = DIR == 0 ? blockIdx.x * TX : blockIdx.y * TY;     // along the line
+  const int l0 = DIR == 0 ? blockIdx.y : blockIdx.x * TX;          // first line
+  const double g = P.gamma;
+  // interfaces i0 .. i0+TL for lines l0 .. l0+TW-1
+  const int nIf = (TL + 1) * TW;
+  const int tid = tx + TX * ty, nth = TX * TY;
+  for (int e = tid; e < nIf; e += nth) {
+    int li, ii;
+    if (DIR == 0) { ii = e; li = 0; } else { li = e % TW; ii = e / TW; }
+    const int i = i0 + ii, l = l0 + li;
+    if (i > N || l >= nl) continue;
+    const long long q = DIR == 0 ? (long long)i + (long long)(P.N0 + 1) * l : (long long)l + (long long)P.N0 * i;
+    const long long pL = cell_of<DIR>(P, i - 1, l), pR = cell_of<DIR>(P, i, l);
+    double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
+    int spm;
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
+      c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
+      if (UPW != UPW_LLF || MODEL == EULER1D) { ucl[m] = U[m * P.ps + pL]; ucr[m] = U[m * P.ps + pR]; }
+    }
+    upwind_flow<MODEL, UPW, double>(a, b, c, d, ucl, ucr, g, DIR, fi, &spa, &spm);
+    double* so = sfi + (long long)(ii * TW + li);
+    const int vs = (TL + 1) * TW;
+#pragma unroll
+    for (int m = 0; m < NF; m++) so[m * vs] = fi[m];
+    for (int m = NF; m < nvars; m++)
+      so[m * vs] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q], fR[m * P.pis + q]);
+  }
+  __syncthreads();
+  // divergence for the tile's cells
+  int ii, li;
+  if (DIR == 0) { ii = tx; li = 0; } else { li = tx; ii = ty; }
+  const int i = i0 + ii, l = l0 + li;
+  if (i >= N || l >= nl) return;
+  const long long p = cell_of<DIR>(P, i, l);
+  const int off = DIR == 0 ? 0 : P.W0;
+  const double dxi = dxinv[off + P.ghosts + i];
+  const int vs = (TL + 1) * TW;
+  for (int m = 0; m < nvars; m++) {
+    const double h = dxi * (sfi[m * vs + (ii + 1) * TW + li] - sfi[m * vs + ii * TW + li]);
+    double* r = rhs + (long long)m * P.ps + p;
+    if (mode == 0) *r = -h;
+    else if (mode == 1) *r = -((-*r) + h);
+    else if (mode == 2) *r = h;
+    else *r = *r + h;
+  }
+}
+
+// ===================================================== viscous + chemistry
+// NavierStokes2DParabolicFunction (NavierStokes2DParabolicFunction.c:41-204)
+// with FirstDerivativeFirstOrder (bias +1 on Q, -1 on the fluxes), fused with
+// SourceFunction -> ChemistrySource (ChemistrySolve.c:18-115) and the RHS
+// accumulation rhs += par; rhs += source (TimeRHSFunctionExplicit.c:67-74).
+// Tile: 32 x 8 interior points.  Cross-derivative terms at ghost columns/rows
+// are zero, as the reference computes derivatives on interior lines only.
+__device__ __forceinline__ void visc_coeffs(const DevParams& P, double T, double& mu, double& kappa) {
+  const double Td = T * P.Tref;
+  const double r15 = exp(1.5 * log(Td / P.T0));   // raiseto (math_ops.h:40)
+  mu = r15 * (P.T0 + P.TS) / (Td + P.TS);
+  kappa = r15 * (P.T0 + P.TA * exp(-P.TB / P.T0)) / (Td + P.TA * exp(-P.TB / Td));
+}
+
+__device__ void chem_source_point(const DevParams& P, const double* __restrict__ U, long long p,
+                                  double hnu_factor, double imap_p, double* __restrict__ rhs) {
+  // ChemistrySetPhotonDensity (ChemistrySolve.c:18-65) + _ChemistrySetRHS_/_ChemistrySetQ_
+  // (chemistry.h:30-137); the energy slot takes the heating of the last layer.
+  const long long ps = P.ps;
+  double n_hnu = hnu_factor * imap_p / (P.ch_c * P.ch_h * P.ch_nu * P.n_O2);
+  const double k0a = P.k[0], k0b = P.k[1], k1a = P.k[2], k1b = P.k[3], k2a = P.k[4], k2b = P.k[5];
+  const double k3a = P.k[6], k3b = P.k[7], k4 = P.k[8], k5 = P.k[9], k6 = P.k[10];
+  double Q = 0.0;
+  for (int iz = 0; iz < P.nz; iz++) {
+    if (iz > 0) {
+      const double damp = 1.0 - P.dz * (P.sO3 * P.n_O2) * U[(P.nflow + P.zstride * (iz - 1) + 1) * ps + p];
+      n_hnu = n_hnu * damp;
+    }
+    const int nfv = P.nflow + P.zstride * iz;
+    const double nO2 = U[(nfv + 0) * ps + p], nO3 = U[(nfv + 1) * ps + p], n1D = U[(nfv + 2) * ps + p];
+    const double n1Dg = U[(nfv + 3) * ps + p], n3Su = U[(nfv + 4) * ps + p], n1Sg = U[(nfv + 5) * ps + p];
+    const double nCO2 = U[(nfv + 6) * ps + p];
+    const double sO3 = -(k0a + k0b) * n_hnu * nO3 - (k2a + k2b) * nO3 * n1D - (k3a + k3b) * nO3 * n1Sg
+                       - k5 * nO3 * n3Su - k6 * n1Dg * nO3;
+    const double s1D = k0a * n_hnu * nO3 - (k1a + k1b) * n1D * nO2 - (k2a + k2b) * n1D * nO3 - k4 * n1D * nCO2;
+    const double s1Dg = k0a * n_hnu * nO3 + k5 * nO3 * n3Su - k6 * n1Dg * nO3;
+    const double s3Su = k2a * nO3 * n1D - k5 * nO3 * n3Su;
+    const double s1Sg = k1a * n1D * nO2 - (k3a + k3b) * nO3 * n1Sg;
+    rhs[(nfv + 1) * ps + p] += sO3;
+    rhs[(nfv + 2) * ps + p] += s1D;
+    rhs[(nfv + 3) * ps + p] += s1Dg;
+    rhs[(nfv + 4) * ps + p] += s3Su;
+    rhs[(nfv + 5) * ps + p] += s1Sg;
+    Q = ((P.q[0] * k0a + P.q[1] * k0b) * n_hnu * nO3 + (P.q[2] * k1a + P.q[3] * k1b) * nO2 * n1D
+         + (P.q[4] * k2a + P.q[5] * k2b) * nO3 * n1D + (P.q[6] * k3a + P.q[7] * k3b) * nO3 * n1Sg
+         + P.q[8] * k4 * n1D * nCO2 + P.q[9] * k5 * nO3 * n3Su + P.q[10] * k6 * n1Dg * nO3)
+        / (P.chem_gamma - 1.0);
+  }
+  rhs[(P.nflow - 1) * ps + p] += Q;
+}
+
+// pulse factor I0 exp(-(t - (t_start+t_pulse))^2 / (2 sigma^2)) or 0 before t_start
+__device__ __forceinline__ double pulse_factor(const DevParams& P, double t) {
+  if (!(t > P.t_start_norm)) return 0.0;
+  const double sigma = P.t_pulse_norm / 2.35482;
+  const double tp = t - (P.t_start_norm + P.t_pulse_norm);
+  return P.I0 * exp(-(tp * tp) / (2 * sigma * sigma));
+}
+
+__global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* __restrict__ U,
+                                                     const double* __restrict__ dxinv,
+                                                     const double* __restrict__ imap,
+                                                     const double* __restrict__ tdev, double cstage,
+                                                     double* __restrict__ rhs, int do_chem) {
+  constexpr int BX = 32, BY = 8, QX = BX + 2, QY = BY + 2, FX = BX + 1, FY = BY + 1;
+  __shared__ double su[QY][QX], sv[QY][QX], sT[QY][QX];
+  __shared__ double fx[3][BY][FX];   // FVx at i in [i0-1, i0+BX), rows j0..j0+BY-1
+  __shared__ double fy[3][FY][BX];   // FVy at j in [j0-1, j0+BY), cols i0..i0+BX-1
+  const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+  const int tid = threadIdx.x + BX * threadIdx.y;
+  const long long ps = P.ps;
+  if (P.viscous) {
+    // Q = (u, v, T = gamma p / rho) on [i0-1, i0+BX] x [j0-1, j0+BY]
+    for (int e = tid; e < QX * QY; e += BX * BY) {
+      const int a = e % QX, b = e / QX;
+      const int i = i0 - 1 + a, j = j0 - 1 + b;
+      double uu = 0.0, vv = 0.0, TT = 0.0;
+      if (i >= -P.ghosts && i < P.N0 + P.ghosts && j >= -P.ghosts && j < P.N1 + P.ghosts) {
+        const long long p = pidx(P, i, j);
+        double rho, e_, pr;
+        ns_flowvar(U[p], U[ps + p], U[2 * ps + p], U[3 * ps + p], P.gamma, rho, uu, vv, e_, pr);
+        TT = P.gamma * pr / rho;
+      }
+      su[b][a] = uu; sv[b][a] = vv; sT[b][a] = TT;
+    }
+    __syncthreads();
+    const double two_third = 2.0 / 3.0, inv_Re = 1.0 / P.Re, inv_Pr = 1.0 / P.Pr;
+    const double igm1 = 1.0 / (P.gamma - 1.0);
+    // viscous fluxes on [i0-1, i0+BX) x [j0-1, j0+BY) (corner cell unused)
+    for (int e = tid; e < FX * FY; e += BX * BY) {
+      const int a = e % FX, b = e / FX;       // a: i - (i0-1), b: j - (j0-1)
+      const int i = i0 - 1 + a, j = j0 - 1 + b;
+      const bool need_x = (b >= 1) && (j < P.N1) && (i < P.N0);   // FVx at interior rows
+      const bool need_y = (a >= 1) && (i < P.N0) && (j < P.N1);   // FVy at interior columns
+      if (!need_x && !need_y) continue;
+      const int qa = a, qb = b;               // (i, j) in the Q tile
+      const double dxi = dxinv[P.ghosts + i], dyi = dxinv[P.W0 + P.ghosts + j];
+      const bool row_int = (j >= 0 && j < P.N1), col_int = (i >= 0 && i < P.N0);
+      const double uc = su[qb][qa], vc = sv[qb][qa], Tc = sT[qb][qa];
+      // first differences (QDerivX only on interior rows, QDerivY only on interior columns)
+      const double ux = row_int ? dxi * (su[qb][qa + 1] - uc) : 0.0;
+      const double vx = row_int ? dxi * (sv[qb][qa + 1] - vc) : 0.0;
+      const double Tx = row_int ? dxi * (sT[qb][qa + 1] - Tc) : 0.0;
+      const double uy = col_int ? dyi * (su[qb + 1][qa] - uc) : 0.0;
+      const double vy = col_int ? dyi * (sv[qb + 1][qa] - vc) : 0.0;
+      const double Ty = col_int ? dyi * (sT[qb + 1][qa] - Tc) : 0.0;
+      double mu, kappa;
+      visc_coeffs(P, Tc, mu, kappa);
+      const double mre = mu * inv_Re, kre = kappa * inv_Re * igm1 * inv_Pr;
+      if (need_x) {
+        const double txx = two_third * mre * (2 * ux - vy), txy = mre * (uy + vx);
+        fx[0][b - 1][a] = txx; fx[1][b - 1][a] = txy; fx[2][b - 1][a] = uc * txx + vc * txy + kre * Tx;
+      }
+      if (need_y) {
+        const double tyx = mre * (uy + vx), tyy = two_third * mre * (-ux + 2 * vy);
+        fy[0][b][a - 1] = tyx; fy[1][b][a - 1] = tyy; fy[2][b][a - 1] = uc * tyx + vc * tyy + kre * Ty;
+      }
+    }
+    __syncthreads();
+  }
+  const int a = threadIdx.x, b = threadIdx.y;
+  const int i = i0 + a, j = j0 + b;
+  if (i >= P.N0 || j >= P.N1) return;
+  const long long p = pidx(P, i, j);
+  if (P.viscous) {
+    const double dxi = dxinv[P.ghosts + i], dyi = dxinv[P.W0 + P.ghosts + j];
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+      const double par = dxi * (fx[m][b][a + 1] - fx[m][b][a]) + dyi * (fy[m][b + 1][a] - fy[m][b][a]);
+      rhs[(m + 1) * ps + p] += par;
+    }
+  }
+  if (do_chem) {
+    const double t = *tdev + cstage * P.dt;
+    chem_source_point(P, U, p, pulse_factor(P, t), imap[p], rhs);
+  }
+}
+
+// chemistry source alone (1D, or 2D without viscosity)
+__global__ void k_source(DevParams P, const double* __restrict__ U, const double* __restrict__ imap,
+                         const double* __restrict__ tdev, double cstage, double* __restrict__ rhs) {
+  long long n = (long long)P.N0 * P.N1;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  int i = (int)(idx % P.N0), j = (int)(idx / P.N0);
+  long long p = pidx(P, i, j);
+  const double t = *tdev + cstage * P.dt;
+  chem_source_point(P, U, p, pulse_factor(P, t), imap[p], rhs);
+}
+
+__global__ void k_advance_time(double* tdev, double dt) { *tdev += dt; }
+
+// =================================================================== batched
+// tridiagLU with the reference's [row * ns + sys] layout: one thread per
+// system, serial Thomas (tridiagLU.c:133-153, 242-262).  Operator-level entry
+// point for parity tests; the fused CRWENO path does not use it.
+__global__ void k_tridiag_serial(double* a, double* b, double* c, double* x, int n, int ns, int* err) {
+  int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= ns) return;
+  int bad = 0;
+  for (int i = 1; i < n; i++) {
+    double bm = b[(long long)(i - 1) * ns + d];
+    if (bm == 0.0) { bad = 1; break; }
+    double f = a[(long long)i * ns + d] / bm;
+    b[(long long)i * ns + d] -= f * c[(long long)(i - 1) * ns + d];
+    a[(long long)i * ns + d] = -f * a[(long long)(i - 1) * ns + d];
+    x[(long long)i * ns + d] -= f * x[(long long)(i - 1) * ns + d];
+  }
+  if (!bad) {
+    const double x0 = x[d];
+    long long e = (long long)(n - 1) * ns + d;
+    if (b[e] == 0.0) bad = 1;
+    else x[e] = (x[e] - a[e] * x0) / b[e];
+    for (int i = n - 2; i >= 0 && !bad; i--) {
+      long long r = (long long)i * ns + d;
+      if (b[r] == 0.0) { bad = 1; break; }
+      x[r] = (x[r] - c[r] * x[r + ns] - a[r] * (i == 0 ? x[r] : x0)) / b[r];
+    }
+  }
+  if (bad) atomicOr(err, 1);
+}
+
+
+// ======================================================= operator-level only
+// Upwind at every interface of direction DIR into an interface array (SoA);
+// the fused path uses k_upwind_div instead.
+template <int MODEL, int UPW, int DIR>
+__global__ void k_upwind_iface(DevParams P, const double* __restrict__ U, const double* __restrict__ uL,
+                               const double* __restrict__ uR, const double* __restrict__ fL,
+                               const double* __restrict__ fR, double* __restrict__ fI) {
+  constexpr int NF = Flow<MODEL>::NF;
+  long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= P.nint[DIR]) return;
+  int i, l;
+  iface_decode<DIR>(P, q, i, l);
+  const long long pL = cell_of<DIR>(P, i - 1, l), pR = cell_of<DIR>(P, i, l);
+  double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
+  int spm;
+  for (int m = 0; m < NF; m++) {
+    a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q]; c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
+    ucl[m] = U[m * P.ps + pL]; ucr[m] = U[m * P.ps + pR];
+  }
+  upwind_flow<MODEL, UPW, double>(a, b, c, d, ucl, ucr, P.gamma, DIR, fi, &spa, &spm);
+  for (int m = 0; m < NF; m++) fI[m * P.pis + q] = fi[m];
+  for (int m = NF; m < P.nvars; m++)
+    fI[m * P.pis + q] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q], fR[m * P.pis + q]);
+}
+
+// FirstDerivativeFirstOrder (FirstDerivativeFirstOrder.c:40-100) on an AoS
+// array with nv values per point: lines along dir that are interior in the
+// other dimension, one-sided at the two extreme ghost points.
+__global__ void k_first_deriv(DevParams P, double* __restrict__ Df, const double* __restrict__ f, int dir,
+                              int bias, int nv) {
+  const int N = dir == 0 ? P.N0 : P.N1, nl = P.ndims == 1 ? 1 : (dir == 0 ? P.N1 : P.N0);
+  const int len = N + 2 * P.ghosts;
+  long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= (long long)len * nl) return;
+  int ii = (int)(idx % len) - P.ghosts, l = (int)(idx / len);
+  auto at = [&](int i) -> long long { return dir == 0 ? pidx(P, i, l) : pidx(P, l, i); };
+  const int mx = bias > 0 ? bias : 0, mn = bias < 0 ? bias : 0;
+  for (int v = 0; v < nv; v++) {
+    double r;
+    if (ii == -P.ghosts) r = f[at(ii + 1) * nv + v] - f[at(ii) * nv + v];
+    else if (ii == N + P.ghosts - 1) r = f[at(ii) * nv + v] - f[at(ii - 1) * nv + v];
+    else r = mx * f[at(ii + 1) * nv + v] - bias * f[at(ii) * nv + v] + mn * f[at(ii - 1) * nv + v];
+    Df[at(ii) * nv + v] = r;
+  }
+}
+
+// ================================================================ launchers
+static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+void launch_aos_to_soa(const double* aos, double* soa, long long npg, int nv, long long ps, cudaStream_t s) {
+  k_aos_to_soa<<<nblk(npg * nv, 256), 256, 0, s>>>(aos, soa, npg, nv, ps);
+}
+void launch_soa_to_aos(const double* soa, double* aos, long long npg, int nv, long long ps, cudaStream_t s) {
+  k_soa_to_aos<<<nblk(npg * nv, 256), 256, 0, s>>>(soa, aos, npg, nv, ps);
+}
+void launch_soa_to_interior(const DevParams& P, const double* soa, double* out, cudaStream_t s) {
+  k_soa_to_interior<<<nblk((long long)P.N0 * P.N1 * P.nvars, 256), 256, 0, s>>>(P, soa, out);
+}
+void launch_interior_to_soa(const DevParams& P, const double* in, double* soa, cudaStream_t s) {
+  k_interior_to_soa<<<nblk((long long)P.N0 * P.N1 * P.nvars, 256), 256, 0, s>>>(P, in, soa);
+}
+void launch_iface_aos_to_soa(const double* aos, double* soa, long long ni, int nv, long long pis, cudaStream_t s) {
+  k_iface_aos_to_soa<<<nblk(ni * nv, 256), 256, 0, s>>>(aos, soa, ni, nv, pis);
+}
+void launch_iface_soa_to_aos(const double* soa, double* aos, long long ni, int nv, long long pis, cudaStream_t s) {
+  k_iface_soa_to_aos<<<nblk(ni * nv, 256), 256, 0, s>>>(soa, aos, ni, nv, pis);
+}
+void launch_bc(const DevParams& P, double* u, const Zone& z, cudaStream_t s) {
+  long long n = (long long)(z.ie[0] - z.is[0]) * (z.ie[1] - z.is[1]);
+  if (n <= 0) return;
+  k_bc_zone<<<nblk(n, 128), 128, 0, s>>>(P, u, z);
+}
+void launch_stage(long long n, double* Us, const double* u, const double* const* d, const double* a, int nterms,
+                  cudaStream_t s) {
+  k_stage<<<nblk(n, 256), 256, 0, s>>>(n, Us, u, nterms > 0 ? d[0] : nullptr, nterms > 0 ? a[0] : 0.0,
+                                        nterms > 1 ? d[1] : nullptr, nterms > 1 ? a[1] : 0.0,
+                                        nterms > 2 ? d[2] : nullptr, nterms > 2 ? a[2] : 0.0, nterms);
+}
+void launch_update(const DevParams& P, double* u, const double* const* d, const double* b, int ns, double* norm_acc,
+                   cudaStream_t s) {
+  long long n = (long long)P.nvars * P.ps;
+  k_update<<<nblk(n, 256), 256, 0, s>>>(P, u, d[0], b[0], ns > 1 ? d[1] : nullptr, ns > 1 ? b[1] : 0.0,
+                                         ns > 2 ? d[2] : nullptr, ns > 2 ? b[2] : 0.0, ns > 3 ? d[3] : nullptr,
+                                         ns > 3 ? b[3] : 0.0, ns, norm_acc);
+}
+void launch_cfl(const DevParams& P, const double* u, const double* dxinv, unsigned long long* out, cudaStream_t s) {
+  k_cfl<<<nblk((long long)P.N0 * P.N1, 256), 256, 0, s>>>(P, u, dxinv, out);
+}
+void launch_flux(const DevParams& P, const double* U, double* F, int dir, cudaStream_t s) {
+  unsigned nb = nblk(P.npg, 256);
+  if (P.model == NS2D) {
+    if (dir == 0) k_flux<NS2D, 0><<<nb, 256, 0, s>>>(P, U, F);
+    else k_flux<NS2D, 1><<<nb, 256, 0, s>>>(P, U, F);
+  } else {
+    k_flux<EULER1D, 0><<<nb, 256, 0, s>>>(P, U, F);
+  }
+}
+void launch_weno5(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                  double* fR, int dir, cudaStream_t s) {
+  long long n = P.nint[dir] * P.nvars;
+  if (dir == 0) k_weno5<0><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
+  else k_weno5<1><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
+}
+
+// rows per thread of the partitioned line solve: the smallest M that keeps a
+// line within one 256-thread CTA (lines of up to 4097 interfaces)
+int crweno_rows_per_thread(int N) {
+  const int rows = N - 1;
+  const int cand[4] = {2, 4, 8, 16};
+  for (int c = 0; c < 4; c++)
+    if ((rows + cand[c] - 1) / cand[c] <= 256) return cand[c];
+  return -1;
+}
+
+template <int M>
+static void crweno_launch_m(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                            double* fR, int dir, int* err, cudaStream_t s) {
+  const int N = dir == 0 ? P.N0 : P.N1;
+  const int nlines = dir == 0 ? P.N1 : P.N0;
+  int Pt = (N - 1 + M - 1) / M;
+  Pt = ((Pt + 31) / 32) * 32;
+  const int lpb = dir == 0 ? 1 : 4;
+  dim3 grid((nlines + lpb - 1) / lpb, P.nvars);
+  size_t smem = (size_t)12 * Pt * sizeof(double);
+  if (dir == 0) k_crweno_line<M, 0><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, lpb, err);
+  else k_crweno_line<M, 1><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, lpb, err);
+}
+
+int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                  double* fR, int dir, int* err, cudaStream_t s) {
+  const int N = dir == 0 ? P.N0 : P.N1;
+  const int M = crweno_rows_per_thread(N);
+  switch (M) {
+    case 2: crweno_launch_m<2>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    case 4: crweno_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    case 8: crweno_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    case 16: crweno_launch_m<16>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    default: return -1;
+  }
+  return 0;
+}
+
+template <int MODEL, int UPW>
+static void upwind_div_dir(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                           const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
+  // the interface-flux tile holds nvars x (tile + 1) doubles: allow more than
+  // the 48 KB default for many-species decks
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_upwind_div<MODEL, UPW, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_upwind_div<MODEL, UPW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  if (dir == 0) {
+    dim3 grid(nblk(P.N0, 128), P.N1), blk(128, 1);
+    size_t smem = (size_t)P.nvars * 129 * sizeof(double);
+    k_upwind_div<MODEL, UPW, 0><<<grid, blk, smem, s>>>(P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+  } else {
+    dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
+    size_t smem = (size_t)P.nvars * 9 * 32 * sizeof(double);
+    k_upwind_div<MODEL, UPW, 1><<<grid, blk, smem, s>>>(P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+  }
+}
+
+template <int MODEL>
+static void upwind_div_model(const DevParams& P, const double* U, const double* uL, const double* uR,
+                             const double* fL, const double* fR, const double* dxinv, double* rhs, int dir,
+                             int mode, cudaStream_t s) {
+  switch (P.upwind) {
+    case UPW_ROE: upwind_div_dir<MODEL, UPW_ROE>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s); break;
+    case UPW_RF: upwind_div_dir<MODEL, UPW_RF>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s); break;
+    case UPW_LLF: upwind_div_dir<MODEL, UPW_LLF>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s); break;
+    default: upwind_div_dir<MODEL, UPW_RUSANOV>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s); break;
+  }
+}
+
+void launch_upwind_div(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                       const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
+  if (P.model == NS2D) upwind_div_model<NS2D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
+  else upwind_div_model<EULER1D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
+}
+
+void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
+                        const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s) {
+  do_visc = do_visc && P.ndims == 2 && P.viscous;
+  do_chem = do_chem && P.chem;
+  if (do_visc) {
+    dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
+    k_visc_source<<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem);
+  } else if (do_chem) {
+    k_source<<<nblk((long long)P.N0 * P.N1, 256), 256, 0, s>>>(P, U, imap, tdev, cstage, rhs);
+  }
+}
+
+void launch_advance_time(double* tdev, double dt, cudaStream_t s) { k_advance_time<<<1, 1, 0, s>>>(tdev, dt); }
+
+template <int MODEL, int UPW>
+static void upwind_iface_m(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                           const double* fR, double* fI, int dir, cudaStream_t s) {
+  unsigned nb = nblk(P.nint[dir], 128);
+  if (dir == 0) k_upwind_iface<MODEL, UPW, 0><<<nb, 128, 0, s>>>(P, U, uL, uR, fL, fR, fI);
+  else k_upwind_iface<MODEL, UPW, 1><<<nb, 128, 0, s>>>(P, U, uL, uR, fL, fR, fI);
+}
+template <int MODEL>
+static void upwind_iface_u(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                           const double* fR, double* fI, int dir, cudaStream_t s) {
+  switch (P.upwind) {
+    case UPW_ROE: upwind_iface_m<MODEL, UPW_ROE>(P, U, uL, uR, fL, fR, fI, dir, s); break;
+    case UPW_RF: upwind_iface_m<MODEL, UPW_RF>(P, U, uL, uR, fL, fR, fI, dir, s); break;
+    case UPW_LLF: upwind_iface_m<MODEL, UPW_LLF>(P, U, uL, uR, fL, fR, fI, dir, s); break;
+    default: upwind_iface_m<MODEL, UPW_RUSANOV>(P, U, uL, uR, fL, fR, fI, dir, s); break;
+  }
+}
+void launch_upwind_iface(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                         const double* fR, double* fI, int dir, cudaStream_t s) {
+  if (P.model == NS2D) upwind_iface_u<NS2D>(P, U, uL, uR, fL, fR, fI, dir, s);
+  else upwind_iface_u<EULER1D>(P, U, uL, uR, fL, fR, fI, dir, s);
+}
+void launch_first_deriv(const DevParams& P, double* Df, const double* f, int dir, int bias, int nv, cudaStream_t s) {
+  const int N = dir == 0 ? P.N0 : P.N1, nl = P.ndims == 1 ? 1 : (dir == 0 ? P.N1 : P.N0);
+  long long n = (long long)(N + 2 * P.ghosts) * nl;
+  k_first_deriv<<<nblk(n, 128), 128, 0, s>>>(P, Df, f, dir, bias, nv);
+}
+
+void launch_tridiag(double* a, double* b, double* c, double* x, int n, int ns, int* err, cudaStream_t s) {
+  k_tridiag_serial<<<nblk(ns, 128), 128, 0, s>>>(a, b, c, x, n, ns, err);
+}
+
+}  // namespace piafs

@@ -1,0 +1,47 @@
+// Launcher interface of the device kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace piafs {
+
+// One boundary zone with its index extents resolved (single rank):
+// [is[d], ie[d]) per dimension, ghost slab along `dim`
+// (InitializeBoundaries.c:296-378).
+struct Zone {
+  int type, dim, face;
+  int is[2], ie[2];
+  double vel[2];
+};
+
+void launch_aos_to_soa(const double* aos, double* soa, long long npg, int nv, long long ps, cudaStream_t s);
+void launch_soa_to_aos(const double* soa, double* aos, long long npg, int nv, long long ps, cudaStream_t s);
+void launch_soa_to_interior(const DevParams& P, const double* soa, double* out, cudaStream_t s);
+void launch_interior_to_soa(const DevParams& P, const double* in, double* soa, cudaStream_t s);
+void launch_iface_aos_to_soa(const double* aos, double* soa, long long ni, int nv, long long pis, cudaStream_t s);
+void launch_iface_soa_to_aos(const double* soa, double* aos, long long ni, int nv, long long pis, cudaStream_t s);
+void launch_bc(const DevParams& P, double* u, const Zone& z, cudaStream_t s);
+void launch_stage(long long n, double* Us, const double* u, const double* const* d, const double* a, int nterms,
+                  cudaStream_t s);
+void launch_update(const DevParams& P, double* u, const double* const* d, const double* b, int ns, double* norm_acc,
+                   cudaStream_t s);
+void launch_cfl(const DevParams& P, const double* u, const double* dxinv, unsigned long long* out, cudaStream_t s);
+void launch_flux(const DevParams& P, const double* U, double* F, int dir, cudaStream_t s);
+void launch_weno5(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                  double* fR, int dir, cudaStream_t s);
+int crweno_rows_per_thread(int N);
+int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                  double* fR, int dir, int* err, cudaStream_t s);
+// mode 0: rhs = -hyp_x; 1: rhs = -((-rhs) + hyp_y); 2: out = hyp_x; 3: out += hyp_y
+void launch_upwind_div(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                       const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s);
+// rhs += par (if do_visc) then rhs += source (if do_chem)
+void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
+                        const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s);
+void launch_upwind_iface(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
+                         const double* fR, double* fI, int dir, cudaStream_t s);
+void launch_first_deriv(const DevParams& P, double* Df, const double* f, int dir, int bias, int nv, cudaStream_t s);
+void launch_advance_time(double* tdev, double dt, cudaStream_t s);
+void launch_tridiag(double* a, double* b, double* c, double* x, int n, int ns, int* err, cudaStream_t s);
+
+}  // namespace piafs

@@ -1,0 +1,68 @@
+"""Regenerate the golden fixtures of tests/golden/ from the reference.
+
+Each fixture directory holds a complete input deck (written by
+piafs_b200.cases with fixed seeds) and ``ref_final.bin``, the final solution
+the reference CPU binary (serial build, oracle/_ref/PIAFS, compiled from the
+llnl/piafs sources by oracle/Makefile) writes for it.  Run from the repository
+root after ``make -C oracle``:
+
+    python tests/golden/make_golden.py
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from piafs_b200 import cases  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref", "PIAFS")
+DT2D = 0.4 / 2048   # CFL 0.4 at 2048^2 (sound speed 1 in the quiescent gas)
+
+CASES = {
+    # the 1D Euler workload itself (N=1024, WENO5, Roe, SSPRK3, 1000 steps)
+    "euler1d_weno5_roe_n1024": (cases.euler1d_density_wave, dict(N=1024, n_iter=1000, dt=1e-4)),
+    "euler1d_crweno5_rusanov_mapped_n200": (cases.euler1d_density_wave, dict(
+        N=200, n_iter=200, dt=1e-3, scheme="crweno5", upwinding="rusanov", weno={"mapped": 1})),
+    "euler1d_weno5_llf_yc_rk4_n128": (cases.euler1d_density_wave, dict(
+        N=128, n_iter=100, dt=2e-3, upwinding="llf-char", time_scheme_type="44", weno={"yc": 1})),
+    "euler1d_crweno5_rf_borges_n97": (cases.euler1d_density_wave, dict(
+        N=97, n_iter=60, dt=2e-3, amp=0.3, scheme="crweno5", upwinding="rf-char", weno={"borges": 1})),
+    # the 2D photochemical workload at small size (same dt as at 2048^2)
+    "ns2d_chem_crweno5_llf_64x48": (cases.ns2d_photochem_beam, dict(N=64, NY=48, n_iter=20, dt=DT2D)),
+    "ns2d_chem_weno5_llf_48x40": (cases.ns2d_photochem_beam, dict(N=48, NY=40, n_iter=20, dt=DT2D, scheme="weno5")),
+    "ns2d_chem_crweno5_rf_borges_32x32": (cases.ns2d_photochem_beam, dict(
+        N=32, NY=32, n_iter=15, dt=DT2D, upwinding="rf-char", weno={"borges": 1})),
+    "ns2d_chem3layer_crweno5_llf_24x20": (cases.ns2d_photochem_beam, dict(
+        N=24, NY=20, n_iter=10, dt=DT2D, extra_chem={"z_mm": 3.0, "nz": 20}, layers=3)),
+    "ns2d_shear_crweno5_llf_re200_48x40": (cases.ns2d_shear_layer, dict(N=48, NY=40, n_iter=30, dt=2e-3)),
+    "ns2d_shear_weno5_roe_re200_40x32": (cases.ns2d_shear_layer, dict(
+        N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", upwinding="roe")),
+    "ns2d_shear_crweno5_rusanov_inviscid_32x36": (cases.ns2d_shear_layer, dict(
+        N=32, NY=36, n_iter=30, dt=2e-3, upwinding="rusanov", Re=-1.0)),
+}
+
+KEEP = {"solver.inp", "boundary.inp", "physics.inp", "chemistry.inp", "weno.inp", "initial.inp", "imap.inp"}
+
+
+def make(name):
+    gen, kw = CASES[name]
+    d = os.path.join(HERE, name)
+    shutil.rmtree(d, ignore_errors=True)
+    meta = gen(d, **kw)
+    subprocess.run([REF], cwd=d, check=True, stdout=subprocess.DEVNULL)
+    last = sorted(f for f in os.listdir(d) if f.startswith("op_") and f.endswith(".bin"))[-1]
+    os.replace(os.path.join(d, last), os.path.join(d, "ref_final.bin"))
+    for f in os.listdir(d):
+        if f not in KEEP and f != "ref_final.bin":
+            os.remove(os.path.join(d, f))
+    return meta
+
+
+if __name__ == "__main__":
+    if not os.path.exists(REF):
+        sys.exit("build the reference first: make -C oracle")
+    for n in (sys.argv[1:] or CASES):
+        print(n, make(n))

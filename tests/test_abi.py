@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every entry point of include/piafs_gpu.h
+(no device work: runs without a GPU)."""
+import ctypes
+import os
+import re
+
+import piafs_b200
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "piafs_gpu.h")
+
+
+def declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(piafs_gpu_\w+)\s*\(", txt)))
+
+
+def test_header_declares_the_bound_functions():
+    assert declared() == sorted(piafs_b200.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = piafs_b200.load_library()
+    for name in declared():
+        assert isinstance(getattr(lib, name), ctypes._CFuncPtr), name
+
+
+def test_error_codes_and_messages_without_device():
+    lib = piafs_b200.load_library()
+    h = ctypes.c_void_p()
+    # a missing deck is reported as an input error before any device work
+    rc = lib.piafs_gpu_create(b"/nonexistent/deck", 0, ctypes.byref(h))
+    assert rc == 2 and b"solver.inp" in lib.piafs_gpu_last_error()
+    assert lib.piafs_gpu_create(None, 0, ctypes.byref(h)) == 1
+
+
+def test_unsupported_options_are_rejected(tmp_path):
+    from piafs_b200 import cases
+    d = tmp_path / "d"
+    cases.euler1d_density_wave(str(d), N=16, n_iter=1)
+    txt = open(d / "solver.inp").read().replace("weno5", "muscl3")
+    open(d / "solver.inp", "w").write(txt)
+    lib = piafs_b200.load_library()
+    h = ctypes.c_void_p()
+    assert lib.piafs_gpu_create(str(d).encode(), 0, ctypes.byref(h)) == 3
+
+
+def test_cli_binary_is_built():
+    assert os.access(piafs_b200.CLI_PATH, os.X_OK)

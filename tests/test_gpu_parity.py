@@ -1,0 +1,281 @@
+"""Parity of the GPU path (libpiafs_gpu.so, sm_100a kernels) with the
+reference and with the CPU oracle.
+
+Tolerance: relative L2 per conserved variable <= 1e-12 (absolute where the
+reference norm is <= 1e-15), the CompareSolutions-style norm of
+Extras/CompareSolutions.c:812-906 applied variable by variable.
+"""
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+import piafs_b200
+from conftest import GOLDEN, golden_cases
+from oracle import oracle
+from piafs_b200 import Simulation, cases, deck
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def assert_close(got, ref, tol=TOL, what=""):
+    norms = deck.rel_norms(np.asarray(got).reshape(ref.shape), ref)
+    worst = max(n[1] for n in norms)
+    assert np.all(np.isfinite(got)), f"{what}: non-finite values"
+    assert worst <= tol, f"{what}: rel L2 per var {[f'{n[1]:.2e}' for n in norms]}"
+    return worst
+
+
+# --------------------------------------------------------- reference goldens
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_final_solution(name):
+    d = os.path.join(GOLDEN, name)
+    with Simulation(d) as sim:
+        sim.time_rk(sim.info["n_iter"])
+        got = sim.solution()
+        assert sim.info["singular"] == 0
+    ref = deck.read_op(os.path.join(d, "ref_final.bin")).u
+    assert_close(got, ref, what=name)
+
+
+def test_solve_writes_reference_format(deck_copy):
+    name = "ns2d_chem_crweno5_llf_64x48"
+    d = deck_copy(name)
+    with Simulation(d) as sim:
+        sim.solve(d)
+    out = sorted(f for f in os.listdir(d) if f.startswith("op_"))
+    assert out == ["op_00000.bin", "op_00001.bin"]
+    ref = deck.read_op(os.path.join(GOLDEN, name, "ref_final.bin"))
+    got = deck.read_op(os.path.join(d, "op_00001.bin"))
+    assert got.ndims == ref.ndims and got.nvars == ref.nvars and list(got.size) == list(ref.size)
+    assert all(np.array_equal(a, b) for a, b in zip(got.grid, ref.grid))
+    assert_close(got.u, ref.u)
+    ini = deck.read_op(os.path.join(d, "op_00000.bin"))
+    _, u0 = deck.read_array_binary(os.path.join(d, "initial.inp"), list(ref.size), ref.nvars)
+    assert np.array_equal(ini.u, u0)
+
+
+def test_cli_drop_in(deck_copy):
+    import subprocess
+    name = "euler1d_crweno5_rusanov_mapped_n200"
+    d = deck_copy(name)
+    subprocess.run([piafs_b200.CLI_PATH], cwd=d, check=True, stdout=subprocess.DEVNULL)
+    got = deck.read_op(os.path.join(d, "op_00001.bin")).u
+    assert_close(got, deck.read_op(os.path.join(GOLDEN, name, "ref_final.bin")).u)
+
+
+def test_intermediate_outputs_and_restart(deck_copy, tmp_path):
+    # file_op_iter output cadence and restart from an op file
+    d = str(tmp_path / "r")
+    cases.euler1d_density_wave(d, N=64, n_iter=12, dt=2e-3, file_op_iter=4)
+    with Simulation(d) as sim:
+        sim.solve(d)
+    out = sorted(f for f in os.listdir(d) if f.startswith("op_"))
+    assert out == ["op_00000.bin", "op_00001.bin", "op_00002.bin", "op_00003.bin"]
+    case = oracle.load(d)
+    want = case.interior(case.run(nsteps=8))
+    assert_close(deck.read_op(os.path.join(d, "op_00002.bin")).u, want)
+
+
+# ------------------------------------------------------- oracle, fresh decks
+FRESH = {
+    "chem_crweno_odd_37x29": (cases.ns2d_photochem_beam, dict(N=37, NY=29, n_iter=6, dt=0.4 / 2048)),
+    "chem_crweno_long_x_1100x5": (cases.ns2d_photochem_beam, dict(N=1100, NY=5, n_iter=3, dt=0.4 / 2048)),
+    "chem_crweno_long_y_6x2100": (cases.ns2d_photochem_beam, dict(N=6, NY=2100, n_iter=3, dt=0.4 / 2048)),
+    "chem_weno5_rusanov_40x33": (cases.ns2d_photochem_beam, dict(N=40, NY=33, n_iter=6, dt=0.4 / 2048,
+                                                                 scheme="weno5", upwinding="rusanov")),
+    "shear_crweno_roe_rk4_45x50": (cases.ns2d_shear_layer, dict(N=45, NY=50, n_iter=8, dt=2e-3, upwinding="roe",
+                                                                time_scheme_type="44")),
+    "shear_weno5_rf_mapped_33x31": (cases.ns2d_shear_layer, dict(N=33, NY=31, n_iter=8, dt=2e-3,
+                                                                 scheme="weno5", upwinding="rf-char",
+                                                                 weno={"mapped": 1})),
+    "euler_crweno_llf_n1500": (cases.euler1d_density_wave, dict(N=1500, n_iter=40, dt=2e-4, scheme="crweno5",
+                                                                upwinding="llf-char")),
+    "euler_weno5_nolimit_n300": (cases.euler1d_density_wave, dict(N=300, n_iter=40, dt=1e-3,
+                                                                  weno={"no_limiting": 1})),
+}
+
+
+@pytest.mark.parametrize("name", sorted(FRESH))
+def test_fresh_deck_matches_oracle(name, tmp_path):
+    gen, kw = FRESH[name]
+    d = str(tmp_path / name)
+    gen(d, **kw)
+    case = oracle.load(d)
+    want = case.interior(case.run())
+    with Simulation(d) as sim:
+        sim.time_rk(case.n_iter)
+        got = sim.solution()
+    assert_close(got, want, what=name)
+
+
+def test_host_step_matches_resident_steps():
+    d = os.path.join(GOLDEN, "ns2d_chem_crweno5_llf_64x48")
+    with Simulation(d) as a, Simulation(d) as b:
+        u = a.state()
+        t = 0.0
+        for _ in range(3):
+            b.time_rk_host(u, t)
+            t += a.info["dt"]
+        a.time_rk(3)
+        assert np.array_equal(a.state(), u)
+
+
+# ------------------------------------------------------- operator level
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+OPS = ["ns2d_chem_crweno5_llf_64x48", "ns2d_chem_weno5_llf_48x40", "ns2d_shear_weno5_roe_re200_40x32",
+       "euler1d_crweno5_rusanov_mapped_n200", "euler1d_crweno5_rf_borges_n97"]
+
+
+def state_after(case, n=4):
+    u = case.run(nsteps=n)
+    oracle.lib().orc_apply_bc(oracle.C.byref(case.P), oracle._dp(u))
+    return u
+
+
+def ghosted_close(got, want, nv, what):
+    assert_close(got.reshape(-1, nv), want.reshape(-1, nv), what=what)
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_rhs_and_terms(name):
+    d = os.path.join(GOLDEN, name)
+    case = oracle.load(d)
+    u = state_after(case)
+    t = 5 * case.dt
+    L = oracle.lib()
+    nv = case.nvars
+    P = oracle.C.byref(case.P)
+    with Simulation(d) as sim:
+        # full RHS
+        want, ubc = case.rhs(u, t)
+        got = dev(np.zeros_like(u)); ud = dev(u)
+        sim.RHSFunction(got, ud, t)
+        ghosted_close(host(got), want, nv, "RHSFunction")
+        ghosted_close(host(ud), ubc, nv, "RHSFunction ghost fill")
+        # hyperbolic
+        w = np.zeros_like(u)
+        L.orc_hyperbolic(P, oracle._dp(w), oracle._dp(u), oracle._dp(case.dxinv))
+        g = dev(np.zeros_like(u))
+        sim.HyperbolicFunction(g, dev(u), t)
+        ghosted_close(host(g), w, nv, "HyperbolicFunction")
+        # parabolic and source
+        if case.ndims == 2:
+            L.orc_parabolic(P, oracle._dp(w), oracle._dp(u), oracle._dp(case.dxinv))
+            sim.ParabolicFunction(g, dev(u), t)
+            ghosted_close(host(g), w, nv, "ParabolicFunction")
+        L.orc_source(P, oracle._dp(w), oracle._dp(u), oracle._dp(case.imap), t)
+        sim.SourceFunction(g, dev(u), t)
+        ghosted_close(host(g), w, nv, "SourceFunction")
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_flux_interp_upwind(name):
+    d = os.path.join(GOLDEN, name)
+    case = oracle.load(d)
+    u = state_after(case)
+    L = oracle.lib()
+    nv = case.nvars
+    P = oracle.C.byref(case.P)
+    with Simulation(d) as sim:
+        for dr in range(case.ndims):
+            fC = np.zeros_like(u)
+            L.orc_flux(P, oracle._dp(fC), oracle._dp(u), dr)
+            g = dev(np.zeros_like(u))
+            sim.FFunction(g, dev(u), dr)
+            ghosted_close(host(g), fC, nv, f"FFunction dir {dr}")
+            ni = int(L.orc_ninterfaces(P, dr))
+            iv = {}
+            for upw in (1, -1):
+                for uflag in (0, 1):
+                    w = np.zeros(ni * nv)
+                    L.orc_interp(P, oracle._dp(w), oracle._dp(fC), oracle._dp(u), upw, dr, uflag)
+                    gi = dev(np.zeros(ni * nv))
+                    sim.InterpolateInterfacesHyp(gi, dev(fC), dev(u), upw, dr, uflag)
+                    ghosted_close(host(gi), w, nv, f"Interp dir {dr} upw {upw} uflag {uflag}")
+                    iv[(upw, uflag)] = w
+            fI = np.zeros(ni * nv)
+            L.orc_upwind(P, oracle._dp(fI), oracle._dp(iv[(1, 0)]), oracle._dp(iv[(-1, 0)]),
+                         oracle._dp(iv[(1, 1)]), oracle._dp(iv[(-1, 1)]), oracle._dp(u), dr)
+            gI = dev(np.zeros(ni * nv))
+            sim.Upwind(gI, dev(iv[(1, 0)]), dev(iv[(-1, 0)]), dev(iv[(1, 1)]), dev(iv[(-1, 1)]), dev(u), dr)
+            ghosted_close(host(gI), fI, nv, f"Upwind dir {dr}")
+
+
+def test_boundary_conditions_and_first_derivative():
+    d = os.path.join(GOLDEN, "ns2d_chem_crweno5_llf_64x48")
+    case = oracle.load(d)
+    u = case.run(nsteps=3)
+    u_bad = u.copy()
+    u_bad.reshape(case.shape_g[0], case.shape_g[1], -1)[:3, :, :] = 7.0     # junk in low-y ghosts
+    want = u_bad.copy()
+    oracle.lib().orc_apply_bc(oracle.C.byref(case.P), oracle._dp(want))
+    with Simulation(d) as sim:
+        g = dev(u_bad)
+        sim.ApplyBoundaryConditions(g)
+        ghosted_close(host(g), want, case.nvars, "ApplyBoundaryConditions")
+        f = np.random.default_rng(1).uniform(-1, 1, u.size)
+        for dr in (0, 1):
+            for bias in (1, -1):
+                w = np.zeros_like(f)
+                oracle.lib().orc_first_derivative(oracle.C.byref(case.P), oracle._dp(w), oracle._dp(f), dr, bias,
+                                                  case.nvars)
+                gd = dev(np.zeros_like(f))
+                sim.FirstDerivativePar(gd, dev(f), dr, bias, case.nvars)
+                assert np.array_equal(host(gd), w)
+
+
+def test_tridiag_lu_matches_oracle():
+    rng = np.random.default_rng(3)
+    n, ns = 513, 37
+    a = rng.uniform(-1, 1, (n, ns)); c = rng.uniform(-1, 1, (n, ns))
+    b = 3 + rng.uniform(0, 1, (n, ns)); x = rng.uniform(-1, 1, (n, ns))
+    a[0] = 0; c[-1] = 0
+    A, B, Cc, X = (np.ascontiguousarray(v) for v in (a, b, c, x))
+    ga, gb, gc, gx = dev(A), dev(B), dev(Cc), dev(X)
+    oracle.lib().orc_tridiag(oracle._dp(A), oracle._dp(B), oracle._dp(Cc), oracle._dp(X), n, ns)
+    piafs_b200.tridiagLU(ga, gb, gc, gx, n, ns)
+    np.testing.assert_allclose(host(gx), X, rtol=1e-13, atol=1e-14)
+    # a zero pivot is reported like the reference's -1
+    z = dev(np.ones((4, 2)))
+    with pytest.raises(piafs_b200.PiafsError):
+        piafs_b200.tridiagLU(dev(np.zeros((4, 2))), dev(np.zeros((4, 2))), dev(np.zeros((4, 2))), z, 4, 2)
+
+
+# --------------------------------------------- full size, size-free checks
+def test_full_size_2048_conservation_symmetry_determinism(tmp_path):
+    """The 2048^2 photochemical workload: mass is conserved (periodic x, slip
+    walls y), a noise-free beam case stays mirror-symmetric about x = 1/2 and
+    y = 1/2, and replays are bitwise deterministic."""
+    d = str(tmp_path / "full")
+    cases.ns2d_photochem_beam(d, N=2048, n_iter=200, noise=0.0)
+    with Simulation(d) as sim:
+        u0 = sim.solution()
+        s0 = sim.state()
+        sim.time_rk(6)
+        u1 = sim.solution()
+        info = sim.info
+        assert info["singular"] == 0 and np.all(np.isfinite(u1))
+        m0, m1 = u0[:, 0].sum(), u1[:, 0].sum()
+        assert abs(m1 - m0) / m0 < 1e-12
+        f = u1.reshape(2048, 2048, -1)
+        assert np.abs(f[:, :, 3] - f[:, ::-1, 3]).max() < 1e-12 * np.abs(f[:, :, 3]).max()
+        assert np.abs(f[:, :, 3] - f[::-1, :, 3]).max() < 1e-12 * np.abs(f[:, :, 3]).max()
+        assert np.abs(f[:, :, 1] + f[:, ::-1, 1]).max() < 1e-12 * max(np.abs(f[:, :, 1]).max(), 1e-300) + 1e-300
+        # the heating changed the energy inside the beam
+        assert f[1024, 1024, 3] > u0.reshape(2048, 2048, -1)[1024, 1024, 3]
+        sim.set_state(s0, 0.0)
+        sim.time_rk(6)
+        assert np.array_equal(sim.solution(), u1)
