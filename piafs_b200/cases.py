@@ -188,3 +188,43 @@ def ns2d_shear_layer(path: str, N: int = 64, NY: Optional[int] = None, n_iter: i
         deck.write_keyfile(os.path.join(path, "weno.inp"), weno)
     deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, 4))
     return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}
+
+
+def ns2d_density_wave(path: str, N: int = 64, NY: Optional[int] = None, axis: int = 0, n_iter: int = 10,
+                      dt: float = 1e-4, amp: float = 0.2, scheme: str = "crweno5", upwinding: str = "llf-char",
+                      Re: float = 100.0, time_scheme_type: str = "ssprk3", op_file_format: str = "binary",
+                      file_op_iter: Optional[int] = None, screen_op_iter: int = 0) -> Dict:
+    """2D Navier-Stokes (no chemistry) density wave along `axis`, periodic in
+    both directions: rho = 1 + amp sin(2 pi s), velocity 1 along the wave,
+    p = 1/gamma, where s is x (axis 0) or y (axis 1)."""
+    os.makedirs(path, exist_ok=True)
+    NX, NY = N, NY or N
+    gamma = 1.4
+    x = np.arange(NX, dtype=np.float64) / NX
+    y = np.arange(NY, dtype=np.float64) / NY
+    X, Y = np.meshgrid(x, y)
+    S = X if axis == 0 else Y
+    rho = 1.0 + amp * np.sin(2 * np.pi * S)
+    p = 1.0 / gamma
+    u = np.zeros((NY, NX, 4))
+    u[..., 0] = rho
+    u[..., 1 + axis] = rho
+    u[..., 3] = p / (gamma - 1.0) + 0.5 * rho
+    deck.write_keyfile(os.path.join(path, "solver.inp"), {
+        "ndims": 2, "nvars": 4, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
+        "time_scheme": "rk", "time_scheme_type": time_scheme_type,
+        "hyp_space_scheme": scheme, "hyp_interp_type": "components", "par_space_scheme": "2",
+        "dt": dt, "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
+        "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
+        "model": "navierstokes2d",
+    })
+    deck.write_boundary(os.path.join(path, "boundary.inp"), [
+        deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0, -1e99, 1e99]),
+        deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0, -1e99, 1e99]),
+        deck.BoundaryZone("periodic", 1, 1, [-1e99, 1e99, 0.0, 0.0]),
+        deck.BoundaryZone("periodic", 1, -1, [-1e99, 1e99, 0.0, 0.0]),
+    ])
+    deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding, "Re": Re,
+                                                           "Pr": 0.72})
+    deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, 4))
+    return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}

@@ -30,13 +30,15 @@ CASES = {
         N=128, n_iter=100, dt=2e-3, upwinding="llf-char", time_scheme_type="44", weno={"yc": 1})),
     "euler1d_crweno5_rf_borges_n97": (cases.euler1d_density_wave, dict(
         N=97, n_iter=60, dt=2e-3, amp=0.3, scheme="crweno5", upwinding="rf-char", weno={"borges": 1})),
-    # the 2D photochemical workload at small size (same dt as at 2048^2)
-    "ns2d_chem_crweno5_llf_64x48": (cases.ns2d_photochem_beam, dict(N=64, NY=48, n_iter=20, dt=DT2D)),
-    "ns2d_chem_weno5_llf_48x40": (cases.ns2d_photochem_beam, dict(N=48, NY=40, n_iter=20, dt=DT2D, scheme="weno5")),
+    # the 2D photochemical workload at small size (same dt as at 2048^2); 60
+    # steps carry the solution past the heating pulse (peak at t = 6.9e-3) so
+    # that every conserved variable holds signal well above round-off
+    "ns2d_chem_crweno5_llf_64x48": (cases.ns2d_photochem_beam, dict(N=64, NY=48, n_iter=60, dt=DT2D)),
+    "ns2d_chem_weno5_llf_48x40": (cases.ns2d_photochem_beam, dict(N=48, NY=40, n_iter=60, dt=DT2D, scheme="weno5")),
     "ns2d_chem_crweno5_rf_borges_32x32": (cases.ns2d_photochem_beam, dict(
-        N=32, NY=32, n_iter=15, dt=DT2D, upwinding="rf-char", weno={"borges": 1})),
+        N=32, NY=32, n_iter=60, dt=DT2D, upwinding="rf-char", weno={"borges": 1})),
     "ns2d_chem3layer_crweno5_llf_24x20": (cases.ns2d_photochem_beam, dict(
-        N=24, NY=20, n_iter=10, dt=DT2D, extra_chem={"z_mm": 3.0, "nz": 20}, layers=3)),
+        N=24, NY=20, n_iter=60, dt=DT2D, extra_chem={"z_mm": 3.0, "nz": 20}, layers=3)),
     "ns2d_shear_crweno5_llf_re200_48x40": (cases.ns2d_shear_layer, dict(N=48, NY=40, n_iter=30, dt=2e-3)),
     "ns2d_shear_weno5_roe_re200_40x32": (cases.ns2d_shear_layer, dict(
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", upwinding="roe")),

