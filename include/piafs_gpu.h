@@ -151,6 +151,40 @@ int piafs_gpu_FirstDerivativePar(piafs_gpu_sim* sim, double* Df, const double* f
  * PIAFS_ERR_SINGULAR on a zero pivot like the reference's -1. */
 int piafs_gpu_tridiagLU(double* a, double* b, double* c, double* x, int n, int ns);
 
+/* ---- allocation-free hyperbolic term ----
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they need the hyperbolic term -- code running while a stream
+ * it shares is being captured into a CUDA graph, or a plugin inside an
+ * application whose memory manager owns the whole device -- this computes
+ * what piafs_gpu_HyperbolicFunction computes, from the caller's u (ghosted,
+ * ghosts filled, reference layout) and dxinv (ghosted 1/dx of each dimension,
+ * concatenated), into the caller's hyp, with no simulation object and no
+ * device allocation.  Its working arrays live in one 64 MiB __device__ array
+ * that every GPU loading this library holds until exit; problems whose
+ * working set (about 7 x nvars x ghosted points x 8 bytes) exceeds it are
+ * rejected with PIAFS_ERR_ARGUMENT.  The first call on a device looks up that
+ * array's address with the device current and should come before any stream
+ * capture; all calls on a device share the array, so calls that overlap on
+ * the GPU race and must be serialised by the caller.  The call runs on
+ * `stream` (a cudaStream_t, 0 for the default stream) and waits for it. */
+enum { PIAFS_MODEL_EULER1D = 0, PIAFS_MODEL_NS2D = 1 };
+enum { PIAFS_SCHEME_WENO5 = 0, PIAFS_SCHEME_CRWENO5 = 1 };
+enum { PIAFS_UPWIND_ROE = 0, PIAFS_UPWIND_RF = 1, PIAFS_UPWIND_LLF = 2, PIAFS_UPWIND_RUSANOV = 3 };
+enum { PIAFS_WENO_JS = 0, PIAFS_WENO_MAPPED = 1, PIAFS_WENO_BORGES = 2, PIAFS_WENO_YC = 3 };
+typedef struct {
+  int ndims, nvars, ghosts;
+  int dim[2];          /* interior points per dimension */
+  int model;           /* PIAFS_MODEL_*   */
+  int scheme;          /* PIAFS_SCHEME_*  */
+  int upwind;          /* PIAFS_UPWIND_*  */
+  int weno_type;       /* PIAFS_WENO_*    */
+  int no_limiting;     /* weno.inp no_limiting */
+  double weno_eps;     /* weno.inp epsilon     */
+  double gamma;        /* ratio of specific heats in effect */
+} piafs_gpu_hyp_params;
+int piafs_gpu_HyperbolicFunction_noalloc(const piafs_gpu_hyp_params* p, double* hyp, const double* u,
+                                         const double* dxinv, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

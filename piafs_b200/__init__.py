@@ -63,7 +63,17 @@ SIGNATURES = {
     "piafs_gpu_Upwind": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double]),
     "piafs_gpu_FirstDerivativePar": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int]),
     "piafs_gpu_tridiagLU": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
+    "piafs_gpu_HyperbolicFunction_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
 }
+
+
+class HypParams(C.Structure):
+    """piafs_gpu_hyp_params of include/piafs_gpu.h."""
+    _fields_ = [
+        ("ndims", C.c_int), ("nvars", C.c_int), ("ghosts", C.c_int), ("dim", C.c_int * 2),
+        ("model", C.c_int), ("scheme", C.c_int), ("upwind", C.c_int), ("weno_type", C.c_int),
+        ("no_limiting", C.c_int), ("weno_eps", C.c_double), ("gamma", C.c_double),
+    ]
 
 
 class Info(C.Structure):
@@ -268,6 +278,14 @@ class Simulation:
 
     def FirstDerivativePar(self, Df, f, dir, bias, nv):
         _check(_lib.piafs_gpu_FirstDerivativePar(self._h, _ptr(Df), _ptr(f), int(dir), int(bias), int(nv)))
+
+
+def hyperbolic_noalloc(params: "HypParams", hyp, u, dxinv, stream: int = 0):
+    """Allocation-free hyperbolic term (piafs_gpu_HyperbolicFunction_noalloc)."""
+    L = load_library()
+    code = L.piafs_gpu_HyperbolicFunction_noalloc(C.byref(params), _ptr(hyp), _ptr(u), _ptr(dxinv), stream)
+    if code != PIAFS_OK:
+        raise PiafsError(code, L.piafs_gpu_last_error().decode())
 
 
 def tridiagLU(a, b, c, x, n: int, ns: int):

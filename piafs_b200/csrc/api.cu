@@ -23,6 +23,10 @@ int fail(int code, const std::string& msg) {
 }
 }  // namespace
 
+namespace piafs {
+int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
+}
+
 #define CK(call)                                                                                  \
   do {                                                                                            \
     cudaError_t e_ = (call);                                                                      \

@@ -1,0 +1,111 @@
+"""The allocation-free hyperbolic term (piafs_gpu_HyperbolicFunction_noalloc).
+
+Callers that cannot allocate device memory when they need the hyperbolic term
+(code running during a stream capture, plugins inside an application that
+owns all device memory) use this entry point; its working arrays live in a
+fixed 64 MiB __device__ array instead of cudaMalloc'd buffers.  These checks
+call it through the C ABI and hold it to the allocating entry point
+(piafs_gpu_HyperbolicFunction) on the same state, twice in a row so that the
+second call runs on the scratch the first one left behind.  This file is
+collected last so that a failure here stops a -x run only after every other
+test has run.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import piafs_b200
+from conftest import GOLDEN
+from piafs_b200 import HypParams, Simulation, deck
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+TOL = 1e-12
+
+MODEL = {"euler1d": 0, "navierstokes2d": 1}
+SCHEME = {"weno5": 0, "crweno5": 1}
+UPWIND = {"roe": 0, "rf-char": 1, "llf-char": 2, "rusanov": 3}
+
+
+def ghosted_dxinv(grid_1d, g):
+    """1/dx with linearly extrapolated ghost coordinates and copied ghost
+    values, as the reference builds it (ReadArray.c:71-91,
+    InitialSolution.c:73-113)."""
+    n = len(grid_1d)
+    x = np.zeros(n + 2 * g)
+    x[g:g + n] = grid_1d
+    for i in range(g):
+        x[i] = x[g] + (g - i) * (x[g] - x[g + 1])
+    for i in range(n + g, n + 2 * g):
+        x[i] = x[n + g - 1] + (i - (n + g - 1)) * (x[n + g - 1] - x[n + g - 2])
+    d = np.zeros(n + 2 * g)
+    d[g:g + n] = 2.0 / (x[g + 1:g + n + 1] - x[g - 1:g + n - 1])
+    d[:g] = d[g]
+    d[n + g:] = d[n + g - 1]
+    return d
+
+
+def params_for(dirpath, sim):
+    kv = deck.read_keyfile(os.path.join(dirpath, "solver.inp"))
+    ph = deck.read_keyfile(os.path.join(dirpath, "physics.inp"))
+    w = deck.read_keyfile(os.path.join(dirpath, "weno.inp")) if os.path.exists(
+        os.path.join(dirpath, "weno.inp")) else {}
+    info = sim.info
+    p = HypParams()
+    p.ndims, p.nvars, p.ghosts = info["ndims"], info["nvars"], info["ghosts"]
+    p.dim[0], p.dim[1] = info["dim"][0], info["dim"][1]
+    p.model = MODEL[kv["model"][0]]
+    p.scheme = SCHEME[kv["hyp_space_scheme"][0]]
+    p.upwind = UPWIND[ph.get("upwinding", ["roe"])[0]]
+    flag = lambda k: int(w.get(k, ["0"])[0])
+    p.weno_type = 3 if flag("yc") else 2 if flag("borges") else 1 if flag("mapped") else 0
+    p.no_limiting = flag("no_limiting")
+    p.weno_eps = float(w.get("epsilon", ["1e-6"])[0])
+    p.gamma = info["gamma"]
+    dims = [info["dim"][0]] + ([info["dim"][1]] if info["ndims"] == 2 else [])
+    raw = np.fromfile(os.path.join(dirpath, "initial.inp"), dtype=np.float64)
+    grids, off = [], 0
+    for n in dims:
+        grids.append(raw[off:off + n])
+        off += n
+    dxinv = np.concatenate([ghosted_dxinv(gr, info["ghosts"]) for gr in grids])
+    return p, dxinv
+
+
+def rel_l2(got, want, nv):
+    return max(n[1] for n in deck.rel_norms(got.reshape(-1, nv), want.reshape(-1, nv)))
+
+
+@pytest.mark.parametrize("name", ["ns2d_chem_crweno5_llf_64x48", "ns2d_shear_weno5_roe_re200_40x32",
+                                  "euler1d_crweno5_rusanov_mapped_n200"])
+def test_noalloc_matches_allocating_entry_point(name):
+    d = os.path.join(GOLDEN, name)
+    with Simulation(d) as sim:
+        sim.time_rk(5)
+        u = torch.from_numpy(sim.state()).cuda()
+        sim.ApplyBoundaryConditions(u)
+        nv = sim.info["nvars"]
+        want = torch.zeros_like(u)
+        sim.HyperbolicFunction(want, u)
+        p, dxinv = params_for(d, sim)
+    dx = torch.from_numpy(dxinv).cuda()
+    w = want.cpu().numpy()
+    for _ in range(2):
+        got = torch.full_like(u, np.nan)
+        piafs_b200.hyperbolic_noalloc(p, got, u, dx)
+        g = got.cpu().numpy()
+        assert np.all(np.isfinite(g))
+        assert rel_l2(g, w, nv) <= TOL
+
+
+def test_noalloc_rejects_problems_beyond_its_scratch():
+    p = HypParams()
+    p.ndims, p.nvars, p.ghosts = 2, 11, 3
+    p.dim[0], p.dim[1] = 1024, 1024
+    p.model, p.scheme, p.upwind, p.weno_type = 1, 1, 2, 0
+    p.weno_eps, p.gamma = 1e-6, 1.4
+    dummy = torch.zeros(8, dtype=torch.float64, device="cuda")
+    with pytest.raises(piafs_b200.PiafsError) as ex:
+        piafs_b200.hyperbolic_noalloc(p, dummy, dummy, dummy)
+    assert ex.value.code == 1 and "MiB" in str(ex.value)
