@@ -151,6 +151,13 @@ int piafs_gpu_FirstDerivativePar(piafs_gpu_sim* sim, double* Df, const double* f
  * PIAFS_ERR_SINGULAR on a zero pivot like the reference's -1. */
 int piafs_gpu_tridiagLU(double* a, double* b, double* c, double* x, int n, int ns);
 
+/* ---- diagnostics ----
+ * No counterpart in the reference.  y[i] = 1/x[i] (device arrays) computed
+ * by the Newton-Raphson reciprocal that the reconstruction and line-solve
+ * kernels use in place of a division, so that callers can check its
+ * accuracy against 1/x; for finite x whose reciprocal is a normal number. */
+int piafs_gpu_reciprocal(const double* x, double* y, long long n);
+
 /* ---- allocation-free hyperbolic term ----
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory when they need the hyperbolic term -- code running while a stream

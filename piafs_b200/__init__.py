@@ -64,6 +64,7 @@ SIGNATURES = {
     "piafs_gpu_FirstDerivativePar": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int]),
     "piafs_gpu_tridiagLU": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
     "piafs_gpu_HyperbolicFunction_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "piafs_gpu_reciprocal": (C.c_int, [_vp, _vp, C.c_longlong]),
 }
 
 
@@ -284,6 +285,14 @@ def hyperbolic_noalloc(params: "HypParams", hyp, u, dxinv, stream: int = 0):
     """Allocation-free hyperbolic term (piafs_gpu_HyperbolicFunction_noalloc)."""
     L = load_library()
     code = L.piafs_gpu_HyperbolicFunction_noalloc(C.byref(params), _ptr(hyp), _ptr(u), _ptr(dxinv), stream)
+    if code != PIAFS_OK:
+        raise PiafsError(code, L.piafs_gpu_last_error().decode())
+
+
+def reciprocal(x, y):
+    """y = 1/x on device arrays by the kernels' Newton-Raphson reciprocal."""
+    L = load_library()
+    code = L.piafs_gpu_reciprocal(_ptr(x), _ptr(y), int(x.numel()))
     if code != PIAFS_OK:
         raise PiafsError(code, L.piafs_gpu_last_error().decode())
 

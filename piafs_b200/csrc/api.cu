@@ -566,4 +566,13 @@ int piafs_gpu_tridiagLU(double* a, double* b, double* c, double* x, int n, int n
   return PIAFS_OK;
 }
 
+int piafs_gpu_reciprocal(const double* x, double* y, long long n) {
+  if (!x || !y || n < 0) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  if (n == 0) return PIAFS_OK;
+  launch_reciprocal(x, y, n, 0);
+  CK(cudaGetLastError());
+  CK(cudaDeviceSynchronize());
+  return PIAFS_OK;
+}
+
 }  // extern "C"

@@ -111,6 +111,24 @@ __device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T
   w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
 }
 
+// Reciprocal 1/x of a finite, nonzero, normal x whose reciprocal is normal.
+// Newton-Raphson iteration for f(y) = 1/y - x, y <- y + y (1 - x y), each
+// step squaring the relative error (P. Markstein, "Computation of elementary
+// functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34
+// (1990) 111-119), started from the hardware estimate of PTX
+// rcp.approx.ftz.f64; two steps take the estimate to within a unit or two in
+// the last place.  x = 0 gives NaN, which callers detect separately.
+#ifdef __CUDACC__
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+#endif
+
 // 3-point candidate values of explicit WENO5 (Interp1PrimFifthOrderWENO.c:144-146)
 template <typename T>
 __device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p1, T p2) {

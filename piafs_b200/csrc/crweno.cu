@@ -1,0 +1,336 @@
+// CRWENO5 interface reconstruction with its tridiagonal line solves (sm_100a).
+//
+// Interp1PrimFifthOrderCRWENO (Interp1PrimFifthOrderCRWENO.c:81-240) builds,
+// for every grid line and solution component, one tridiagonal system per
+// upwind bias and per reconstructed array (u and the flux f), and solves them
+// with tridiagLU (tridiagLU.c:86-277).  Here one CTA owns one (line, component,
+// array) and solves the left- and the right-biased systems of that array
+// together, one thread per M consecutive rows:
+//
+//   * the M + 5 cells a thread needs are loaded once for both systems; the
+//     smoothness indicators of every 3-cell window and the two-cell averages
+//     of the compact right-hand side are computed once per window and shared,
+//     since the right-biased stencil is the mirror image of the left-biased
+//     one (the left system at interface i uses windows centred at i-2, i-1,
+//     i; the right one the mirrored windows centred at i+1, i, i-1);
+//   * the chunk of M rows is reduced in registers (the first row is the
+//     chunk's separator; the others are eliminated down and up, so that each
+//     reads x = rho - alpha X_k - gamma X_{k+1} in the separators X);
+//   * the separator system, one unknown per thread and per bias, is solved by
+//     parallel cyclic reduction on rows scaled to a unit diagonal (three
+//     values per row), both biases in the same steps and barriers;
+//   * every row is recovered from its two separators and the results are
+//     staged in shared memory so that the x-direction stores are coalesced.
+//
+// Rows 0 and N are the WENO5 rows with the WENO5 optimal weights (physical
+// boundaries, also on periodic domains, Interp1PrimFifthOrderCRWENO.c:164-175);
+// they are computed directly and folded into rows 1 and N-1.  Rows past N-1
+// are identity rows.  Divisions are reciprocals by Newton-Raphson refinement
+// (rcp_nr), so results agree with the reference to rounding, not bit for bit.
+#include "kernels.h"
+
+namespace piafs {
+
+namespace {
+
+constexpr int WT_NOLIM = 4;   // no_limiting: optimal weights everywhere
+
+// Nonlinear CRWENO5 weights (optimal weights 0.2, 0.5, 0.3) from the three
+// smoothness indicators of one stencil; tau is the WENO-Z / Yamaleev-Carpenter
+// reference indicator (interpolation.h:255-545).
+template <int WT>
+__device__ __forceinline__ void crw_weights(double b1, double b2, double b3, double tau, double eps, double& w1,
+                                            double& w2, double& w3) {
+  constexpr double c1 = 0.2, c2 = 0.5, c3 = 0.3;
+  if (WT == WT_NOLIM) {
+    w1 = c1; w2 = c2; w3 = c3;
+  } else if (WT == W_JS || WT == W_MAPPED) {
+    // c_k/q_k / sum_m c_m/q_m with q = (beta + eps)^2, as c_k prod_{m!=k} q_m / sum
+    const double s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
+    const double q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
+    const double a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
+    const double inv = rcp_nr(a1 + a2 + a3);
+    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+    if (WT == W_MAPPED) {   // Henrick-Aslam-Powers mapping
+      const double x1 = w1, x2 = w2, x3 = w3;
+      const double A1 = x1 * (c1 + c1 * c1 - 3.0 * c1 * x1 + x1 * x1) * rcp_nr(c1 * c1 + x1 * (1.0 - 2.0 * c1));
+      const double A2 = x2 * (c2 + c2 * c2 - 3.0 * c2 * x2 + x2 * x2) * rcp_nr(c2 * c2 + x2 * (1.0 - 2.0 * c2));
+      const double A3 = x3 * (c3 + c3 * c3 - 3.0 * c3 * x3 + x3 * x3) * rcp_nr(c3 * c3 + x3 * (1.0 - 2.0 * c3));
+      const double inv2 = rcp_nr(A1 + A2 + A3);
+      w1 = A1 * inv2; w2 = A2 * inv2; w3 = A3 * inv2;
+    }
+  } else {
+    const double r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
+    const double a1 = c1 * (1.0 + r1 * r1), a2 = c2 * (1.0 + r2 * r2), a3 = c3 * (1.0 + r3 * r3);
+    const double inv = rcp_nr(a1 + a2 + a3);
+    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+  }
+}
+
+// WENO5 boundary-row value at interface i (optimal weights 0.1, 0.6, 0.3,
+// Interp1PrimFifthOrderCRWENO.c:164-175 with the explicit WENO5 candidates)
+__device__ __forceinline__ double crw_edge(const DevParams& P, const double* src, long long st, int i, int upw) {
+  double m3, m2, m1, p1, p2;
+  if (upw > 0) { m3 = src[(i - 3) * st]; m2 = src[(i - 2) * st]; m1 = src[(i - 1) * st]; p1 = src[i * st]; p2 = src[(i + 1) * st]; }
+  else         { m3 = src[(i + 2) * st]; m2 = src[(i + 1) * st]; m1 = src[i * st]; p1 = src[(i - 1) * st]; p2 = src[(i - 2) * st]; }
+  double w1, w2, w3;
+  if (P.no_limiting) { w1 = 0.1; w2 = 0.6; w3 = 0.3; }
+  else weno_weights(P.weno_type, 0.1, 0.6, 0.3, m3, m2, m1, p1, p2, P.eps, w1, w2, w3);
+  return weno5_value(w1, w2, w3, m3, m2, m1, p1, p2);
+}
+
+// padded index into the output staging buffer (conflict-free for the strided
+// writes of the recovery and the unit-stride reads of the store)
+__device__ __forceinline__ int stg(int i) { return i + (i >> 4); }
+
+}  // namespace
+
+template <int M, int DIR, int WT>
+__global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
+    k_crweno_pair(DevParams P, const double* __restrict__ U, const double* __restrict__ F, double* __restrict__ uL,
+                  double* __restrict__ uR, double* __restrict__ fL, double* __restrict__ fR,
+                  int* __restrict__ err) {
+  static_assert(M >= 2, "a chunk needs a separator and at least one interior row");
+  extern __shared__ double sm[];
+  const int Pt = blockDim.x, k = threadIdx.x;
+  double* pc = sm;               // PCR rows, [2 buffers][2 biases][a, c, d][Pt]
+  double* tp = sm + 12 * Pt;     // last-row coefficients per chunk, [2][3][Pt]
+  double* sy = sm + 18 * Pt;     // separator values, [2][Pt]
+  double* so = sm + 20 * Pt;     // output staging, [2][stg(N) + 1]
+  const int line = blockIdx.x, v = blockIdx.y;
+  const bool isF = blockIdx.z != 0;
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const long long st = DIR == 0 ? 1 : P.W0;
+  const long long ist = DIR == 0 ? 1 : P.N0;
+  const long long base = DIR == 0 ? pidx(P, 0, line) : pidx(P, line, 0);
+  const long long ibase = DIR == 0 ? (long long)(P.N0 + 1) * line : line;
+  const double* src = (isF ? F : U) + (long long)v * P.ps + base;
+  double* oL = (isF ? fL : uL) + (long long)v * P.pis + ibase;
+  double* oR = (isF ? fR : uR) + (long long)v * P.pis + ibase;
+  const int s = 1 + k * M;          // separator row (interface) of this thread
+  const int kN = (N - 2) / M;       // thread owning row N-1
+  const double eps = P.eps;
+
+  // cells s-3 .. s+M+1
+  double c[M + 5];
+#pragma unroll
+  for (int r = 0; r < M + 5; r++) {
+    const int cell = s - 3 + r;
+    c[r] = cell <= N + 2 ? src[cell * st] : 0.0;
+  }
+  double x0[2] = {0.0, 0.0}, xN[2] = {0.0, 0.0};
+  if (k == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
+  if (k == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
+
+  // smoothness indicators of the windows centred at cells s-2+t (t = 0..M+2):
+  // b1: 13/12 d^2 + 1/4 (a-4b+3c)^2, b2: .. (a-c)^2, b3: .. (3a-4b+c)^2
+  double b1[M + 3], b2[M + 3], b3[M + 3];
+  if (WT != WT_NOLIM) {
+#pragma unroll
+    for (int t = 0; t < M + 3; t++) {
+      const double a = c[t], b = c[t + 1], cc = c[t + 2];
+      const double d = a - 2.0 * b + cc;
+      const double e1 = a - 4.0 * b + 3.0 * cc, e2 = a - cc, e3 = 3.0 * a - 4.0 * b + cc;
+      const double dd = (13.0 / 12.0) * d * d;
+      b1[t] = dd + 0.25 * e1 * e1;
+      b2[t] = dd + 0.25 * e2 * e2;
+      b3[t] = dd + 0.25 * e3 * e3;
+    }
+  }
+  // two-cell averages of the compact right-hand side, cells (s-3+j, s-2+j):
+  // pp = 5/6 left + 1/6 right, qq = 1/6 left + 5/6 right
+  constexpr double s6 = 1.0 / 6.0, s56 = 5.0 * (1.0 / 6.0);
+  double pp[M + 3], qq[M + 3];
+#pragma unroll
+  for (int j = 1; j < M + 3; j++) {
+    pp[j] = s56 * c[j] + s6 * c[j + 1];
+    qq[j] = s6 * c[j] + s56 * c[j + 1];
+  }
+
+  // ---- rows and the downward elimination, both biases (q = 0 left, 1 right)
+  double As[2], Bs[2], Cs[2], Rs[2];
+  double al[2][M], cg[2][M], rh[2][M];
+  int bad = 0;
+#pragma unroll
+  for (int r = 0; r < M; r++) {
+    const int i = s + r;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      double A = 0.0, B = 1.0, C = 0.0, R = 0.0;
+      if (i <= N - 1) {
+        double w1, w2, w3, f1, f2, f3, tau = 0.0;
+        if (q == 0) {
+          if (WT == W_BORGES) tau = fabs(b3[r + 2] - b1[r]);
+          if (WT == W_YC) { const double t4 = c[r] - 4.0 * c[r + 1] + 6.0 * c[r + 2] - 4.0 * c[r + 3] + c[r + 4]; tau = t4 * t4; }
+          crw_weights<WT>(b1[r], b2[r + 1], b3[r + 2], tau, eps, w1, w2, w3);
+          f1 = qq[r + 1]; f2 = pp[r + 2]; f3 = qq[r + 2];
+        } else {
+          if (WT == W_BORGES) tau = fabs(b1[r + 1] - b3[r + 3]);
+          if (WT == W_YC) { const double t4 = c[r + 5] - 4.0 * c[r + 4] + 6.0 * c[r + 3] - 4.0 * c[r + 2] + c[r + 1]; tau = t4 * t4; }
+          crw_weights<WT>(b3[r + 3], b2[r + 2], b1[r + 1], tau, eps, w1, w2, w3);
+          f1 = pp[r + 3]; f2 = qq[r + 2]; f3 = pp[r + 2];
+        }
+        constexpr double t3 = 1.0 / 3.0;
+        const double lo = (2.0 * t3) * w1 + t3 * w2, hi = t3 * w3;
+        B = t3 * w1 + (2.0 * t3) * w2 + (2.0 * t3) * w3;
+        A = q == 0 ? lo : hi;
+        C = q == 0 ? hi : lo;
+        R = w1 * f1 + w2 * f2 + w3 * f3;
+        if (i == 1) { R -= A * x0[q]; A = 0.0; }
+        if (i == N - 1) { R -= C * xN[q]; C = 0.0; }
+      }
+      if (r == 0) { As[q] = A; Bs[q] = B; Cs[q] = C; Rs[q] = R; continue; }
+      // rows scaled to a unit diagonal: x_r + cg_r x_{r+1} = rh_r - al_r X_k
+      const double be = r == 1 ? B : B - A * cg[q][r - 1];
+      bad |= (be == 0.0);
+      const double rb = rcp_nr(be);
+      if (r == 1) { al[q][1] = A * rb; rh[q][1] = R * rb; }
+      else { al[q][r] = -(A * al[q][r - 1]) * rb; rh[q][r] = (R - A * rh[q][r - 1]) * rb; }
+      cg[q][r] = C * rb;
+    }
+  }
+  // ---- upward elimination: x_{s+r} = rh_r - al_r X_k - cg_r X_{k+1}
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+#pragma unroll
+    for (int r = M - 2; r >= 1; r--) {
+      const double g = cg[q][r];
+      al[q][r] -= g * al[q][r + 1];
+      rh[q][r] -= g * rh[q][r + 1];
+      cg[q][r] = -(g * cg[q][r + 1]);
+    }
+    tp[(q * 3 + 0) * Pt + k] = al[q][M - 1];
+    tp[(q * 3 + 1) * Pt + k] = cg[q][M - 1];
+    tp[(q * 3 + 2) * Pt + k] = rh[q][M - 1];
+  }
+  __syncthreads();
+
+  // ---- separator equations As x_{s-1} + Bs X_k + Cs x_{s+1} = Rs, with
+  //      x_{s-1} from the previous chunk's last row and x_{s+1} from row 1
+  double a[2], cq[2], d[2];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    double alp = 0.0, gap = 0.0, rhp = 0.0;
+    if (k > 0) { alp = tp[(q * 3 + 0) * Pt + k - 1]; gap = tp[(q * 3 + 1) * Pt + k - 1]; rhp = tp[(q * 3 + 2) * Pt + k - 1]; }
+    const double b = Bs[q] - As[q] * gap - Cs[q] * al[q][1];
+    bad |= (b == 0.0);
+    const double rb = rcp_nr(b);
+    a[q] = -(As[q] * alp) * rb;
+    cq[q] = -(Cs[q] * cg[q][1]) * rb;
+    d[q] = (Rs[q] - As[q] * rhp - Cs[q] * rh[q][1]) * rb;
+    pc[(q * 3 + 0) * Pt + k] = a[q];
+    pc[(q * 3 + 1) * Pt + k] = cq[q];
+    pc[(q * 3 + 2) * Pt + k] = d[q];
+  }
+  if (bad) atomicOr(err, 1);
+  __syncthreads();
+  // ---- parallel cyclic reduction on unit-diagonal rows a x_{k-dl} + x_k + c x_{k+dl} = d
+  int buf = 0;
+  for (int dl = 1; dl < Pt; dl <<= 1) {
+    const double* cur = pc + buf * 6 * Pt;
+    double* nxt = pc + (buf ^ 1) * 6 * Pt;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      double am = 0.0, cm = 0.0, dm = 0.0, ap = 0.0, cp = 0.0, dp = 0.0;
+      if (k - dl >= 0) { am = cur[(q * 3 + 0) * Pt + k - dl]; cm = cur[(q * 3 + 1) * Pt + k - dl]; dm = cur[(q * 3 + 2) * Pt + k - dl]; }
+      if (k + dl < Pt) { ap = cur[(q * 3 + 0) * Pt + k + dl]; cp = cur[(q * 3 + 1) * Pt + k + dl]; dp = cur[(q * 3 + 2) * Pt + k + dl]; }
+      const double bn = 1.0 - a[q] * cm - cq[q] * ap;
+      const double rb = rcp_nr(bn);
+      const double an = -(a[q] * am) * rb, cn = -(cq[q] * cp) * rb;
+      d[q] = (d[q] - a[q] * dm - cq[q] * dp) * rb;
+      a[q] = an; cq[q] = cn;
+      nxt[(q * 3 + 0) * Pt + k] = a[q];
+      nxt[(q * 3 + 1) * Pt + k] = cq[q];
+      nxt[(q * 3 + 2) * Pt + k] = d[q];
+    }
+    buf ^= 1;
+    __syncthreads();
+  }
+  sy[k] = d[0];
+  sy[Pt + k] = d[1];
+  __syncthreads();
+
+  // ---- recover every row
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const double Xk = d[q];
+    const double Xn = k + 1 < Pt ? sy[q * Pt + k + 1] : 0.0;
+    double* o = so + q * (stg(N) + 1);
+    if (s <= N - 1) o[stg(s)] = Xk;
+#pragma unroll
+    for (int r = 1; r < M; r++) {
+      const int i = s + r;
+      if (i <= N - 1) o[stg(i)] = rh[q][r] - al[q][r] * Xk - cg[q][r] * Xn;
+    }
+    if (k == 0) o[0] = x0[q];
+    if (k == kN) o[stg(N)] = xN[q];
+  }
+  __syncthreads();
+  for (int i = k; i <= N; i += Pt) {
+    oL[i * ist] = so[stg(i)];
+    oR[i * ist] = so[stg(N) + 1 + stg(i)];
+  }
+}
+
+// rows per thread: the smallest M that keeps a line within one 256-thread CTA
+// (lines of up to 4097 interfaces)
+int crweno_rows_per_thread(int N) {
+  const int rows = N - 1;
+  const int cand[4] = {2, 4, 8, 16};
+  for (int c = 0; c < 4; c++)
+    if ((rows + cand[c] - 1) / cand[c] <= 256) return cand[c];
+  return -1;
+}
+
+namespace {
+
+template <int M, int DIR, int WT>
+void crweno_launch(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                   double* fR, int* err, cudaStream_t s) {
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const int nlines = DIR == 0 ? P.N1 : P.N0;
+  int Pt = (N - 1 + M - 1) / M;
+  Pt = ((Pt + 31) / 32) * 32;
+  const size_t smem = (size_t)(20 * Pt + 2 * (N + (N >> 4) + 1)) * sizeof(double);
+  // the largest line this M serves: 256 M + 1 interfaces
+  raise_smem_limit<k_crweno_pair<M, DIR, WT>>((20 * 256 + 2 * (256 * M + 2 + ((256 * M + 2) >> 4) + 1)) *
+                                              (int)sizeof(double));
+  dim3 grid(nlines, P.nvars, 2);
+  k_crweno_pair<M, DIR, WT><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, err);
+}
+
+template <int M, int DIR>
+void crweno_launch_wt(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                      double* fR, int* err, cudaStream_t s) {
+  if (P.no_limiting) return crweno_launch<M, DIR, WT_NOLIM>(P, U, F, uL, uR, fL, fR, err, s);
+  switch (P.weno_type) {
+    case W_MAPPED: return crweno_launch<M, DIR, W_MAPPED>(P, U, F, uL, uR, fL, fR, err, s);
+    case W_BORGES: return crweno_launch<M, DIR, W_BORGES>(P, U, F, uL, uR, fL, fR, err, s);
+    case W_YC: return crweno_launch<M, DIR, W_YC>(P, U, F, uL, uR, fL, fR, err, s);
+    default: return crweno_launch<M, DIR, W_JS>(P, U, F, uL, uR, fL, fR, err, s);
+  }
+}
+
+template <int M>
+void crweno_launch_m(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                     double* fR, int dir, int* err, cudaStream_t s) {
+  if (dir == 0) crweno_launch_wt<M, 0>(P, U, F, uL, uR, fL, fR, err, s);
+  else crweno_launch_wt<M, 1>(P, U, F, uL, uR, fL, fR, err, s);
+}
+
+}  // namespace
+
+int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                  double* fR, int dir, int* err, cudaStream_t s) {
+  const int N = dir == 0 ? P.N0 : P.N1;
+  switch (crweno_rows_per_thread(N)) {
+    case 2: crweno_launch_m<2>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    case 4: crweno_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    case 8: crweno_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    case 16: crweno_launch_m<16>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
+    default: return -1;
+  }
+  return 0;
+}
+
+}  // namespace piafs

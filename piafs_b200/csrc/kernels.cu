@@ -3,7 +3,8 @@
 // Per RK stage the host enqueues, for each direction d:
 //   k_flux          cell-centred flux F_d(U) at every point (FFunction)
 //   k_weno5 or      interface values uL,uR,fL,fR (InterpolateInterfacesHyp
-//   k_crweno_line     with the weights of SetInterpLimiterVar fused in)
+//   k_crweno_pair     with the weights of SetInterpLimiterVar fused in;
+//                     crweno.cu)
 //   k_upwind_div    upwind flux at interfaces + conservative difference,
 //                   accumulated into the stage derivative (Upwind +
 //                   HyperbolicFunction's dxinv*(fI[j+1]-fI[j]))
@@ -265,172 +266,6 @@ __global__ void k_weno5(DevParams P, const double* __restrict__ U, const double*
   fL[o] = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
   if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
   fR[o] = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
-}
-
-// ================================================================== CRWENO5
-// Interp1PrimFifthOrderCRWENO (Interp1PrimFifthOrderCRWENO.c:81-240) with the
-// tridiagonal solve of tridiagLU (tridiagLU.c:86-277) replaced by a
-// partitioned solve in the spirit of tridiagLU's own substructuring (its
-// stages 1-4 with "ranks" = threads): one CTA per line, each thread owns M
-// consecutive rows in registers.  The first row of each chunk is a separator;
-// the chunk's other rows are eliminated down and up so that each is
-// x_i = rho_i - alpha_i X_k - gamma_i X_{k+1} in the separators X.  The
-// separator equations form a tridiagonal system with one unknown per thread,
-// solved by parallel cyclic reduction in shared memory; then every row is
-// recovered from its two separators.
-//
-// Rows 0 and N are the WENO5 rows with B = 1 (physical boundaries, also on
-// periodic domains, :164-175); they are solved directly and folded into rows 1
-// and N-1.  Rows past N-1 are identity rows.
-__device__ __forceinline__ void crweno_row(const DevParams& P, const double* fv, int r, int upw,
-                                           double& A, double& B, double& C, double& R) {
-  double m3, m2, m1, p1, p2;
-  if (upw > 0) { m3 = fv[r]; m2 = fv[r + 1]; m1 = fv[r + 2]; p1 = fv[r + 3]; p2 = fv[r + 4]; }
-  else         { m3 = fv[r + 5]; m2 = fv[r + 4]; m1 = fv[r + 3]; p1 = fv[r + 2]; p2 = fv[r + 1]; }
-  double w1, w2, w3;
-  if (P.no_limiting) { w1 = 0.2; w2 = 0.5; w3 = 0.3; }
-  else weno_weights(P.weno_type, 0.2, 0.5, 0.3, m3, m2, m1, p1, p2, P.eps, w1, w2, w3);
-  const double s6 = 1.0 / 6.0, t3 = 1.0 / 3.0;
-  double f1 = s6 * m2 + (5.0 * s6) * m1;
-  double f2 = (5.0 * s6) * m1 + s6 * p1;
-  double f3 = s6 * m1 + (5.0 * s6) * p1;
-  double lo = (2.0 * t3) * w1 + t3 * w2, hi = t3 * w3;
-  B = t3 * w1 + (2.0 * t3) * w2 + (2.0 * t3) * w3;
-  if (upw > 0) { A = lo; C = hi; } else { C = lo; A = hi; }
-  R = w1 * f1 + w2 * f2 + w3 * f3;
-}
-
-// WENO5 boundary row value at interface i (WENO optimal weights)
-__device__ __forceinline__ double crweno_edge(const DevParams& P, const double* src, long long st, int i, int upw) {
-  double m3, m2, m1, p1, p2;
-  if (upw > 0) { m3 = src[(i - 3) * st]; m2 = src[(i - 2) * st]; m1 = src[(i - 1) * st]; p1 = src[i * st]; p2 = src[(i + 1) * st]; }
-  else         { m3 = src[(i + 2) * st]; m2 = src[(i + 1) * st]; m1 = src[i * st]; p1 = src[(i - 1) * st]; p2 = src[(i - 2) * st]; }
-  double w1, w2, w3;
-  if (P.no_limiting) { w1 = 0.1; w2 = 0.6; w3 = 0.3; }
-  else weno_weights(P.weno_type, 0.1, 0.6, 0.3, m3, m2, m1, p1, p2, P.eps, w1, w2, w3);
-  return weno5_value(w1, w2, w3, m3, m2, m1, p1, p2);
-}
-
-template <int M, int DIR>
-__global__ void __launch_bounds__(256) k_crweno_line(DevParams P, const double* __restrict__ U,
-                                                      const double* __restrict__ F, double* __restrict__ uL,
-                                                      double* __restrict__ uR, double* __restrict__ fL,
-                                                      double* __restrict__ fR, int lines_per_block,
-                                                      int* __restrict__ err) {
-  static_assert(M >= 2, "a chunk needs a separator and at least one interior row");
-  extern __shared__ double sm[];
-  const int Pt = blockDim.x, k = threadIdx.x;
-  double* pa = sm;            // PCR buffers [2][4][Pt]
-  double* tp = sm + 8 * Pt;   // last-row spikes published per chunk [3][Pt]
-  double* sy = sm + 11 * Pt;  // separator values [Pt]
-  const int v = blockIdx.y;
-  const int N = DIR == 0 ? P.N0 : P.N1;
-  const int nlines = DIR == 0 ? P.N1 : P.N0;
-  const long long st = DIR == 0 ? 1 : P.W0;
-  const long long ist = DIR == 0 ? 1 : P.N0;
-  const int s = 1 + k * M;                       // separator row of this thread
-  const int kN = (N - 2) / M;                    // thread owning row N-1
-  for (int lc = 0; lc < lines_per_block; lc++) {
-    const int line = blockIdx.x * lines_per_block + lc;
-    if (line >= nlines) break;
-    const long long base = DIR == 0 ? pidx(P, 0, line) : pidx(P, line, 0);
-    const long long ibase = DIR == 0 ? (long long)(P.N0 + 1) * line : line;
-    for (int sys = 0; sys < 4; sys++) {
-      const int upw = (sys & 1) ? -1 : 1;
-      const double* src = (sys < 2 ? U : F) + (long long)v * P.ps + base;
-      double* out = (sys == 0 ? uL : sys == 1 ? uR : sys == 2 ? fL : fR) + (long long)v * P.pis + ibase;
-      double fv[M + 5];
-#pragma unroll
-      for (int r = 0; r < M + 5; r++) {
-        const int c = s - 3 + r;
-        fv[r] = (c <= N + 2) ? src[c * st] : 0.0;
-      }
-      double x0 = 0.0, xN = 0.0;
-      if (k == 0) x0 = crweno_edge(P, src, st, 0, upw);
-      if (k == kN) xN = crweno_edge(P, src, st, N, upw);
-      // ---- rows; the separator row r = 0 is kept as built
-      double As = 0.0, Bs = 1.0, Cs = 0.0, Rs = 0.0;
-      double al[M], be[M], cc[M], rh[M], rb[M];
-      int bad = 0;
-#pragma unroll
-      for (int r = 0; r < M; r++) {
-        const int i = s + r;
-        double A = 0.0, B = 1.0, C = 0.0, R = 0.0;
-        if (i <= N - 1) {
-          crweno_row(P, fv, r, upw, A, B, C, R);
-          if (i == 1) { R -= A * x0; A = 0.0; }
-          if (i == N - 1) { R -= C * xN; C = 0.0; }
-        }
-        if (r == 0) { As = A; Bs = B; Cs = C; Rs = R; continue; }
-        // downward elimination of the interior rows, spike on the separator X_k
-        if (r == 1) { al[1] = A; be[1] = B; rh[1] = R; }
-        else {
-          const double f = A * rb[r - 1];
-          be[r] = B - f * cc[r - 1];
-          al[r] = -f * al[r - 1];
-          rh[r] = R - f * rh[r - 1];
-        }
-        cc[r] = C;
-        bad |= (be[r] == 0.0);
-        rb[r] = 1.0 / be[r];
-      }
-      // ---- upward elimination, normalised: x_{s+r} = rh - al X_k - cc X_{k+1}
-      al[M - 1] *= rb[M - 1]; rh[M - 1] *= rb[M - 1]; cc[M - 1] *= rb[M - 1];
-#pragma unroll
-      for (int r = M - 2; r >= 1; r--) {
-        const double c = cc[r];
-        al[r] = (al[r] - c * al[r + 1]) * rb[r];
-        rh[r] = (rh[r] - c * rh[r + 1]) * rb[r];
-        cc[r] = -(c * cc[r + 1]) * rb[r];
-      }
-      if (bad) atomicOr(err, 1);
-      tp[k] = al[M - 1]; tp[Pt + k] = cc[M - 1]; tp[2 * Pt + k] = rh[M - 1];
-      __syncthreads();
-      // ---- separator equation: As x_{s-1} + Bs X_k + Cs x_{s+1} = Rs with
-      //      x_{s-1} = rho_p - alpha_p X_{k-1} - gamma_p X_k (previous chunk's
-      //      last row) and x_{s+1} = rh[1] - al[1] X_k - cc[1] X_{k+1}
-      double alp = 0.0, gap = 0.0, rhp = 0.0;
-      if (k > 0) { alp = tp[k - 1]; gap = tp[Pt + k - 1]; rhp = tp[2 * Pt + k - 1]; }
-      {
-        double a = -(As * alp);
-        double b = Bs - As * gap - Cs * al[1];
-        double c = -(Cs * cc[1]);
-        double d = Rs - As * rhp - Cs * rh[1];
-        int buf = 0;
-        pa[k] = a; pa[Pt + k] = b; pa[2 * Pt + k] = c; pa[3 * Pt + k] = d;
-        __syncthreads();
-        for (int dl = 1; dl < Pt; dl <<= 1) {
-          const double* cur = pa + buf * 4 * Pt;
-          double* nxt = pa + (buf ^ 1) * 4 * Pt;
-          double am = 0.0, bm = 1.0, cm = 0.0, dm = 0.0, ap = 0.0, bp = 1.0, cp = 0.0, dp = 0.0;
-          if (k - dl >= 0) { am = cur[k - dl]; bm = cur[Pt + k - dl]; cm = cur[2 * Pt + k - dl]; dm = cur[3 * Pt + k - dl]; }
-          if (k + dl < Pt) { ap = cur[k + dl]; bp = cur[Pt + k + dl]; cp = cur[2 * Pt + k + dl]; dp = cur[3 * Pt + k + dl]; }
-          const double alpha = -a / bm, gamma = -c / bp;
-          a = alpha * am;
-          c = gamma * cp;
-          b = b + alpha * cm + gamma * ap;
-          d = d + alpha * dm + gamma * dp;
-          nxt[k] = a; nxt[Pt + k] = b; nxt[2 * Pt + k] = c; nxt[3 * Pt + k] = d;
-          buf ^= 1;
-          __syncthreads();
-        }
-        sy[k] = d / b;
-      }
-      __syncthreads();
-      // ---- recover every row
-      const double Xk = sy[k];
-      const double Xn = k + 1 < Pt ? sy[k + 1] : 0.0;
-      if (s <= N - 1) out[s * ist] = Xk;
-#pragma unroll
-      for (int r = 1; r < M; r++) {
-        const int i = s + r;
-        if (i <= N - 1) out[i * ist] = rh[r] - al[r] * Xk - cc[r] * Xn;
-      }
-      if (k == 0) out[0] = x0;
-      if (k == kN) out[(long long)N * ist] = xN;
-      __syncthreads();   // shared buffers are reused by the next system
-    }
-  }
 }
 
 // ============================================================ upwind + div
@@ -737,6 +572,14 @@ __global__ void k_first_deriv(DevParams P, double* __restrict__ Df, const double
 // ================================================================ launchers
 static inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
+__global__ void k_reciprocal(const double* __restrict__ x, double* __restrict__ y, long long n) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) y[i] = rcp_nr(x[i]);
+}
+void launch_reciprocal(const double* x, double* y, long long n, cudaStream_t s) {
+  k_reciprocal<<<nblk(n, 256), 256, 0, s>>>(x, y, n);
+}
+
 void launch_aos_to_soa(const double* aos, double* soa, long long npg, int nv, long long ps, cudaStream_t s) {
   k_aos_to_soa<<<nblk(npg * nv, 256), 256, 0, s>>>(aos, soa, npg, nv, ps);
 }
@@ -792,55 +635,13 @@ void launch_weno5(const DevParams& P, const double* U, const double* F, double* 
   else k_weno5<1><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
 }
 
-// rows per thread of the partitioned line solve: the smallest M that keeps a
-// line within one 256-thread CTA (lines of up to 4097 interfaces)
-int crweno_rows_per_thread(int N) {
-  const int rows = N - 1;
-  const int cand[4] = {2, 4, 8, 16};
-  for (int c = 0; c < 4; c++)
-    if ((rows + cand[c] - 1) / cand[c] <= 256) return cand[c];
-  return -1;
-}
-
-template <int M>
-static void crweno_launch_m(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                            double* fR, int dir, int* err, cudaStream_t s) {
-  const int N = dir == 0 ? P.N0 : P.N1;
-  const int nlines = dir == 0 ? P.N1 : P.N0;
-  int Pt = (N - 1 + M - 1) / M;
-  Pt = ((Pt + 31) / 32) * 32;
-  const int lpb = dir == 0 ? 1 : 4;
-  dim3 grid((nlines + lpb - 1) / lpb, P.nvars);
-  size_t smem = (size_t)12 * Pt * sizeof(double);
-  if (dir == 0) k_crweno_line<M, 0><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, lpb, err);
-  else k_crweno_line<M, 1><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, lpb, err);
-}
-
-int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                  double* fR, int dir, int* err, cudaStream_t s) {
-  const int N = dir == 0 ? P.N0 : P.N1;
-  const int M = crweno_rows_per_thread(N);
-  switch (M) {
-    case 2: crweno_launch_m<2>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
-    case 4: crweno_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
-    case 8: crweno_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
-    case 16: crweno_launch_m<16>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
-    default: return -1;
-  }
-  return 0;
-}
-
 template <int MODEL, int UPW>
 static void upwind_div_dir(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
                            const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
   // the interface-flux tile holds nvars x (tile + 1) doubles: allow more than
   // the 48 KB default for many-species decks
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_upwind_div<MODEL, UPW, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_upwind_div<MODEL, UPW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr = true;
-  }
+  raise_smem_limit<k_upwind_div<MODEL, UPW, 0>>(200 * 1024);
+  raise_smem_limit<k_upwind_div<MODEL, UPW, 1>>(200 * 1024);
   if (dir == 0) {
     dim3 grid(nblk(P.N0, 128), P.N1), blk(128, 1);
     size_t smem = (size_t)P.nvars * 129 * sizeof(double);

@@ -1,9 +1,22 @@
 // Launcher interface of the device kernels (kernels.cu).
 #pragma once
+#include <atomic>
 #include <cuda_runtime.h>
 #include "common.cuh"
 
 namespace piafs {
+
+// Raise a kernel's dynamic shared-memory limit, once per device.
+template <auto Kernel>
+inline void raise_smem_limit(int bytes) {
+  static std::atomic<unsigned long long> done{0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (done.load() & bit) return;
+  cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done.fetch_or(bit);
+}
 
 // One boundary zone with its index extents resolved (single rank):
 // [is[d], ie[d]) per dimension, ghost slab along `dim`
@@ -29,6 +42,7 @@ void launch_cfl(const DevParams& P, const double* u, const double* dxinv, unsign
 void launch_flux(const DevParams& P, const double* U, double* F, int dir, cudaStream_t s);
 void launch_weno5(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
                   double* fR, int dir, cudaStream_t s);
+// CRWENO5 interface values (crweno.cu); -1 if a line is too long
 int crweno_rows_per_thread(int N);
 int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
                   double* fR, int dir, int* err, cudaStream_t s);
@@ -42,6 +56,7 @@ void launch_upwind_iface(const DevParams& P, const double* U, const double* uL, 
                          const double* fR, double* fI, int dir, cudaStream_t s);
 void launch_first_deriv(const DevParams& P, double* Df, const double* f, int dir, int bias, int nv, cudaStream_t s);
 void launch_advance_time(double* tdev, double dt, cudaStream_t s);
+void launch_reciprocal(const double* x, double* y, long long n, cudaStream_t s);
 void launch_tridiag(double* a, double* b, double* c, double* x, int n, int ns, int* err, cudaStream_t s);
 
 }  // namespace piafs
