@@ -48,6 +48,8 @@ struct piafs_gpu_sim {
   double* fC = nullptr;
   double* iface[5] = {nullptr};            // uL, uR, fL, fR, operator scratch
   double* scratch = nullptr;               // ghosted plane set for operator calls
+  double* ut = nullptr;                    // transposed state of the y-direction CRWENO5 pass
+  DevParams PT;                            // the transposed grid
   double* dxinv = nullptr;
   double* imap = nullptr;
   double* tdev = nullptr;                  // simulation time on the device
@@ -76,6 +78,7 @@ static void free_sim(piafs_gpu_sim* s) {
   cudaFree(s->fC);
   for (auto p : s->iface) cudaFree(p);
   cudaFree(s->scratch);
+  cudaFree(s->ut);
   cudaFree(s->dxinv);
   cudaFree(s->imap);
   cudaFree(s->tdev);
@@ -89,20 +92,41 @@ static void free_sim(piafs_gpu_sim* s) {
 }
 
 // -------------------------------------------------------------- the RHS
+// One direction of the hyperbolic term: cell-centred flux, interface values,
+// upwinding and the conservative difference into rhs (mode as in
+// launch_upwind_div).  The y-direction CRWENO5 pass of a 2D run works on a
+// transposed copy of U so that its lines, the tridiagonal systems, are
+// contiguous in memory; the result lands in rhs in the standard layout.  If
+// `ev` is given, an event is recorded after each of the three phases.
+static void enqueue_hyp_dir(piafs_gpu_sim* s, const double* U, double* rhs, int d, int mode,
+                            cudaEvent_t* ev = nullptr, int* k = nullptr) {
+  const DevParams& P = s->P;
+  double* const* I = s->iface;
+  auto mark = [&]() { if (ev) cudaEventRecord(ev[++*k], s->stream); };
+  if (d == 1 && s->ut) {
+    launch_transpose(P, U, s->ut, s->stream);
+    launch_flux(P, s->ut, s->fC, 1, s->stream);
+    mark();
+    launch_crweno(s->PT, s->ut, s->fC, I[0], I[1], I[2], I[3], 0, s->err, s->stream);
+    mark();
+    launch_upwind_div_t(P, s->ut, I[0], I[1], I[2], I[3], s->dxinv, rhs, mode, s->stream);
+    mark();
+    return;
+  }
+  launch_flux(P, U, s->fC, d, s->stream);
+  mark();
+  if (P.scheme == WENO5) launch_weno5(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
+  else launch_crweno(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->err, s->stream);
+  mark();
+  launch_upwind_div(P, U, I[0], I[1], I[2], I[3], s->dxinv, rhs, d, mode, s->stream);
+  mark();
+}
+
 // TimeRHSFunctionExplicit (TimeRHSFunctionExplicit.c:29-77) on SoA arrays:
 // rhs = -hyp + par + source; U must have its ghosts filled.
 static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const double* tdev, double cstage) {
-  const DevParams& P = s->P;
-  for (int d = 0; d < P.ndims; d++) {
-    launch_flux(P, U, s->fC, d, s->stream);
-    if (P.scheme == WENO5)
-      launch_weno5(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->stream);
-    else
-      launch_crweno(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->err, s->stream);
-    launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, rhs, d, d == 0 ? 0 : 1,
-                      s->stream);
-  }
-  launch_visc_source(P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream);
+  for (int d = 0; d < s->P.ndims; d++) enqueue_hyp_dir(s, U, rhs, d, d == 0 ? 0 : 1);
+  launch_visc_source(s->P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream);
 }
 
 static void enqueue_bc(piafs_gpu_sim* s, double* u) {
@@ -208,6 +232,13 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   if (e == cudaSuccess) e = alloc(&s->fC, planes);
   for (int k = 0; k < 5 && e == cudaSuccess; k++) e = alloc(&s->iface[k], iplanes);
   if (e == cudaSuccess) e = alloc(&s->scratch, planes);
+  // transposed y pass: 2D CRWENO5 (PIAFS_GPU_NO_YTRANSPOSE=1 keeps the
+  // column-strided kernels instead)
+  const char* noyt = std::getenv("PIAFS_GPU_NO_YTRANSPOSE");
+  if (e == cudaSuccess && P.ndims == 2 && P.scheme == CRWENO5 && !(noyt && noyt[0] == '1')) {
+    e = alloc(&s->ut, planes);
+    s->PT = transposed_params(P);
+  }
   if (e == cudaSuccess) e = alloc(&s->dxinv, d.dxinv.size());
   if (e == cudaSuccess) e = alloc(&s->imap, d.imap.size());
   if (e == cudaSuccess) e = alloc(&s->tdev, 1);
@@ -252,10 +283,12 @@ int piafs_gpu_get_info(piafs_gpu_sim* s, piafs_gpu_info* info) {
   info->ninterfaces[0] = s->P.nint[0]; info->ninterfaces[1] = s->P.nint[1];
   info->cfl = s->last_cfl; info->norm = s->last_norm; info->singular = s->singular;
   // kernels per step: prestep BCs, per stage (combine + BCs for s > 0, three
-  // per direction, viscous/source), update, clock
+  // per direction plus the transpose of the y pass, viscous/source), update,
+  // clock
   const int nz = (int)d.zones.size();
   const int vs = ((s->P.ndims == 2 && s->P.viscous) || s->P.chem) ? 1 : 0;
-  info->launches_per_step = nz + d.nstages * (3 * s->P.ndims + vs) + (d.nstages - 1) * (1 + nz) + 2;
+  const int tr = s->ut ? 1 : 0;
+  info->launches_per_step = nz + d.nstages * (3 * s->P.ndims + tr + vs) + (d.nstages - 1) * (1 + nz) + 2;
   return PIAFS_OK;
 }
 
@@ -344,18 +377,7 @@ int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) 
     enqueue_bc(s, U);
     int k = 0;
     CK(cudaEventRecord(ev[0], s->stream));
-    for (int d = 0; d < P.ndims; d++) {
-      launch_flux(P, U, s->fC, d, s->stream);
-      CK(cudaEventRecord(ev[++k], s->stream));
-      if (P.scheme == WENO5)
-        launch_weno5(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->stream);
-      else
-        launch_crweno(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->err, s->stream);
-      CK(cudaEventRecord(ev[++k], s->stream));
-      launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, R, d, d == 0 ? 0 : 1,
-                        s->stream);
-      CK(cudaEventRecord(ev[++k], s->stream));
-    }
+    for (int d = 0; d < P.ndims; d++) enqueue_hyp_dir(s, U, R, d, d == 0 ? 0 : 1, ev.data(), &k);
     launch_visc_source(P, U, s->dxinv, s->imap, s->tdev, 0.0, R, 1, 1, s->stream);
     CK(cudaEventRecord(ev[++k], s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -465,15 +487,7 @@ int piafs_gpu_HyperbolicFunction(piafs_gpu_sim* s, double* hyp, const double* u,
   double* H = s->Ud[0];
   to_soa(s, u, U);
   CK(cudaMemsetAsync(H, 0, (size_t)P.nvars * P.ps * sizeof(double), s->stream));
-  for (int d = 0; d < P.ndims; d++) {
-    launch_flux(P, U, s->fC, d, s->stream);
-    if (P.scheme == WENO5)
-      launch_weno5(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->stream);
-    else
-      launch_crweno(P, U, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], d, s->err, s->stream);
-    launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, H, d, d == 0 ? 2 : 3,
-                      s->stream);
-  }
+  for (int d = 0; d < P.ndims; d++) enqueue_hyp_dir(s, U, H, d, d == 0 ? 2 : 3);
   launch_soa_to_aos(H, hyp, P.npg, P.nvars, P.ps, s->stream);
   return finish(s);
 }

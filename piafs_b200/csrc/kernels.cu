@@ -70,6 +70,27 @@ __global__ void k_iface_soa_to_aos(const double* __restrict__ soa, double* __res
   aos[idx] = soa[v * pis + q];
 }
 
+// Plane-wise transpose of a ghosted state: in[v][j][i] (i fastest, W0 x W1)
+// to out[v][i][j] (j fastest), through 32 x 32 shared-memory tiles.  The
+// y-direction CRWENO5 pass runs on the transposed copy so that its lines are
+// contiguous in memory.
+__global__ void k_transpose_planes(const double* __restrict__ in, double* __restrict__ out, int W0, int W1,
+                                   long long ps) {
+  __shared__ double tile[32][33];
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const double* a = in + blockIdx.z * ps;
+  double* b = out + blockIdx.z * ps;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int i = i0 + threadIdx.x, j = j0 + r;
+    if (i < W0 && j < W1) tile[r][threadIdx.x] = a[(long long)j * W0 + i];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int j = j0 + threadIdx.x, i = i0 + r;
+    if (i < W0 && j < W1) b[(long long)i * W1 + j] = tile[threadIdx.x][r];
+  }
+}
+
 // ================================================================ boundaries
 // One zone of ApplyBoundaryConditions: BCPeriodicU (BCPeriodic.c:22-62),
 // BCExtrapolateU (BCExtrapolate.c:16-50), BCSlipWallU (BCSlipWall.c:24-136).
@@ -340,6 +361,62 @@ __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* _
   }
 }
 
+// y-direction upwind + divergence on the transposed copy: UT holds the
+// state with j fastest (pidx of the transposed grid) and the interface arrays
+// hold column i's N1+1 interfaces contiguously, q = j + (N1+1) i.  The result
+// goes to rhs in the standard layout with the same modes as k_upwind_div.
+// Tile: 32 cells along y x 8 columns; the divergence phase maps consecutive
+// threads to consecutive columns so that the rhs accesses come in 64-byte runs.
+template <int UPW>
+__global__ void __launch_bounds__(256) k_upwind_div_t(DevParams P, const double* __restrict__ UT,
+                                                      const double* __restrict__ uL, const double* __restrict__ uR,
+                                                      const double* __restrict__ fL, const double* __restrict__ fR,
+                                                      const double* __restrict__ dxinv, double* __restrict__ rhs,
+                                                      int mode) {
+  extern __shared__ double sfi[];
+  constexpr int NF = Flow<NS2D>::NF, TJ = 32, TI = 8, LJ = TJ + 1;
+  const int nvars = P.nvars, N0 = P.N0, N1 = P.N1, g = P.ghosts, W1 = P.W1;
+  const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+  const int tid = threadIdx.x;
+  const int vs = LJ * TI;
+  const double gam = P.gamma;
+  for (int e = tid; e < vs; e += 256) {
+    const int jj = e % LJ, li = e / LJ;
+    const int j = j0 + jj, i = i0 + li;
+    if (j > N1 || i >= N0) continue;
+    const long long q = (long long)(N1 + 1) * i + j;
+    const long long pR = (long long)(j + g) + (long long)W1 * (i + g), pL = pR - 1;
+    double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
+    int spm;
+#pragma unroll
+    for (int m = 0; m < NF; m++) {
+      a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
+      c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
+      if (UPW != UPW_LLF) { ucl[m] = UT[m * P.ps + pL]; ucr[m] = UT[m * P.ps + pR]; }
+    }
+    upwind_flow<NS2D, UPW, double>(a, b, c, d, ucl, ucr, gam, 1, fi, &spa, &spm);
+    double* so = sfi + e;
+#pragma unroll
+    for (int m = 0; m < NF; m++) so[m * vs] = fi[m];
+    for (int m = NF; m < nvars; m++)
+      so[m * vs] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q], fR[m * P.pis + q]);
+  }
+  __syncthreads();
+  const int li = tid % TI, jj = tid / TI;
+  const int i = i0 + li, j = j0 + jj;
+  if (i >= N0 || j >= N1) return;
+  const long long p = pidx(P, i, j);
+  const double dxi = dxinv[P.W0 + g + j];
+  for (int m = 0; m < nvars; m++) {
+    const double h = dxi * (sfi[m * vs + li * LJ + jj + 1] - sfi[m * vs + li * LJ + jj]);
+    double* r = rhs + (long long)m * P.ps + p;
+    if (mode == 0) *r = -h;
+    else if (mode == 1) *r = -((-*r) + h);
+    else if (mode == 2) *r = h;
+    else *r = *r + h;
+  }
+}
+
 // ===================================================== viscous + chemistry
 // NavierStokes2DParabolicFunction (NavierStokes2DParabolicFunction.c:41-204)
 // with FirstDerivativeFirstOrder (bias +1 on Q, -1 on the fluxes), fused with
@@ -598,6 +675,17 @@ void launch_iface_aos_to_soa(const double* aos, double* soa, long long ni, int n
 void launch_iface_soa_to_aos(const double* soa, double* aos, long long ni, int nv, long long pis, cudaStream_t s) {
   k_iface_soa_to_aos<<<nblk(ni * nv, 256), 256, 0, s>>>(soa, aos, ni, nv, pis);
 }
+void launch_transpose(const DevParams& P, const double* in, double* out, cudaStream_t s) {
+  dim3 grid(nblk(P.W0, 32), nblk(P.W1, 32), P.nvars), blk(32, 8);
+  k_transpose_planes<<<grid, blk, 0, s>>>(in, out, P.W0, P.W1, P.ps);
+}
+DevParams transposed_params(const DevParams& P) {
+  DevParams T = P;
+  T.N0 = P.N1; T.N1 = P.N0;
+  T.W0 = P.W1; T.W1 = P.W0;
+  T.nint[0] = P.nint[1]; T.nint[1] = P.nint[0];
+  return T;
+}
 void launch_bc(const DevParams& P, double* u, const Zone& z, cudaStream_t s) {
   long long n = (long long)(z.ie[0] - z.is[0]) * (z.ie[1] - z.is[1]);
   if (n <= 0) return;
@@ -669,6 +757,25 @@ void launch_upwind_div(const DevParams& P, const double* U, const double* uL, co
                        const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
   if (P.model == NS2D) upwind_div_model<NS2D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
   else upwind_div_model<EULER1D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
+}
+
+template <int UPW>
+static void upwind_div_t_u(const DevParams& P, const double* UT, const double* uL, const double* uR,
+                           const double* fL, const double* fR, const double* dxinv, double* rhs, int mode,
+                           cudaStream_t s) {
+  raise_smem_limit<k_upwind_div_t<UPW>>(200 * 1024);
+  dim3 grid(nblk(P.N1, 32), nblk(P.N0, 8));
+  size_t smem = (size_t)P.nvars * 33 * 8 * sizeof(double);
+  k_upwind_div_t<UPW><<<grid, 256, smem, s>>>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode);
+}
+void launch_upwind_div_t(const DevParams& P, const double* UT, const double* uL, const double* uR, const double* fL,
+                         const double* fR, const double* dxinv, double* rhs, int mode, cudaStream_t s) {
+  switch (P.upwind) {
+    case UPW_ROE: upwind_div_t_u<UPW_ROE>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
+    case UPW_RF: upwind_div_t_u<UPW_RF>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
+    case UPW_RUSANOV: upwind_div_t_u<UPW_RUSANOV>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
+    default: upwind_div_t_u<UPW_LLF>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
+  }
 }
 
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,

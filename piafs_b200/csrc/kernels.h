@@ -34,6 +34,10 @@ void launch_interior_to_soa(const DevParams& P, const double* in, double* soa, c
 void launch_iface_aos_to_soa(const double* aos, double* soa, long long ni, int nv, long long pis, cudaStream_t s);
 void launch_iface_soa_to_aos(const double* soa, double* aos, long long ni, int nv, long long pis, cudaStream_t s);
 void launch_bc(const DevParams& P, double* u, const Zone& z, cudaStream_t s);
+// 2D only: plane-wise transpose of a ghosted state (j fastest in `out`) and
+// the parameters that describe the transposed grid (dimensions swapped)
+void launch_transpose(const DevParams& P, const double* in, double* out, cudaStream_t s);
+DevParams transposed_params(const DevParams& P);
 void launch_stage(long long n, double* Us, const double* u, const double* const* d, const double* a, int nterms,
                   cudaStream_t s);
 void launch_update(const DevParams& P, double* u, const double* const* d, const double* b, int ns, double* norm_acc,
@@ -49,6 +53,10 @@ int launch_crweno(const DevParams& P, const double* U, const double* F, double* 
 // mode 0: rhs = -hyp_x; 1: rhs = -((-rhs) + hyp_y); 2: out = hyp_x; 3: out += hyp_y
 void launch_upwind_div(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
                        const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s);
+// y-direction upwind + divergence from the transposed state UT and interface
+// arrays of the transposed grid (NS2D), into rhs in the standard layout
+void launch_upwind_div_t(const DevParams& P, const double* UT, const double* uL, const double* uR, const double* fL,
+                         const double* fR, const double* dxinv, double* rhs, int mode, cudaStream_t s);
 // rhs += par (if do_visc) then rhs += source (if do_chem)
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
                         const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s);
