@@ -108,9 +108,10 @@ int piafs_gpu_synchronize(piafs_gpu_sim* sim);
 /* Time each kernel phase of one right-hand-side evaluation on the current
  * state with CUDA events on the simulation's stream, averaged over `reps`
  * evaluations.  ms[k] receives the mean duration of phase k; phases are, per
- * direction d = 0..ndims-1, [3d] flux, [3d+1] interface reconstruction
- * (WENO5 or the CRWENO5 line solve), [3d+2] upwinding + divergence, then
- * [3 ndims] viscous + source.  nphases (in/out) is the capacity / count. */
+ * direction d = 0..ndims-1, [2d] flux (with the transpose of a transposed
+ * y pass), [2d+1] interface reconstruction (WENO5 or the CRWENO5 line
+ * solve), then [2 ndims] upwinding + divergence of all directions and
+ * [2 ndims + 1] viscous + source.  nphases (in/out) is the capacity / count. */
 int piafs_gpu_profile_rhs(piafs_gpu_sim* sim, int reps, double* ms, int* nphases);
 
 /* max CFL of the current state (NavierStokes2DComputeCFL.c /

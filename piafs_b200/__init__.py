@@ -237,8 +237,8 @@ class Simulation:
         _check(_lib.piafs_gpu_profile_rhs(self._h, int(reps), ms, C.byref(n)))
         names = []
         for d in range(self.info["ndims"]):
-            names += [f"flux_{'xy'[d]}", f"reconstruct_{'xy'[d]}", f"upwind_div_{'xy'[d]}"]
-        names.append("viscous_source")
+            names += [f"flux_{'xy'[d]}", f"reconstruct_{'xy'[d]}"]
+        names += ["upwind_div", "viscous_source"]
         return dict(zip(names, list(ms)[: n.value]))
 
     def solve(self, output_dir: Optional[str] = None):

@@ -47,6 +47,7 @@ struct piafs_gpu_sim {
   double* Ud[MAX_STAGES] = {nullptr};
   double* fC = nullptr;
   double* iface[5] = {nullptr};            // uL, uR, fL, fR, operator scratch
+  double* iface_y[4] = {nullptr};          // uL, uR, fL, fR of the y direction (2D)
   double* scratch = nullptr;               // ghosted plane set for operator calls
   double* ut = nullptr;                    // transposed state of the y-direction CRWENO5 pass
   DevParams PT;                            // the transposed grid
@@ -77,6 +78,7 @@ static void free_sim(piafs_gpu_sim* s) {
   for (auto p : s->Ud) cudaFree(p);
   cudaFree(s->fC);
   for (auto p : s->iface) cudaFree(p);
+  for (auto p : s->iface_y) cudaFree(p);
   cudaFree(s->scratch);
   cudaFree(s->ut);
   cudaFree(s->dxinv);
@@ -92,24 +94,19 @@ static void free_sim(piafs_gpu_sim* s) {
 }
 
 // -------------------------------------------------------------- the RHS
-// One direction of the hyperbolic term: cell-centred flux, interface values,
-// upwinding and the conservative difference into rhs (mode as in
-// launch_upwind_div).  The y-direction CRWENO5 pass of a 2D run works on a
-// transposed copy of U so that its lines, the tridiagonal systems, are
-// contiguous in memory; the result lands in rhs in the standard layout.  If
-// `ev` is given, an event is recorded after each of the three phases.
-static void enqueue_hyp_dir(piafs_gpu_sim* s, const double* U, double* rhs, int d, int mode,
-                            cudaEvent_t* ev = nullptr, int* k = nullptr) {
+// Cell-centred flux and interface values (uL, uR, fL, fR into I) of
+// direction d.  The y pass of a 2D CRWENO5 run works on a transposed copy of
+// U so that its lines, the tridiagonal systems, are contiguous in memory; its
+// interface arrays are then in the transposed layout.  If `ev` is given, an
+// event is recorded after the flux and after the reconstruction.
+static void enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* const* I, cudaEvent_t* ev, int* k) {
   const DevParams& P = s->P;
-  double* const* I = s->iface;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[++*k], s->stream); };
   if (d == 1 && s->ut) {
     launch_transpose(P, U, s->ut, s->stream);
     launch_flux(P, s->ut, s->fC, 1, s->stream);
     mark();
     launch_crweno(s->PT, s->ut, s->fC, I[0], I[1], I[2], I[3], 0, s->err, s->stream);
-    mark();
-    launch_upwind_div_t(P, s->ut, I[0], I[1], I[2], I[3], s->dxinv, rhs, mode, s->stream);
     mark();
     return;
   }
@@ -118,14 +115,30 @@ static void enqueue_hyp_dir(piafs_gpu_sim* s, const double* U, double* rhs, int 
   if (P.scheme == WENO5) launch_weno5(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
   else launch_crweno(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->err, s->stream);
   mark();
-  launch_upwind_div(P, U, I[0], I[1], I[2], I[3], s->dxinv, rhs, d, mode, s->stream);
-  mark();
+}
+
+// HyperbolicFunction (HyperbolicFunction.c:35-119) over all directions into
+// out: -hyp (neg, the stage derivative's first term) or hyp.  In 2D both
+// directions' interfaces are reconstructed first and one kernel upwinds them
+// and forms the divergence.
+static void enqueue_hyp(piafs_gpu_sim* s, const double* U, double* out, bool neg, cudaEvent_t* ev = nullptr,
+                        int* k = nullptr) {
+  const DevParams& P = s->P;
+  enqueue_recon(s, U, 0, s->iface, ev, k);
+  if (P.ndims == 1) {
+    launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, out, 0, neg ? 0 : 2,
+                      s->stream);
+  } else {
+    enqueue_recon(s, U, 1, s->iface_y, ev, k);
+    launch_upwind_div2d(P, U, s->ut, s->iface, s->iface_y, s->dxinv, out, neg ? 1 : 0, s->stream);
+  }
+  if (ev) cudaEventRecord(ev[++*k], s->stream);
 }
 
 // TimeRHSFunctionExplicit (TimeRHSFunctionExplicit.c:29-77) on SoA arrays:
 // rhs = -hyp + par + source; U must have its ghosts filled.
 static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const double* tdev, double cstage) {
-  for (int d = 0; d < s->P.ndims; d++) enqueue_hyp_dir(s, U, rhs, d, d == 0 ? 0 : 1);
+  enqueue_hyp(s, U, rhs, true);
   launch_visc_source(s->P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream);
 }
 
@@ -231,6 +244,7 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   for (int k = 0; k < d.nstages && e == cudaSuccess; k++) e = alloc(&s->Ud[k], planes);
   if (e == cudaSuccess) e = alloc(&s->fC, planes);
   for (int k = 0; k < 5 && e == cudaSuccess; k++) e = alloc(&s->iface[k], iplanes);
+  for (int k = 0; k < 4 && e == cudaSuccess && P.ndims == 2; k++) e = alloc(&s->iface_y[k], iplanes);
   if (e == cudaSuccess) e = alloc(&s->scratch, planes);
   // transposed y pass: 2D CRWENO5 (PIAFS_GPU_NO_YTRANSPOSE=1 keeps the
   // column-strided kernels instead)
@@ -282,13 +296,13 @@ int piafs_gpu_get_info(piafs_gpu_sim* s, piafs_gpu_info* info) {
   info->npoints_ghosted = s->P.npg;
   info->ninterfaces[0] = s->P.nint[0]; info->ninterfaces[1] = s->P.nint[1];
   info->cfl = s->last_cfl; info->norm = s->last_norm; info->singular = s->singular;
-  // kernels per step: prestep BCs, per stage (combine + BCs for s > 0, three
-  // per direction plus the transpose of the y pass, viscous/source), update,
-  // clock
+  // kernels per step: prestep BCs, per stage (combine + BCs for s > 0, flux
+  // and reconstruction per direction plus the transpose of a transposed y
+  // pass, one upwind/divergence kernel, viscous/source), update, clock
   const int nz = (int)d.zones.size();
   const int vs = ((s->P.ndims == 2 && s->P.viscous) || s->P.chem) ? 1 : 0;
   const int tr = s->ut ? 1 : 0;
-  info->launches_per_step = nz + d.nstages * (3 * s->P.ndims + tr + vs) + (d.nstages - 1) * (1 + nz) + 2;
+  info->launches_per_step = nz + d.nstages * (2 * s->P.ndims + 1 + tr + vs) + (d.nstages - 1) * (1 + nz) + 2;
   return PIAFS_OK;
 }
 
@@ -365,7 +379,7 @@ int piafs_gpu_synchronize(piafs_gpu_sim* s) {
 int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) {
   if (!s || !ms || !nphases || reps < 1) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
   const DevParams& P = s->P;
-  const int np = 3 * P.ndims + 1;
+  const int np = P.ndims == 1 ? 4 : 6;
   if (*nphases < np) return fail(PIAFS_ERR_ARGUMENT, "ms[] too small");
   *nphases = np;
   std::vector<cudaEvent_t> ev(np + 1);
@@ -377,7 +391,7 @@ int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) 
     enqueue_bc(s, U);
     int k = 0;
     CK(cudaEventRecord(ev[0], s->stream));
-    for (int d = 0; d < P.ndims; d++) enqueue_hyp_dir(s, U, R, d, d == 0 ? 0 : 1, ev.data(), &k);
+    enqueue_hyp(s, U, R, true, ev.data(), &k);
     launch_visc_source(P, U, s->dxinv, s->imap, s->tdev, 0.0, R, 1, 1, s->stream);
     CK(cudaEventRecord(ev[++k], s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -487,7 +501,7 @@ int piafs_gpu_HyperbolicFunction(piafs_gpu_sim* s, double* hyp, const double* u,
   double* H = s->Ud[0];
   to_soa(s, u, U);
   CK(cudaMemsetAsync(H, 0, (size_t)P.nvars * P.ps * sizeof(double), s->stream));
-  for (int d = 0; d < P.ndims; d++) enqueue_hyp_dir(s, U, H, d, d == 0 ? 2 : 3);
+  enqueue_hyp(s, U, H, false);
   launch_soa_to_aos(H, hyp, P.npg, P.nvars, P.ps, s->stream);
   return finish(s);
 }

@@ -361,59 +361,93 @@ __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* _
   }
 }
 
-// y-direction upwind + divergence on the transposed copy: UT holds the
-// state with j fastest (pidx of the transposed grid) and the interface arrays
-// hold column i's N1+1 interfaces contiguously, q = j + (N1+1) i.  The result
-// goes to rhs in the standard layout with the same modes as k_upwind_div.
-// Tile: 32 cells along y x 8 columns; the divergence phase maps consecutive
-// threads to consecutive columns so that the rhs accesses come in 64-byte runs.
-template <int UPW>
-__global__ void __launch_bounds__(256) k_upwind_div_t(DevParams P, const double* __restrict__ UT,
-                                                      const double* __restrict__ uL, const double* __restrict__ uR,
-                                                      const double* __restrict__ fL, const double* __restrict__ fR,
+// Upwind flux of all components at one interface q of direction DIR into
+// so[m * sm_stride] (NavierStokes2DUpwind*); cells pL / pR are the cells left
+// and right of the interface in `cells`.
+template <int UPW, int DIR>
+__device__ __forceinline__ void iface_upwind(const DevParams& P, const double* __restrict__ uL,
+                                             const double* __restrict__ uR, const double* __restrict__ fL,
+                                             const double* __restrict__ fR, long long q,
+                                             const double* __restrict__ cells, long long pL, long long pR,
+                                             double* so, int sm_stride) {
+  constexpr int NF = Flow<NS2D>::NF;
+  double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
+  int spm;
+#pragma unroll
+  for (int m = 0; m < NF; m++) {
+    a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
+    c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
+    if (UPW != UPW_LLF) { ucl[m] = cells[m * P.ps + pL]; ucr[m] = cells[m * P.ps + pR]; }
+  }
+  upwind_flow<NS2D, UPW, double>(a, b, c, d, ucl, ucr, P.gamma, DIR, fi, &spa, &spm);
+#pragma unroll
+  for (int m = 0; m < NF; m++) so[m * sm_stride] = fi[m];
+  for (int m = NF; m < P.nvars; m++)
+    so[m * sm_stride] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q],
+                                       fR[m * P.pis + q]);
+}
+
+// Both directions of the 2D hyperbolic term in one pass: upwind fluxes at the
+// x and y interfaces of a 16 x 15 tile (one of each per thread), then
+// hyp = dxinv_x (fIx[i+1] - fIx[i]) + dxinv_y (fIy[j+1] - fIy[j])
+// (HyperbolicFunction.c:97-112, the x term first) and rhs = -hyp (neg = 1,
+// TimeRHSFunctionExplicit.c:64-66) or out = hyp (neg = 0): the same sum, in
+// the same order, that the per-direction kernels accumulate, with the stage
+// derivative written once.  The y-interface arrays are in the transposed
+// layout (q = j + (N1+1) i, cell values from UT) when YT, else in the
+// standard one (q = i + N0 j, cell values from U).
+template <int UPW, bool YT>
+__global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double* __restrict__ U,
+                                                      const double* __restrict__ UT,
+                                                      const double* __restrict__ xuL, const double* __restrict__ xuR,
+                                                      const double* __restrict__ xfL, const double* __restrict__ xfR,
+                                                      const double* __restrict__ yuL, const double* __restrict__ yuR,
+                                                      const double* __restrict__ yfL, const double* __restrict__ yfR,
                                                       const double* __restrict__ dxinv, double* __restrict__ rhs,
-                                                      int mode) {
-  extern __shared__ double sfi[];
-  constexpr int NF = Flow<NS2D>::NF, TJ = 32, TI = 8, LJ = TJ + 1;
-  const int nvars = P.nvars, N0 = P.N0, N1 = P.N1, g = P.ghosts, W1 = P.W1;
-  const int j0 = blockIdx.x * TJ, i0 = blockIdx.y * TI;
+                                                      int neg) {
+  extern __shared__ double sf[];
+  constexpr int TI = 16, TJ = 15, LX = TI + 1, LY = TJ + 2;   // LY padded against bank conflicts
+  constexpr int NX = LX * TJ, NY = TI * LY;
+  const int nvars = P.nvars, N0 = P.N0, N1 = P.N1, g = P.ghosts;
+  const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
   const int tid = threadIdx.x;
-  const int vs = LJ * TI;
-  const double gam = P.gamma;
-  for (int e = tid; e < vs; e += 256) {
-    const int jj = e % LJ, li = e / LJ;
-    const int j = j0 + jj, i = i0 + li;
-    if (j > N1 || i >= N0) continue;
-    const long long q = (long long)(N1 + 1) * i + j;
-    const long long pR = (long long)(j + g) + (long long)W1 * (i + g), pL = pR - 1;
-    double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
-    int spm;
-#pragma unroll
-    for (int m = 0; m < NF; m++) {
-      a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
-      c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
-      if (UPW != UPW_LLF) { ucl[m] = UT[m * P.ps + pL]; ucr[m] = UT[m * P.ps + pR]; }
+  double* sx = sf;               // x-interface fluxes [m][row jj][ii = 0..TI]
+  double* sy = sf + nvars * NX;  // y-interface fluxes [m][column ii][jj = 0..TJ]
+  if (tid < NX) {                // (TI + 1) x TJ x-interfaces
+    const int ii = tid % LX, jj = tid / LX;
+    const int i = i0 + ii, j = j0 + jj;
+    if (i <= N0 && j < N1) {
+      const long long pR = pidx(P, i, j);
+      iface_upwind<UPW, 0>(P, xuL, xuR, xfL, xfR, i + (long long)(N0 + 1) * j, U, pR - 1, pR, sx + jj * LX + ii, NX);
     }
-    upwind_flow<NS2D, UPW, double>(a, b, c, d, ucl, ucr, gam, 1, fi, &spa, &spm);
-    double* so = sfi + e;
-#pragma unroll
-    for (int m = 0; m < NF; m++) so[m * vs] = fi[m];
-    for (int m = NF; m < nvars; m++)
-      so[m * vs] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q], fR[m * P.pis + q]);
+  }
+  {                              // TI x (TJ + 1) y-interfaces
+    int ii, jj;
+    if (YT) { jj = tid % (TJ + 1); ii = tid / (TJ + 1); }
+    else { ii = tid % TI; jj = tid / TI; }
+    const int i = i0 + ii, j = j0 + jj;
+    if (j <= N1 && i < N0) {
+      if (YT) {
+        const long long pR = (long long)(j + g) + (long long)P.W1 * (i + g);
+        iface_upwind<UPW, 1>(P, yuL, yuR, yfL, yfR, j + (long long)(N1 + 1) * i, UT, pR - 1, pR, sy + ii * LY + jj, NY);
+      } else {
+        const long long pR = pidx(P, i, j);
+        iface_upwind<UPW, 1>(P, yuL, yuR, yfL, yfR, i + (long long)N0 * j, U, pR - P.W0, pR, sy + ii * LY + jj, NY);
+      }
+    }
   }
   __syncthreads();
-  const int li = tid % TI, jj = tid / TI;
-  const int i = i0 + li, j = j0 + jj;
+  if (tid >= TI * TJ) return;
+  const int ii = tid % TI, jj = tid / TI;
+  const int i = i0 + ii, j = j0 + jj;
   if (i >= N0 || j >= N1) return;
   const long long p = pidx(P, i, j);
-  const double dxi = dxinv[P.W0 + g + j];
+  const double dxi = dxinv[g + i], dyi = dxinv[P.W0 + g + j];
   for (int m = 0; m < nvars; m++) {
-    const double h = dxi * (sfi[m * vs + li * LJ + jj + 1] - sfi[m * vs + li * LJ + jj]);
-    double* r = rhs + (long long)m * P.ps + p;
-    if (mode == 0) *r = -h;
-    else if (mode == 1) *r = -((-*r) + h);
-    else if (mode == 2) *r = h;
-    else *r = *r + h;
+    const double hx = dxi * (sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii]);
+    const double hy = dyi * (sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
+    const double h = hx + hy;
+    rhs[(long long)m * P.ps + p] = neg ? -h : h;
   }
 }
 
@@ -759,23 +793,29 @@ void launch_upwind_div(const DevParams& P, const double* U, const double* uL, co
   else upwind_div_model<EULER1D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
 }
 
-template <int UPW>
-static void upwind_div_t_u(const DevParams& P, const double* UT, const double* uL, const double* uR,
-                           const double* fL, const double* fR, const double* dxinv, double* rhs, int mode,
-                           cudaStream_t s) {
-  raise_smem_limit<k_upwind_div_t<UPW>>(200 * 1024);
-  dim3 grid(nblk(P.N1, 32), nblk(P.N0, 8));
-  size_t smem = (size_t)P.nvars * 33 * 8 * sizeof(double);
-  k_upwind_div_t<UPW><<<grid, 256, smem, s>>>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode);
+template <int UPW, bool YT>
+static void upwind_div2d_u(const DevParams& P, const double* U, const double* UT, const double* const* xi,
+                           const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
+  raise_smem_limit<k_upwind_div2d<UPW, YT>>(200 * 1024);
+  dim3 grid(nblk(P.N0, 16), nblk(P.N1, 15));
+  size_t smem = (size_t)P.nvars * (17 * 15 + 16 * 17) * sizeof(double);
+  k_upwind_div2d<UPW, YT><<<grid, 256, smem, s>>>(P, U, UT, xi[0], xi[1], xi[2], xi[3], yi[0], yi[1], yi[2], yi[3],
+                                                   dxinv, rhs, neg);
 }
-void launch_upwind_div_t(const DevParams& P, const double* UT, const double* uL, const double* uR, const double* fL,
-                         const double* fR, const double* dxinv, double* rhs, int mode, cudaStream_t s) {
+template <bool YT>
+static void upwind_div2d_yt(const DevParams& P, const double* U, const double* UT, const double* const* xi,
+                            const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
   switch (P.upwind) {
-    case UPW_ROE: upwind_div_t_u<UPW_ROE>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
-    case UPW_RF: upwind_div_t_u<UPW_RF>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
-    case UPW_RUSANOV: upwind_div_t_u<UPW_RUSANOV>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
-    default: upwind_div_t_u<UPW_LLF>(P, UT, uL, uR, fL, fR, dxinv, rhs, mode, s); break;
+    case UPW_ROE: upwind_div2d_u<UPW_ROE, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    case UPW_RF: upwind_div2d_u<UPW_RF, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    case UPW_RUSANOV: upwind_div2d_u<UPW_RUSANOV, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    default: upwind_div2d_u<UPW_LLF, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
   }
+}
+void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const double* const* xi,
+                         const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
+  if (UT) upwind_div2d_yt<true>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+  else upwind_div2d_yt<false>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
 }
 
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,

@@ -53,10 +53,11 @@ int launch_crweno(const DevParams& P, const double* U, const double* F, double* 
 // mode 0: rhs = -hyp_x; 1: rhs = -((-rhs) + hyp_y); 2: out = hyp_x; 3: out += hyp_y
 void launch_upwind_div(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
                        const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s);
-// y-direction upwind + divergence from the transposed state UT and interface
-// arrays of the transposed grid (NS2D), into rhs in the standard layout
-void launch_upwind_div_t(const DevParams& P, const double* UT, const double* uL, const double* uR, const double* fL,
-                         const double* fR, const double* dxinv, double* rhs, int mode, cudaStream_t s);
+// both directions of a 2D hyperbolic term in one pass: xi / yi are the
+// (uL, uR, fL, fR) interface arrays of x and y; y in the transposed layout
+// with cell values from UT when UT is given.  rhs = -hyp (neg) or hyp.
+void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const double* const* xi,
+                         const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
 // rhs += par (if do_visc) then rhs += source (if do_chem)
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
                         const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s);
