@@ -67,7 +67,13 @@ const char* piafs_gpu_last_error(void);
  * current CUDA device.  Replaces the reference's ReadInputs, Initialize,
  * InitialSolution, InitializeBoundaries, InitializeSolvers and
  * InitializePhysics (src/main.cpp:126-212).  `precision` is one of
- * PIAFS_PRECISION_*. */
+ * PIAFS_PRECISION_*: FP64 throughout, or MIXED -- FP32 reconstruction
+ * weights and rows, upwind fluxes, viscous stencils and chemistry source on
+ * the FP64 conserved state, FP64 RK stage accumulation and FP64 tridiagonal
+ * solves.  In the mixed path the time step, RHSFunction, HyperbolicFunction,
+ * ParabolicFunction and SourceFunction use the mixed kernels; the lower-level
+ * operator entry points (FFunction, InterpolateInterfacesHyp, Upwind,
+ * FirstDerivativePar) stay FP64. */
 int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** sim);
 void piafs_gpu_destroy(piafs_gpu_sim* sim);
 int piafs_gpu_get_info(piafs_gpu_sim* sim, piafs_gpu_info* info);

@@ -130,7 +130,9 @@ static void enqueue_hyp(piafs_gpu_sim* s, const double* U, double* out, bool neg
                       s->stream);
   } else {
     enqueue_recon(s, U, 1, s->iface_y, ev, k);
-    launch_upwind_div2d(P, U, s->ut, s->iface, s->iface_y, s->dxinv, out, neg ? 1 : 0, s->stream);
+    const void* xi[4] = {s->iface[0], s->iface[1], s->iface[2], s->iface[3]};
+    const void* yi[4] = {s->iface_y[0], s->iface_y[1], s->iface_y[2], s->iface_y[3]};
+    launch_upwind_div2d(P, U, s->ut, xi, yi, s->dxinv, out, neg ? 1 : 0, s->stream);
   }
   if (ev) cudaEventRecord(ev[++*k], s->stream);
 }
@@ -219,14 +221,15 @@ const char* piafs_gpu_last_error(void) { return g_err.c_str(); }
 int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   if (!deck_dir || !out) return fail(PIAFS_ERR_ARGUMENT, "null argument");
   *out = nullptr;
-  if (precision != PIAFS_PRECISION_FP64)
-    return fail(PIAFS_ERR_UNSUPPORTED, "only the FP64 path is available in this build");
+  if (precision != PIAFS_PRECISION_FP64 && precision != PIAFS_PRECISION_MIXED)
+    return fail(PIAFS_ERR_ARGUMENT, "precision must be PIAFS_PRECISION_FP64 or PIAFS_PRECISION_MIXED");
   auto* s = new piafs_gpu_sim();
   std::string err;
   int r = read_deck(deck_dir, s->deck, err);
   if (!r) r = make_params(s->deck, s->P, err);
   if (r) { delete s; return fail(r, err); }
   s->precision = precision;
+  s->P.mixed = precision == PIAFS_PRECISION_MIXED ? 1 : 0;
   const char* ng = std::getenv("PIAFS_GPU_NO_GRAPH");
   s->use_graph = !(ng && ng[0] == '1');
   const DevParams& P = s->P;
@@ -247,9 +250,10 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   for (int k = 0; k < 4 && e == cudaSuccess && P.ndims == 2; k++) e = alloc(&s->iface_y[k], iplanes);
   if (e == cudaSuccess) e = alloc(&s->scratch, planes);
   // transposed y pass: 2D CRWENO5 (PIAFS_GPU_NO_YTRANSPOSE=1 keeps the
-  // column-strided kernels instead)
+  // column-strided kernels instead in the FP64 path; the mixed path has only
+  // the transposed one)
   const char* noyt = std::getenv("PIAFS_GPU_NO_YTRANSPOSE");
-  if (e == cudaSuccess && P.ndims == 2 && P.scheme == CRWENO5 && !(noyt && noyt[0] == '1')) {
+  if (e == cudaSuccess && P.ndims == 2 && P.scheme == CRWENO5 && (P.mixed || !(noyt && noyt[0] == '1'))) {
     e = alloc(&s->ut, planes);
     s->PT = transposed_params(P);
   }
@@ -544,7 +548,8 @@ int piafs_gpu_FFunction(piafs_gpu_sim* s, double* f, const double* u, int dir, d
 int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* s, double* fI, const double* fC, const double* u, int upw,
                                        int dir, int uflag) {
   if (!s || !fI || !fC || !u || dir < 0 || dir >= s->P.ndims) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
-  const DevParams& P = s->P;
+  DevParams P = s->P;
+  P.mixed = 0;   // operator-level entry points are FP64
   to_soa(s, u, s->scratch);
   to_soa(s, fC, s->fC);
   if (P.scheme == WENO5)

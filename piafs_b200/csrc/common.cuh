@@ -41,6 +41,7 @@ struct DevParams {
   double k[11], q[11];
   double chem_gamma, I0, ch_c, ch_h, ch_nu, n_O2, t_start_norm, t_pulse_norm, sO3, dz;
   double dt;
+  int mixed;             // 1: FP32 inner arithmetic on FP64 state (mixed precision)
 };
 
 __host__ __device__ inline long long pidx(const DevParams& P, int i, int j) {
@@ -126,6 +127,13 @@ __device__ __forceinline__ double rcp_nr(double x) {
   y = fma(y, e, y);
   e = fma(-x, y, 1.0);
   return fma(y, e, y);
+}
+// FP32 reciprocal of the mixed-precision inner arithmetic: the hardware
+// approximation of PTX rcp.approx.ftz.f32 (within about 1 ulp of FP32).
+__device__ __forceinline__ float rcp_nr(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 #endif
 

@@ -27,6 +27,8 @@
 // they are computed directly and folded into rows 1 and N-1.  Rows past N-1
 // are identity rows.  Divisions are reciprocals by Newton-Raphson refinement
 // (rcp_nr), so results agree with the reference to rounding, not bit for bit.
+#include <type_traits>
+
 #include "kernels.h"
 
 namespace piafs {
@@ -38,31 +40,30 @@ constexpr int WT_NOLIM = 4;   // no_limiting: optimal weights everywhere
 // Nonlinear CRWENO5 weights (optimal weights 0.2, 0.5, 0.3) from the three
 // smoothness indicators of one stencil; tau is the WENO-Z / Yamaleev-Carpenter
 // reference indicator (interpolation.h:255-545).
-template <int WT>
-__device__ __forceinline__ void crw_weights(double b1, double b2, double b3, double tau, double eps, double& w1,
-                                            double& w2, double& w3) {
-  constexpr double c1 = 0.2, c2 = 0.5, c3 = 0.3;
+template <int WT, typename R>
+__device__ __forceinline__ void crw_weights(R b1, R b2, R b3, R tau, R eps, R& w1, R& w2, R& w3) {
+  constexpr R c1 = R(0.2), c2 = R(0.5), c3 = R(0.3);
   if (WT == WT_NOLIM) {
     w1 = c1; w2 = c2; w3 = c3;
   } else if (WT == W_JS || WT == W_MAPPED) {
     // c_k/q_k / sum_m c_m/q_m with q = (beta + eps)^2, as c_k prod_{m!=k} q_m / sum
-    const double s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
-    const double q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
-    const double a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
-    const double inv = rcp_nr(a1 + a2 + a3);
+    const R s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
+    const R q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
+    const R a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
+    const R inv = rcp_nr(a1 + a2 + a3);
     w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
     if (WT == W_MAPPED) {   // Henrick-Aslam-Powers mapping
-      const double x1 = w1, x2 = w2, x3 = w3;
-      const double A1 = x1 * (c1 + c1 * c1 - 3.0 * c1 * x1 + x1 * x1) * rcp_nr(c1 * c1 + x1 * (1.0 - 2.0 * c1));
-      const double A2 = x2 * (c2 + c2 * c2 - 3.0 * c2 * x2 + x2 * x2) * rcp_nr(c2 * c2 + x2 * (1.0 - 2.0 * c2));
-      const double A3 = x3 * (c3 + c3 * c3 - 3.0 * c3 * x3 + x3 * x3) * rcp_nr(c3 * c3 + x3 * (1.0 - 2.0 * c3));
-      const double inv2 = rcp_nr(A1 + A2 + A3);
+      const R x1 = w1, x2 = w2, x3 = w3;
+      const R A1 = x1 * (c1 + c1 * c1 - R(3) * c1 * x1 + x1 * x1) * rcp_nr(c1 * c1 + x1 * (R(1) - R(2) * c1));
+      const R A2 = x2 * (c2 + c2 * c2 - R(3) * c2 * x2 + x2 * x2) * rcp_nr(c2 * c2 + x2 * (R(1) - R(2) * c2));
+      const R A3 = x3 * (c3 + c3 * c3 - R(3) * c3 * x3 + x3 * x3) * rcp_nr(c3 * c3 + x3 * (R(1) - R(2) * c3));
+      const R inv2 = rcp_nr(A1 + A2 + A3);
       w1 = A1 * inv2; w2 = A2 * inv2; w3 = A3 * inv2;
     }
   } else {
-    const double r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
-    const double a1 = c1 * (1.0 + r1 * r1), a2 = c2 * (1.0 + r2 * r2), a3 = c3 * (1.0 + r3 * r3);
-    const double inv = rcp_nr(a1 + a2 + a3);
+    const R r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
+    const R a1 = c1 * (R(1) + r1 * r1), a2 = c2 * (R(1) + r2 * r2), a3 = c3 * (R(1) + r3 * r3);
+    const R inv = rcp_nr(a1 + a2 + a3);
     w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
   }
 }
@@ -79,18 +80,40 @@ __device__ __forceinline__ double crw_edge(const DevParams& P, const double* src
   return weno5_value(w1, w2, w3, m3, m2, m1, p1, p2);
 }
 
+// the same on values taken relative to `ref`, in FP32 (mixed precision)
+__device__ __forceinline__ float crw_edge_f(const DevParams& P, const double* src, long long st, int i, int upw,
+                                            double ref) {
+  auto at = [&](int c) { return (float)(src[c * st] - ref); };
+  float m3, m2, m1, p1, p2;
+  if (upw > 0) { m3 = at(i - 3); m2 = at(i - 2); m1 = at(i - 1); p1 = at(i); p2 = at(i + 1); }
+  else         { m3 = at(i + 2); m2 = at(i + 1); m1 = at(i); p1 = at(i - 1); p2 = at(i - 2); }
+  float w1, w2, w3;
+  if (P.no_limiting) { w1 = 0.1f; w2 = 0.6f; w3 = 0.3f; }
+  else weno_weights(P.weno_type, 0.1f, 0.6f, 0.3f, m3, m2, m1, p1, p2, (float)P.eps, w1, w2, w3);
+  return weno5_value(w1, w2, w3, m3, m2, m1, p1, p2);
+}
+
 // padded index into the output staging buffer (conflict-free for the strided
 // writes of the recovery and the unit-stride reads of the store)
 __device__ __forceinline__ int stg(int i) { return i + (i >> 4); }
 
 }  // namespace
 
-template <int M, int DIR, int WT>
+// MX (mixed precision): the cells are taken relative to the line's first
+// interior value (FP64 subtraction, then FP32), the weights and the rows are
+// built in FP32, the elimination and the separator solve run in FP64, and the
+// interface values are stored in FP32 relative to that same reference.  The
+// reconstruction reproduces constants, so the shift is exact in exact
+// arithmetic; it keeps O(1) backgrounds out of the FP32 rounding, and the
+// upwind/divergence kernel that reads these values only differences them
+// along the line or adds the reference back.
+template <int M, int DIR, int WT, bool MX>
 __global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
-    k_crweno_pair(DevParams P, const double* __restrict__ U, const double* __restrict__ F, double* __restrict__ uL,
-                  double* __restrict__ uR, double* __restrict__ fL, double* __restrict__ fR,
-                  int* __restrict__ err) {
+    k_crweno_pair(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
+                  void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
   static_assert(M >= 2, "a chunk needs a separator and at least one interior row");
+  typedef typename std::conditional<MX, float, double>::type R;   // row arithmetic
+  typedef typename std::conditional<MX, float, double>::type O;   // interface storage
   extern __shared__ double sm[];
   const int Pt = blockDim.x, k = threadIdx.x;
   double* pc = sm;               // PCR rows, [2 buffers][2 biases][a, c, d][Pt]
@@ -105,42 +128,48 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
   const long long base = DIR == 0 ? pidx(P, 0, line) : pidx(P, line, 0);
   const long long ibase = DIR == 0 ? (long long)(P.N0 + 1) * line : line;
   const double* src = (isF ? F : U) + (long long)v * P.ps + base;
-  double* oL = (isF ? fL : uL) + (long long)v * P.pis + ibase;
-  double* oR = (isF ? fR : uR) + (long long)v * P.pis + ibase;
+  O* oL = (O*)(isF ? fL : uL) + (long long)v * P.pis + ibase;
+  O* oR = (O*)(isF ? fR : uR) + (long long)v * P.pis + ibase;
   const int s = 1 + k * M;          // separator row (interface) of this thread
   const int kN = (N - 2) / M;       // thread owning row N-1
-  const double eps = P.eps;
+  const R eps = (R)P.eps;
+  const double ref = MX ? src[0] : 0.0;
 
   // cells s-3 .. s+M+1
-  double c[M + 5];
+  R c[M + 5];
 #pragma unroll
   for (int r = 0; r < M + 5; r++) {
     const int cell = s - 3 + r;
-    c[r] = cell <= N + 2 ? src[cell * st] : 0.0;
+    c[r] = cell <= N + 2 ? (R)(src[cell * st] - ref) : R(0);
   }
-  double x0[2] = {0.0, 0.0}, xN[2] = {0.0, 0.0};
-  if (k == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
-  if (k == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
+  R x0[2] = {R(0), R(0)}, xN[2] = {R(0), R(0)};
+  if (MX) {
+    if (k == 0) { x0[0] = crw_edge_f(P, src, st, 0, 1, ref); x0[1] = crw_edge_f(P, src, st, 0, -1, ref); }
+    if (k == kN) { xN[0] = crw_edge_f(P, src, st, N, 1, ref); xN[1] = crw_edge_f(P, src, st, N, -1, ref); }
+  } else {
+    if (k == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
+    if (k == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
+  }
 
   // smoothness indicators of the windows centred at cells s-2+t (t = 0..M+2):
   // b1: 13/12 d^2 + 1/4 (a-4b+3c)^2, b2: .. (a-c)^2, b3: .. (3a-4b+c)^2
-  double b1[M + 3], b2[M + 3], b3[M + 3];
+  R b1[M + 3], b2[M + 3], b3[M + 3];
   if (WT != WT_NOLIM) {
 #pragma unroll
     for (int t = 0; t < M + 3; t++) {
-      const double a = c[t], b = c[t + 1], cc = c[t + 2];
-      const double d = a - 2.0 * b + cc;
-      const double e1 = a - 4.0 * b + 3.0 * cc, e2 = a - cc, e3 = 3.0 * a - 4.0 * b + cc;
-      const double dd = (13.0 / 12.0) * d * d;
-      b1[t] = dd + 0.25 * e1 * e1;
-      b2[t] = dd + 0.25 * e2 * e2;
-      b3[t] = dd + 0.25 * e3 * e3;
+      const R a = c[t], b = c[t + 1], cc = c[t + 2];
+      const R d = a - R(2) * b + cc;
+      const R e1 = a - R(4) * b + R(3) * cc, e2 = a - cc, e3 = R(3) * a - R(4) * b + cc;
+      const R dd = R(13.0 / 12.0) * d * d;
+      b1[t] = dd + R(0.25) * e1 * e1;
+      b2[t] = dd + R(0.25) * e2 * e2;
+      b3[t] = dd + R(0.25) * e3 * e3;
     }
   }
   // two-cell averages of the compact right-hand side, cells (s-3+j, s-2+j):
   // pp = 5/6 left + 1/6 right, qq = 1/6 left + 5/6 right
-  constexpr double s6 = 1.0 / 6.0, s56 = 5.0 * (1.0 / 6.0);
-  double pp[M + 3], qq[M + 3];
+  constexpr R s6 = R(1.0 / 6.0), s56 = R(5.0 * (1.0 / 6.0));
+  R pp[M + 3], qq[M + 3];
 #pragma unroll
   for (int j = 1; j < M + 3; j++) {
     pp[j] = s56 * c[j] + s6 * c[j + 1];
@@ -156,36 +185,37 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
     const int i = s + r;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      double A = 0.0, B = 1.0, C = 0.0, R = 0.0;
+      R Ar = R(0), Br = R(1), Cr = R(0), Rr = R(0);
       if (i <= N - 1) {
-        double w1, w2, w3, f1, f2, f3, tau = 0.0;
+        R w1, w2, w3, f1, f2, f3, tau = R(0);
         if (q == 0) {
           if (WT == W_BORGES) tau = fabs(b3[r + 2] - b1[r]);
-          if (WT == W_YC) { const double t4 = c[r] - 4.0 * c[r + 1] + 6.0 * c[r + 2] - 4.0 * c[r + 3] + c[r + 4]; tau = t4 * t4; }
-          crw_weights<WT>(b1[r], b2[r + 1], b3[r + 2], tau, eps, w1, w2, w3);
+          if (WT == W_YC) { const R t4 = c[r] - R(4) * c[r + 1] + R(6) * c[r + 2] - R(4) * c[r + 3] + c[r + 4]; tau = t4 * t4; }
+          crw_weights<WT, R>(b1[r], b2[r + 1], b3[r + 2], tau, eps, w1, w2, w3);
           f1 = qq[r + 1]; f2 = pp[r + 2]; f3 = qq[r + 2];
         } else {
           if (WT == W_BORGES) tau = fabs(b1[r + 1] - b3[r + 3]);
-          if (WT == W_YC) { const double t4 = c[r + 5] - 4.0 * c[r + 4] + 6.0 * c[r + 3] - 4.0 * c[r + 2] + c[r + 1]; tau = t4 * t4; }
-          crw_weights<WT>(b3[r + 3], b2[r + 2], b1[r + 1], tau, eps, w1, w2, w3);
+          if (WT == W_YC) { const R t4 = c[r + 5] - R(4) * c[r + 4] + R(6) * c[r + 3] - R(4) * c[r + 2] + c[r + 1]; tau = t4 * t4; }
+          crw_weights<WT, R>(b3[r + 3], b2[r + 2], b1[r + 1], tau, eps, w1, w2, w3);
           f1 = pp[r + 3]; f2 = qq[r + 2]; f3 = pp[r + 2];
         }
-        constexpr double t3 = 1.0 / 3.0;
-        const double lo = (2.0 * t3) * w1 + t3 * w2, hi = t3 * w3;
-        B = t3 * w1 + (2.0 * t3) * w2 + (2.0 * t3) * w3;
-        A = q == 0 ? lo : hi;
-        C = q == 0 ? hi : lo;
-        R = w1 * f1 + w2 * f2 + w3 * f3;
-        if (i == 1) { R -= A * x0[q]; A = 0.0; }
-        if (i == N - 1) { R -= C * xN[q]; C = 0.0; }
+        constexpr R t3 = R(1.0 / 3.0), t23 = R(2.0 * (1.0 / 3.0));
+        const R lo = t23 * w1 + t3 * w2, hi = t3 * w3;
+        Br = t3 * w1 + t23 * w2 + t23 * w3;
+        Ar = q == 0 ? lo : hi;
+        Cr = q == 0 ? hi : lo;
+        Rr = w1 * f1 + w2 * f2 + w3 * f3;
+        if (i == 1) { Rr -= Ar * x0[q]; Ar = R(0); }
+        if (i == N - 1) { Rr -= Cr * xN[q]; Cr = R(0); }
       }
-      if (r == 0) { As[q] = A; Bs[q] = B; Cs[q] = C; Rs[q] = R; continue; }
+      const double A = Ar, B = Br, C = Cr, Rv = Rr;
+      if (r == 0) { As[q] = A; Bs[q] = B; Cs[q] = C; Rs[q] = Rv; continue; }
       // rows scaled to a unit diagonal: x_r + cg_r x_{r+1} = rh_r - al_r X_k
       const double be = r == 1 ? B : B - A * cg[q][r - 1];
       bad |= (be == 0.0);
       const double rb = rcp_nr(be);
-      if (r == 1) { al[q][1] = A * rb; rh[q][1] = R * rb; }
-      else { al[q][r] = -(A * al[q][r - 1]) * rb; rh[q][r] = (R - A * rh[q][r - 1]) * rb; }
+      if (r == 1) { al[q][1] = A * rb; rh[q][1] = Rv * rb; }
+      else { al[q][r] = -(A * al[q][r - 1]) * rb; rh[q][r] = (Rv - A * rh[q][r - 1]) * rb; }
       cg[q][r] = C * rb;
     }
   }
@@ -267,8 +297,8 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
   }
   __syncthreads();
   for (int i = k; i <= N; i += Pt) {
-    oL[i * ist] = so[stg(i)];
-    oR[i * ist] = so[stg(N) + 1 + stg(i)];
+    oL[i * ist] = (O)so[stg(i)];
+    oR[i * ist] = (O)so[stg(N) + 1 + stg(i)];
   }
 }
 
@@ -284,45 +314,49 @@ int crweno_rows_per_thread(int N) {
 
 namespace {
 
-template <int M, int DIR, int WT>
-void crweno_launch(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                   double* fR, int* err, cudaStream_t s) {
+template <int M, int DIR, int WT, bool MX>
+void crweno_launch(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                   int* err, cudaStream_t s) {
   const int N = DIR == 0 ? P.N0 : P.N1;
   const int nlines = DIR == 0 ? P.N1 : P.N0;
   int Pt = (N - 1 + M - 1) / M;
   Pt = ((Pt + 31) / 32) * 32;
   const size_t smem = (size_t)(20 * Pt + 2 * (N + (N >> 4) + 1)) * sizeof(double);
   // the largest line this M serves: 256 M + 1 interfaces
-  raise_smem_limit<k_crweno_pair<M, DIR, WT>>((20 * 256 + 2 * (256 * M + 2 + ((256 * M + 2) >> 4) + 1)) *
+  raise_smem_limit<k_crweno_pair<M, DIR, WT, MX>>((20 * 256 + 2 * (256 * M + 2 + ((256 * M + 2) >> 4) + 1)) *
                                               (int)sizeof(double));
   dim3 grid(nlines, P.nvars, 2);
-  k_crweno_pair<M, DIR, WT><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, err);
+  k_crweno_pair<M, DIR, WT, MX><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, err);
 }
 
-template <int M, int DIR>
-void crweno_launch_wt(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                      double* fR, int* err, cudaStream_t s) {
-  if (P.no_limiting) return crweno_launch<M, DIR, WT_NOLIM>(P, U, F, uL, uR, fL, fR, err, s);
+template <int M, int DIR, bool MX>
+void crweno_launch_wt(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                      int* err, cudaStream_t s) {
+  if (P.no_limiting) return crweno_launch<M, DIR, WT_NOLIM, MX>(P, U, F, uL, uR, fL, fR, err, s);
   switch (P.weno_type) {
-    case W_MAPPED: return crweno_launch<M, DIR, W_MAPPED>(P, U, F, uL, uR, fL, fR, err, s);
-    case W_BORGES: return crweno_launch<M, DIR, W_BORGES>(P, U, F, uL, uR, fL, fR, err, s);
-    case W_YC: return crweno_launch<M, DIR, W_YC>(P, U, F, uL, uR, fL, fR, err, s);
-    default: return crweno_launch<M, DIR, W_JS>(P, U, F, uL, uR, fL, fR, err, s);
+    case W_MAPPED: return crweno_launch<M, DIR, W_MAPPED, MX>(P, U, F, uL, uR, fL, fR, err, s);
+    case W_BORGES: return crweno_launch<M, DIR, W_BORGES, MX>(P, U, F, uL, uR, fL, fR, err, s);
+    case W_YC: return crweno_launch<M, DIR, W_YC, MX>(P, U, F, uL, uR, fL, fR, err, s);
+    default: return crweno_launch<M, DIR, W_JS, MX>(P, U, F, uL, uR, fL, fR, err, s);
   }
 }
 
+// the mixed-precision path runs x-direction lines only (its y pass always
+// works on the transposed copy)
 template <int M>
-void crweno_launch_m(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                     double* fR, int dir, int* err, cudaStream_t s) {
-  if (dir == 0) crweno_launch_wt<M, 0>(P, U, F, uL, uR, fL, fR, err, s);
-  else crweno_launch_wt<M, 1>(P, U, F, uL, uR, fL, fR, err, s);
+void crweno_launch_m(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                     int dir, int* err, cudaStream_t s) {
+  if (P.mixed) crweno_launch_wt<M, 0, true>(P, U, F, uL, uR, fL, fR, err, s);
+  else if (dir == 0) crweno_launch_wt<M, 0, false>(P, U, F, uL, uR, fL, fR, err, s);
+  else crweno_launch_wt<M, 1, false>(P, U, F, uL, uR, fL, fR, err, s);
 }
 
 }  // namespace
 
-int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                  double* fR, int dir, int* err, cudaStream_t s) {
+int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                  int dir, int* err, cudaStream_t s) {
   const int N = dir == 0 ? P.N0 : P.N1;
+  if (P.mixed && dir != 0) return -1;
   switch (crweno_rows_per_thread(N)) {
     case 2: crweno_launch_m<2>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
     case 4: crweno_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s); break;

@@ -11,6 +11,7 @@
 // then k_visc_source (ParabolicFunction + SourceFunction) and the RK
 // kernels k_stage / k_update (TimeRK).  All state is FP64.
 #include <cstdio>
+#include <type_traits>
 #include "kernels.h"
 #include "physics.cuh"
 
@@ -256,10 +257,14 @@ __device__ __forceinline__ long long cell_of(const DevParams& P, int i, int l) {
 // Interp1PrimFifthOrderWENO (Interp1PrimFifthOrderWENO.c:77-171) for the four
 // (upw, uflag) combinations with the weights of
 // WENOFifthOrderCalculateWeights fused in; one thread per (interface, var).
-template <int DIR>
+// MX (mixed precision): cells relative to the line's first interior value
+// (FP64 subtraction), weights and values in FP32, stored as FP32 relative to
+// that reference, as in the mixed CRWENO5 kernel.
+template <int DIR, bool MX>
 __global__ void k_weno5(DevParams P, const double* __restrict__ U, const double* __restrict__ F,
-                        double* __restrict__ uL, double* __restrict__ uR, double* __restrict__ fL,
-                        double* __restrict__ fR) {
+                        void* __restrict__ uLv, void* __restrict__ uRv, void* __restrict__ fLv,
+                        void* __restrict__ fRv) {
+  typedef typename std::conditional<MX, float, double>::type R;
   const long long ni = P.nint[DIR];
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (idx >= ni * P.nvars) return;
@@ -271,12 +276,18 @@ __global__ void k_weno5(DevParams P, const double* __restrict__ U, const double*
   const long long c0 = cell_of<DIR>(P, i, l);    // cell i (right of the interface)
   const double* u = U + (long long)v * P.ps + c0;
   const double* f = F + (long long)v * P.ps + c0;
-  double a[6], b[6];     // cells i-3 .. i+2
+  double ru = 0.0, rf = 0.0;
+  if (MX) {
+    const long long l0 = cell_of<DIR>(P, 0, l);
+    ru = U[(long long)v * P.ps + l0]; rf = F[(long long)v * P.ps + l0];
+  }
+  R a[6], b[6];     // cells i-3 .. i+2
 #pragma unroll
-  for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * st]; b[r] = f[(r - 3) * st]; }
-  const double c1 = 0.1, c2 = 0.6, c3 = 0.3, eps = P.eps;
-  double w1, w2, w3;
+  for (int r = 0; r < 6; r++) { a[r] = (R)(u[(r - 3) * st] - ru); b[r] = (R)(f[(r - 3) * st] - rf); }
+  const R c1 = R(0.1), c2 = R(0.6), c3 = R(0.3), eps = (R)P.eps;
+  R w1, w2, w3;
   const long long o = (long long)v * P.pis + q;
+  R* uL = (R*)uLv; R* uR = (R*)uRv; R* fL = (R*)fLv; R* fR = (R*)fRv;
   // left-biased: (m3..p2) = cells i-3..i+1 ; right-biased: cells i+2..i-2
   if (P.no_limiting) { w1 = c1; w2 = c2; w3 = c3; }
   else weno_weights(P.weno_type, c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
@@ -296,13 +307,19 @@ __global__ void k_weno5(DevParams P, const double* __restrict__ U, const double*
 // mode 0: rhs = -hyp_x (first direction); 1: rhs <- -((-rhs) + hyp_y);
 // mode 2: out = hyp_x; 3: out <- out + hyp_y (the hyperbolic term alone).
 // Tile: DIR 0: 128 cells of one row; DIR 1: 32 columns x 8 rows.
-template <int MODEL, int UPW, int DIR>
+// MX (mixed precision, 1D): FP32 interface values relative to the line's
+// reference, fluxes in deviation form (upwind_flow_dev), FP32 differences.
+template <int MODEL, int UPW, int DIR, bool MX>
 __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* __restrict__ U,
-                                                    const double* __restrict__ uL, const double* __restrict__ uR,
-                                                    const double* __restrict__ fL, const double* __restrict__ fR,
+                                                    const void* __restrict__ uLv, const void* __restrict__ uRv,
+                                                    const void* __restrict__ fLv, const void* __restrict__ fRv,
                                                     const double* __restrict__ dxinv, double* __restrict__ rhs,
                                                     int mode) {
-  extern __shared__ double sfi[];
+  typedef typename std::conditional<MX, float, double>::type T;
+  extern __shared__ double sfd[];
+  T* sfi = (T*)sfd;
+  const T* uL = (const T*)uLv; const T* uR = (const T*)uRv;
+  const T* fL = (const T*)fLv; const T* fR = (const T*)fRv;
   constexpr int NF = Flow<MODEL>::NF;
   const int TX = DIR == 0 ? 128 : 32, TY = DIR == 0 ? 1 : 8;
   const int TL = DIR == 0 ? TX : TY;             // cells along the line in the tile
@@ -325,16 +342,17 @@ __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* _
     if (i > N || l >= nl) continue;
     const long long q = DIR == 0 ? (long long)i + (long long)(P.N0 + 1) * l : (long long)l + (long long)P.N0 * i;
     const long long pL = cell_of<DIR>(P, i - 1, l), pR = cell_of<DIR>(P, i, l);
-    double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
+    T a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
     int spm;
 #pragma unroll
     for (int m = 0; m < NF; m++) {
       a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
       c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
-      if (UPW != UPW_LLF || MODEL == EULER1D) { ucl[m] = U[m * P.ps + pL]; ucr[m] = U[m * P.ps + pR]; }
+      if (UPW != UPW_LLF || MODEL == EULER1D) { ucl[m] = (T)U[m * P.ps + pL]; ucr[m] = (T)U[m * P.ps + pR]; }
     }
-    upwind_flow<MODEL, UPW, double>(a, b, c, d, ucl, ucr, g, DIR, fi, &spa, &spm);
-    double* so = sfi + (long long)(ii * TW + li);
+    if (MX) upwind_flow_dev<MODEL, UPW, T>(a, b, c, d, a, b, ucl, ucr, (T)g, DIR, fi, &spa, &spm);
+    else upwind_flow<MODEL, UPW, T>(a, b, c, d, ucl, ucr, (T)g, DIR, fi, &spa, &spm);
+    T* so = sfi + (long long)(ii * TW + li);
     const int vs = (TL + 1) * TW;
 #pragma unroll
     for (int m = 0; m < NF; m++) so[m * vs] = fi[m];
@@ -349,10 +367,10 @@ __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* _
   if (i >= N || l >= nl) return;
   const long long p = cell_of<DIR>(P, i, l);
   const int off = DIR == 0 ? 0 : P.W0;
-  const double dxi = dxinv[off + P.ghosts + i];
+  const T dxi = (T)dxinv[off + P.ghosts + i];
   const int vs = (TL + 1) * TW;
   for (int m = 0; m < nvars; m++) {
-    const double h = dxi * (sfi[m * vs + (ii + 1) * TW + li] - sfi[m * vs + ii * TW + li]);
+    const double h = (double)(dxi * (sfi[m * vs + (ii + 1) * TW + li] - sfi[m * vs + ii * TW + li]));
     double* r = rhs + (long long)m * P.ps + p;
     if (mode == 0) *r = -h;
     else if (mode == 1) *r = -((-*r) + h);
@@ -363,23 +381,39 @@ __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* _
 
 // Upwind flux of all components at one interface q of direction DIR into
 // so[m * sm_stride] (NavierStokes2DUpwind*); cells pL / pR are the cells left
-// and right of the interface in `cells`.
-template <int UPW, int DIR>
-__device__ __forceinline__ void iface_upwind(const DevParams& P, const double* __restrict__ uL,
-                                             const double* __restrict__ uR, const double* __restrict__ fL,
-                                             const double* __restrict__ fR, long long q,
+// and right of the interface in `cells`.  MX: the interface arrays hold
+// floats relative to the line's reference values, uref (absolute, FP64) are
+// those references for the flow variables, the flux is computed in FP32 in
+// deviation form and stored relative to the line's flux reference.
+template <int UPW, int DIR, bool MX>
+__device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __restrict__ uLv,
+                                             const void* __restrict__ uRv, const void* __restrict__ fLv,
+                                             const void* __restrict__ fRv, long long q,
                                              const double* __restrict__ cells, long long pL, long long pR,
-                                             double* so, int sm_stride) {
+                                             const double* uref,
+                                             typename std::conditional<MX, float, double>::type* so, int sm_stride) {
+  typedef typename std::conditional<MX, float, double>::type T;
   constexpr int NF = Flow<NS2D>::NF;
-  double a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
+  const T* uL = (const T*)uLv; const T* uR = (const T*)uRv;
+  const T* fL = (const T*)fLv; const T* fR = (const T*)fRv;
+  T a[4], b[4], c[4], d[4], ucl[4], ucr[4], fi[4], spa;
   int spm;
 #pragma unroll
   for (int m = 0; m < NF; m++) {
     a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
     c[m] = fL[m * P.pis + q]; d[m] = fR[m * P.pis + q];
-    if (UPW != UPW_LLF) { ucl[m] = cells[m * P.ps + pL]; ucr[m] = cells[m * P.ps + pR]; }
+    if (UPW != UPW_LLF) { ucl[m] = (T)cells[m * P.ps + pL]; ucr[m] = (T)cells[m * P.ps + pR]; }
   }
-  upwind_flow<NS2D, UPW, double>(a, b, c, d, ucl, ucr, P.gamma, DIR, fi, &spa, &spm);
+  if (MX) {
+    T aL[4], aR[4];
+    if (UPW == UPW_LLF || UPW == UPW_RF) {
+#pragma unroll
+      for (int m = 0; m < NF; m++) { const T r = (T)uref[m]; aL[m] = r + a[m]; aR[m] = r + b[m]; }
+    }
+    upwind_flow_dev<NS2D, UPW, T>(a, b, c, d, aL, aR, ucl, ucr, (T)P.gamma, DIR, fi, &spa, &spm);
+  } else {
+    upwind_flow<NS2D, UPW, T>(a, b, c, d, ucl, ucr, (T)P.gamma, DIR, fi, &spa, &spm);
+  }
 #pragma unroll
   for (int m = 0; m < NF; m++) so[m * sm_stride] = fi[m];
   for (int m = NF; m < P.nvars; m++)
@@ -395,30 +429,41 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const double* _
 // the same order, that the per-direction kernels accumulate, with the stage
 // derivative written once.  The y-interface arrays are in the transposed
 // layout (q = j + (N1+1) i, cell values from UT) when YT, else in the
-// standard one (q = i + N0 j, cell values from U).
-template <int UPW, bool YT>
+// standard one (q = i + N0 j, cell values from U).  MX: mixed precision (FP32
+// interface values relative to their line's reference, FP32 fluxes and
+// differences, FP64 result).
+template <int UPW, bool YT, bool MX>
 __global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double* __restrict__ U,
                                                       const double* __restrict__ UT,
-                                                      const double* __restrict__ xuL, const double* __restrict__ xuR,
-                                                      const double* __restrict__ xfL, const double* __restrict__ xfR,
-                                                      const double* __restrict__ yuL, const double* __restrict__ yuR,
-                                                      const double* __restrict__ yfL, const double* __restrict__ yfR,
+                                                      const void* __restrict__ xuL, const void* __restrict__ xuR,
+                                                      const void* __restrict__ xfL, const void* __restrict__ xfR,
+                                                      const void* __restrict__ yuL, const void* __restrict__ yuR,
+                                                      const void* __restrict__ yfL, const void* __restrict__ yfR,
                                                       const double* __restrict__ dxinv, double* __restrict__ rhs,
                                                       int neg) {
-  extern __shared__ double sf[];
+  typedef typename std::conditional<MX, float, double>::type T;
+  extern __shared__ double sfd[];
+  T* sf = (T*)sfd;
   constexpr int TI = 16, TJ = 15, LX = TI + 1, LY = TJ + 2;   // LY padded against bank conflicts
   constexpr int NX = LX * TJ, NY = TI * LY;
   const int nvars = P.nvars, N0 = P.N0, N1 = P.N1, g = P.ghosts;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
   const int tid = threadIdx.x;
-  double* sx = sf;               // x-interface fluxes [m][row jj][ii = 0..TI]
-  double* sy = sf + nvars * NX;  // y-interface fluxes [m][column ii][jj = 0..TJ]
+  T* sx = sf;               // x-interface fluxes [m][row jj][ii = 0..TI]
+  T* sy = sf + nvars * NX;  // y-interface fluxes [m][column ii][jj = 0..TJ]
+  double uref[4];
   if (tid < NX) {                // (TI + 1) x TJ x-interfaces
     const int ii = tid % LX, jj = tid / LX;
     const int i = i0 + ii, j = j0 + jj;
     if (i <= N0 && j < N1) {
       const long long pR = pidx(P, i, j);
-      iface_upwind<UPW, 0>(P, xuL, xuR, xfL, xfR, i + (long long)(N0 + 1) * j, U, pR - 1, pR, sx + jj * LX + ii, NX);
+      if (MX && (UPW == UPW_LLF || UPW == UPW_RF)) {
+        const long long p0 = pidx(P, 0, j);
+#pragma unroll
+        for (int m = 0; m < 4; m++) uref[m] = U[m * P.ps + p0];
+      }
+      iface_upwind<UPW, 0, MX>(P, xuL, xuR, xfL, xfR, i + (long long)(N0 + 1) * j, U, pR - 1, pR, uref,
+                               sx + jj * LX + ii, NX);
     }
   }
   {                              // TI x (TJ + 1) y-interfaces
@@ -427,12 +472,19 @@ __global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double*
     else { ii = tid % TI; jj = tid / TI; }
     const int i = i0 + ii, j = j0 + jj;
     if (j <= N1 && i < N0) {
+      if (MX && (UPW == UPW_LLF || UPW == UPW_RF)) {
+        const long long p0 = pidx(P, i, 0);
+#pragma unroll
+        for (int m = 0; m < 4; m++) uref[m] = U[m * P.ps + p0];
+      }
       if (YT) {
         const long long pR = (long long)(j + g) + (long long)P.W1 * (i + g);
-        iface_upwind<UPW, 1>(P, yuL, yuR, yfL, yfR, j + (long long)(N1 + 1) * i, UT, pR - 1, pR, sy + ii * LY + jj, NY);
+        iface_upwind<UPW, 1, MX>(P, yuL, yuR, yfL, yfR, j + (long long)(N1 + 1) * i, UT, pR - 1, pR, uref,
+                                 sy + ii * LY + jj, NY);
       } else {
         const long long pR = pidx(P, i, j);
-        iface_upwind<UPW, 1>(P, yuL, yuR, yfL, yfR, i + (long long)N0 * j, U, pR - P.W0, pR, sy + ii * LY + jj, NY);
+        iface_upwind<UPW, 1, MX>(P, yuL, yuR, yfL, yfR, i + (long long)N0 * j, U, pR - P.W0, pR, uref,
+                                 sy + ii * LY + jj, NY);
       }
     }
   }
@@ -442,11 +494,11 @@ __global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double*
   const int i = i0 + ii, j = j0 + jj;
   if (i >= N0 || j >= N1) return;
   const long long p = pidx(P, i, j);
-  const double dxi = dxinv[g + i], dyi = dxinv[P.W0 + g + j];
+  const T dxi = (T)dxinv[g + i], dyi = (T)dxinv[P.W0 + g + j];
   for (int m = 0; m < nvars; m++) {
-    const double hx = dxi * (sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii]);
-    const double hy = dyi * (sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
-    const double h = hx + hy;
+    const T hx = dxi * (sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii]);
+    const T hy = dyi * (sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
+    const double h = (double)(hx + hy);
     rhs[(long long)m * P.ps + p] = neg ? -h : h;
   }
 }
@@ -458,48 +510,51 @@ __global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double*
 // accumulation rhs += par; rhs += source (TimeRHSFunctionExplicit.c:67-74).
 // Tile: 32 x 8 interior points.  Cross-derivative terms at ghost columns/rows
 // are zero, as the reference computes derivatives on interior lines only.
-__device__ __forceinline__ void visc_coeffs(const DevParams& P, double T, double& mu, double& kappa) {
-  const double Td = T * P.Tref;
-  const double r15 = exp(1.5 * log(Td / P.T0));   // raiseto (math_ops.h:40)
-  mu = r15 * (P.T0 + P.TS) / (Td + P.TS);
-  kappa = r15 * (P.T0 + P.TA * exp(-P.TB / P.T0)) / (Td + P.TA * exp(-P.TB / Td));
+template <typename T>
+__device__ __forceinline__ void visc_coeffs(const DevParams& P, T Temp, T& mu, T& kappa) {
+  const T Td = Temp * (T)P.Tref, T0 = (T)P.T0;
+  const T r15 = exp(T(1.5) * log(Td / T0));   // raiseto (math_ops.h:40)
+  mu = r15 * (T0 + (T)P.TS) / (Td + (T)P.TS);
+  kappa = r15 * (T0 + (T)P.TA * exp(-(T)P.TB / T0)) / (Td + (T)P.TA * exp(-(T)P.TB / Td));
 }
 
+// ChemistrySetPhotonDensity (ChemistrySolve.c:18-65) + _ChemistrySetRHS_ /
+// _ChemistrySetQ_ (chemistry.h:30-137) at point p, arithmetic in T, added to
+// the FP64 rhs; the energy slot takes the heating of the last layer.
+template <typename T>
 __device__ void chem_source_point(const DevParams& P, const double* __restrict__ U, long long p,
                                   double hnu_factor, double imap_p, double* __restrict__ rhs) {
-  // ChemistrySetPhotonDensity (ChemistrySolve.c:18-65) + _ChemistrySetRHS_/_ChemistrySetQ_
-  // (chemistry.h:30-137); the energy slot takes the heating of the last layer.
   const long long ps = P.ps;
-  double n_hnu = hnu_factor * imap_p / (P.ch_c * P.ch_h * P.ch_nu * P.n_O2);
-  const double k0a = P.k[0], k0b = P.k[1], k1a = P.k[2], k1b = P.k[3], k2a = P.k[4], k2b = P.k[5];
-  const double k3a = P.k[6], k3b = P.k[7], k4 = P.k[8], k5 = P.k[9], k6 = P.k[10];
-  double Q = 0.0;
+  T n_hnu = (T)(hnu_factor * imap_p / (P.ch_c * P.ch_h * P.ch_nu * P.n_O2));
+  const T k0a = (T)P.k[0], k0b = (T)P.k[1], k1a = (T)P.k[2], k1b = (T)P.k[3], k2a = (T)P.k[4], k2b = (T)P.k[5];
+  const T k3a = (T)P.k[6], k3b = (T)P.k[7], k4 = (T)P.k[8], k5 = (T)P.k[9], k6 = (T)P.k[10];
+  T Q = T(0);
   for (int iz = 0; iz < P.nz; iz++) {
     if (iz > 0) {
-      const double damp = 1.0 - P.dz * (P.sO3 * P.n_O2) * U[(P.nflow + P.zstride * (iz - 1) + 1) * ps + p];
+      const T damp = T(1) - (T)P.dz * (T)(P.sO3 * P.n_O2) * (T)U[(P.nflow + P.zstride * (iz - 1) + 1) * ps + p];
       n_hnu = n_hnu * damp;
     }
     const int nfv = P.nflow + P.zstride * iz;
-    const double nO2 = U[(nfv + 0) * ps + p], nO3 = U[(nfv + 1) * ps + p], n1D = U[(nfv + 2) * ps + p];
-    const double n1Dg = U[(nfv + 3) * ps + p], n3Su = U[(nfv + 4) * ps + p], n1Sg = U[(nfv + 5) * ps + p];
-    const double nCO2 = U[(nfv + 6) * ps + p];
-    const double sO3 = -(k0a + k0b) * n_hnu * nO3 - (k2a + k2b) * nO3 * n1D - (k3a + k3b) * nO3 * n1Sg
-                       - k5 * nO3 * n3Su - k6 * n1Dg * nO3;
-    const double s1D = k0a * n_hnu * nO3 - (k1a + k1b) * n1D * nO2 - (k2a + k2b) * n1D * nO3 - k4 * n1D * nCO2;
-    const double s1Dg = k0a * n_hnu * nO3 + k5 * nO3 * n3Su - k6 * n1Dg * nO3;
-    const double s3Su = k2a * nO3 * n1D - k5 * nO3 * n3Su;
-    const double s1Sg = k1a * n1D * nO2 - (k3a + k3b) * nO3 * n1Sg;
-    rhs[(nfv + 1) * ps + p] += sO3;
-    rhs[(nfv + 2) * ps + p] += s1D;
-    rhs[(nfv + 3) * ps + p] += s1Dg;
-    rhs[(nfv + 4) * ps + p] += s3Su;
-    rhs[(nfv + 5) * ps + p] += s1Sg;
-    Q = ((P.q[0] * k0a + P.q[1] * k0b) * n_hnu * nO3 + (P.q[2] * k1a + P.q[3] * k1b) * nO2 * n1D
-         + (P.q[4] * k2a + P.q[5] * k2b) * nO3 * n1D + (P.q[6] * k3a + P.q[7] * k3b) * nO3 * n1Sg
-         + P.q[8] * k4 * n1D * nCO2 + P.q[9] * k5 * nO3 * n3Su + P.q[10] * k6 * n1Dg * nO3)
-        / (P.chem_gamma - 1.0);
+    const T nO2 = (T)U[(nfv + 0) * ps + p], nO3 = (T)U[(nfv + 1) * ps + p], n1D = (T)U[(nfv + 2) * ps + p];
+    const T n1Dg = (T)U[(nfv + 3) * ps + p], n3Su = (T)U[(nfv + 4) * ps + p], n1Sg = (T)U[(nfv + 5) * ps + p];
+    const T nCO2 = (T)U[(nfv + 6) * ps + p];
+    const T sO3 = -(k0a + k0b) * n_hnu * nO3 - (k2a + k2b) * nO3 * n1D - (k3a + k3b) * nO3 * n1Sg
+                  - k5 * nO3 * n3Su - k6 * n1Dg * nO3;
+    const T s1D = k0a * n_hnu * nO3 - (k1a + k1b) * n1D * nO2 - (k2a + k2b) * n1D * nO3 - k4 * n1D * nCO2;
+    const T s1Dg = k0a * n_hnu * nO3 + k5 * nO3 * n3Su - k6 * n1Dg * nO3;
+    const T s3Su = k2a * nO3 * n1D - k5 * nO3 * n3Su;
+    const T s1Sg = k1a * n1D * nO2 - (k3a + k3b) * nO3 * n1Sg;
+    rhs[(nfv + 1) * ps + p] += (double)sO3;
+    rhs[(nfv + 2) * ps + p] += (double)s1D;
+    rhs[(nfv + 3) * ps + p] += (double)s1Dg;
+    rhs[(nfv + 4) * ps + p] += (double)s3Su;
+    rhs[(nfv + 5) * ps + p] += (double)s1Sg;
+    Q = (((T)P.q[0] * k0a + (T)P.q[1] * k0b) * n_hnu * nO3 + ((T)P.q[2] * k1a + (T)P.q[3] * k1b) * nO2 * n1D
+         + ((T)P.q[4] * k2a + (T)P.q[5] * k2b) * nO3 * n1D + ((T)P.q[6] * k3a + (T)P.q[7] * k3b) * nO3 * n1Sg
+         + (T)P.q[8] * k4 * n1D * nCO2 + (T)P.q[9] * k5 * nO3 * n3Su + (T)P.q[10] * k6 * n1Dg * nO3)
+        / ((T)P.chem_gamma - T(1));
   }
-  rhs[(P.nflow - 1) * ps + p] += Q;
+  rhs[(P.nflow - 1) * ps + p] += (double)Q;
 }
 
 // pulse factor I0 exp(-(t - (t_start+t_pulse))^2 / (2 sigma^2)) or 0 before t_start
@@ -510,35 +565,48 @@ __device__ __forceinline__ double pulse_factor(const DevParams& P, double t) {
   return P.I0 * exp(-(tp * tp) / (2 * sigma * sigma));
 }
 
+// MX (mixed precision): velocities and temperature, their differences, the
+// viscous fluxes and the chemistry in FP32; the temperature is held relative
+// to the tile's first point (taken in FP64) so that its differences keep
+// FP32's relative precision; the result is added to the FP64 rhs.
+template <bool MX>
 __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* __restrict__ U,
                                                      const double* __restrict__ dxinv,
                                                      const double* __restrict__ imap,
                                                      const double* __restrict__ tdev, double cstage,
                                                      double* __restrict__ rhs, int do_chem) {
+  typedef typename std::conditional<MX, float, double>::type T;
   constexpr int BX = 32, BY = 8, QX = BX + 2, QY = BY + 2, FX = BX + 1, FY = BY + 1;
-  __shared__ double su[QY][QX], sv[QY][QX], sT[QY][QX];
-  __shared__ double fx[3][BY][FX];   // FVx at i in [i0-1, i0+BX), rows j0..j0+BY-1
-  __shared__ double fy[3][FY][BX];   // FVy at j in [j0-1, j0+BY), cols i0..i0+BX-1
+  __shared__ T su[QY][QX], sv[QY][QX], sT[QY][QX];
+  __shared__ T fx[3][BY][FX];   // FVx at i in [i0-1, i0+BX), rows j0..j0+BY-1
+  __shared__ T fy[3][FY][BX];   // FVy at j in [j0-1, j0+BY), cols i0..i0+BX-1
   const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
   const int tid = threadIdx.x + BX * threadIdx.y;
   const long long ps = P.ps;
   if (P.viscous) {
+    double Tref = 0.0;
+    if (MX) {
+      const long long p0 = pidx(P, i0, j0);
+      double rho, uu, vv, e_, pr;
+      ns_flowvar(U[p0], U[ps + p0], U[2 * ps + p0], U[3 * ps + p0], P.gamma, rho, uu, vv, e_, pr);
+      Tref = P.gamma * pr / rho;
+    }
     // Q = (u, v, T = gamma p / rho) on [i0-1, i0+BX] x [j0-1, j0+BY]
     for (int e = tid; e < QX * QY; e += BX * BY) {
       const int a = e % QX, b = e / QX;
       const int i = i0 - 1 + a, j = j0 - 1 + b;
-      double uu = 0.0, vv = 0.0, TT = 0.0;
+      double uu = 0.0, vv = 0.0, TT = Tref;
       if (i >= -P.ghosts && i < P.N0 + P.ghosts && j >= -P.ghosts && j < P.N1 + P.ghosts) {
         const long long p = pidx(P, i, j);
         double rho, e_, pr;
         ns_flowvar(U[p], U[ps + p], U[2 * ps + p], U[3 * ps + p], P.gamma, rho, uu, vv, e_, pr);
         TT = P.gamma * pr / rho;
       }
-      su[b][a] = uu; sv[b][a] = vv; sT[b][a] = TT;
+      su[b][a] = (T)uu; sv[b][a] = (T)vv; sT[b][a] = (T)(TT - Tref);
     }
     __syncthreads();
-    const double two_third = 2.0 / 3.0, inv_Re = 1.0 / P.Re, inv_Pr = 1.0 / P.Pr;
-    const double igm1 = 1.0 / (P.gamma - 1.0);
+    const T two_third = T(2.0 / 3.0), inv_Re = (T)(1.0 / P.Re), inv_Pr = (T)(1.0 / P.Pr);
+    const T igm1 = (T)(1.0 / (P.gamma - 1.0));
     // viscous fluxes on [i0-1, i0+BX) x [j0-1, j0+BY) (corner cell unused)
     for (int e = tid; e < FX * FY; e += BX * BY) {
       const int a = e % FX, b = e / FX;       // a: i - (i0-1), b: j - (j0-1)
@@ -547,25 +615,25 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
       const bool need_y = (a >= 1) && (i < P.N0) && (j < P.N1);   // FVy at interior columns
       if (!need_x && !need_y) continue;
       const int qa = a, qb = b;               // (i, j) in the Q tile
-      const double dxi = dxinv[P.ghosts + i], dyi = dxinv[P.W0 + P.ghosts + j];
+      const T dxi = (T)dxinv[P.ghosts + i], dyi = (T)dxinv[P.W0 + P.ghosts + j];
       const bool row_int = (j >= 0 && j < P.N1), col_int = (i >= 0 && i < P.N0);
-      const double uc = su[qb][qa], vc = sv[qb][qa], Tc = sT[qb][qa];
+      const T uc = su[qb][qa], vc = sv[qb][qa], Tc = sT[qb][qa];
       // first differences (QDerivX only on interior rows, QDerivY only on interior columns)
-      const double ux = row_int ? dxi * (su[qb][qa + 1] - uc) : 0.0;
-      const double vx = row_int ? dxi * (sv[qb][qa + 1] - vc) : 0.0;
-      const double Tx = row_int ? dxi * (sT[qb][qa + 1] - Tc) : 0.0;
-      const double uy = col_int ? dyi * (su[qb + 1][qa] - uc) : 0.0;
-      const double vy = col_int ? dyi * (sv[qb + 1][qa] - vc) : 0.0;
-      const double Ty = col_int ? dyi * (sT[qb + 1][qa] - Tc) : 0.0;
-      double mu, kappa;
-      visc_coeffs(P, Tc, mu, kappa);
-      const double mre = mu * inv_Re, kre = kappa * inv_Re * igm1 * inv_Pr;
+      const T ux = row_int ? dxi * (su[qb][qa + 1] - uc) : T(0);
+      const T vx = row_int ? dxi * (sv[qb][qa + 1] - vc) : T(0);
+      const T Tx = row_int ? dxi * (sT[qb][qa + 1] - Tc) : T(0);
+      const T uy = col_int ? dyi * (su[qb + 1][qa] - uc) : T(0);
+      const T vy = col_int ? dyi * (sv[qb + 1][qa] - vc) : T(0);
+      const T Ty = col_int ? dyi * (sT[qb + 1][qa] - Tc) : T(0);
+      T mu, kappa;
+      visc_coeffs<T>(P, MX ? (T)Tref + Tc : Tc, mu, kappa);
+      const T mre = mu * inv_Re, kre = kappa * inv_Re * igm1 * inv_Pr;
       if (need_x) {
-        const double txx = two_third * mre * (2 * ux - vy), txy = mre * (uy + vx);
+        const T txx = two_third * mre * (T(2) * ux - vy), txy = mre * (uy + vx);
         fx[0][b - 1][a] = txx; fx[1][b - 1][a] = txy; fx[2][b - 1][a] = uc * txx + vc * txy + kre * Tx;
       }
       if (need_y) {
-        const double tyx = mre * (uy + vx), tyy = two_third * mre * (-ux + 2 * vy);
+        const T tyx = mre * (uy + vx), tyy = two_third * mre * (-ux + T(2) * vy);
         fy[0][b][a - 1] = tyx; fy[1][b][a - 1] = tyy; fy[2][b][a - 1] = uc * tyx + vc * tyy + kre * Ty;
       }
     }
@@ -576,20 +644,21 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
   if (i >= P.N0 || j >= P.N1) return;
   const long long p = pidx(P, i, j);
   if (P.viscous) {
-    const double dxi = dxinv[P.ghosts + i], dyi = dxinv[P.W0 + P.ghosts + j];
+    const T dxi = (T)dxinv[P.ghosts + i], dyi = (T)dxinv[P.W0 + P.ghosts + j];
 #pragma unroll
     for (int m = 0; m < 3; m++) {
-      const double par = dxi * (fx[m][b][a + 1] - fx[m][b][a]) + dyi * (fy[m][b + 1][a] - fy[m][b][a]);
-      rhs[(m + 1) * ps + p] += par;
+      const T par = dxi * (fx[m][b][a + 1] - fx[m][b][a]) + dyi * (fy[m][b + 1][a] - fy[m][b][a]);
+      rhs[(m + 1) * ps + p] += (double)par;
     }
   }
   if (do_chem) {
     const double t = *tdev + cstage * P.dt;
-    chem_source_point(P, U, p, pulse_factor(P, t), imap[p], rhs);
+    chem_source_point<T>(P, U, p, pulse_factor(P, t), imap[p], rhs);
   }
 }
 
 // chemistry source alone (1D, or 2D without viscosity)
+template <bool MX>
 __global__ void k_source(DevParams P, const double* __restrict__ U, const double* __restrict__ imap,
                          const double* __restrict__ tdev, double cstage, double* __restrict__ rhs) {
   long long n = (long long)P.N0 * P.N1;
@@ -598,7 +667,7 @@ __global__ void k_source(DevParams P, const double* __restrict__ U, const double
   int i = (int)(idx % P.N0), j = (int)(idx / P.N0);
   long long p = pidx(P, i, j);
   const double t = *tdev + cstage * P.dt;
-  chem_source_point(P, U, p, pulse_factor(P, t), imap[p], rhs);
+  chem_source_point<typename std::conditional<MX, float, double>::type>(P, U, p, pulse_factor(P, t), imap[p], rhs);
 }
 
 __global__ void k_advance_time(double* tdev, double dt) { *tdev += dt; }
@@ -750,35 +819,48 @@ void launch_flux(const DevParams& P, const double* U, double* F, int dir, cudaSt
     k_flux<EULER1D, 0><<<nb, 256, 0, s>>>(P, U, F);
   }
 }
-void launch_weno5(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                  double* fR, int dir, cudaStream_t s) {
+void launch_weno5(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                  int dir, cudaStream_t s) {
   long long n = P.nint[dir] * P.nvars;
-  if (dir == 0) k_weno5<0><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
-  else k_weno5<1><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
-}
-
-template <int MODEL, int UPW>
-static void upwind_div_dir(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
-                           const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
-  // the interface-flux tile holds nvars x (tile + 1) doubles: allow more than
-  // the 48 KB default for many-species decks
-  raise_smem_limit<k_upwind_div<MODEL, UPW, 0>>(200 * 1024);
-  raise_smem_limit<k_upwind_div<MODEL, UPW, 1>>(200 * 1024);
-  if (dir == 0) {
-    dim3 grid(nblk(P.N0, 128), P.N1), blk(128, 1);
-    size_t smem = (size_t)P.nvars * 129 * sizeof(double);
-    k_upwind_div<MODEL, UPW, 0><<<grid, blk, smem, s>>>(P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+  if (P.mixed) {
+    if (dir == 0) k_weno5<0, true><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
+    else k_weno5<1, true><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
   } else {
-    dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
-    size_t smem = (size_t)P.nvars * 9 * 32 * sizeof(double);
-    k_upwind_div<MODEL, UPW, 1><<<grid, blk, smem, s>>>(P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+    if (dir == 0) k_weno5<0, false><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
+    else k_weno5<1, false><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
   }
 }
 
+template <int MODEL, int UPW>
+static void upwind_div_dir(const DevParams& P, const double* U, const void* uL, const void* uR, const void* fL,
+                           const void* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
+  // the interface-flux tile holds nvars x (tile + 1) values: allow more than
+  // the 48 KB default for many-species decks
+  if (dir == 0) {
+    dim3 grid(nblk(P.N0, 128), P.N1), blk(128, 1);
+    if constexpr (MODEL == EULER1D) {
+      if (P.mixed) {
+        raise_smem_limit<k_upwind_div<MODEL, UPW, 0, true>>(200 * 1024);
+        k_upwind_div<MODEL, UPW, 0, true><<<grid, blk, (size_t)P.nvars * 129 * sizeof(float), s>>>(
+            P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+        return;
+      }
+    }
+    {
+      raise_smem_limit<k_upwind_div<MODEL, UPW, 0, false>>(200 * 1024);
+      k_upwind_div<MODEL, UPW, 0, false><<<grid, blk, (size_t)P.nvars * 129 * sizeof(double), s>>>(
+          P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+    }
+  } else {
+    dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
+    raise_smem_limit<k_upwind_div<MODEL, UPW, 1, false>>(200 * 1024);
+    k_upwind_div<MODEL, UPW, 1, false><<<grid, blk, (size_t)P.nvars * 9 * 32 * sizeof(double), s>>>(
+        P, U, uL, uR, fL, fR, dxinv, rhs, mode);
+  }
+}
 template <int MODEL>
-static void upwind_div_model(const DevParams& P, const double* U, const double* uL, const double* uR,
-                             const double* fL, const double* fR, const double* dxinv, double* rhs, int dir,
-                             int mode, cudaStream_t s) {
+static void upwind_div_model(const DevParams& P, const double* U, const void* uL, const void* uR, const void* fL,
+                             const void* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
   switch (P.upwind) {
     case UPW_ROE: upwind_div_dir<MODEL, UPW_ROE>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s); break;
     case UPW_RF: upwind_div_dir<MODEL, UPW_RF>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s); break;
@@ -787,35 +869,40 @@ static void upwind_div_model(const DevParams& P, const double* U, const double* 
   }
 }
 
-void launch_upwind_div(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
-                       const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
+void launch_upwind_div(const DevParams& P, const double* U, const void* uL, const void* uR, const void* fL,
+                       const void* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s) {
   if (P.model == NS2D) upwind_div_model<NS2D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
   else upwind_div_model<EULER1D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
 }
 
-template <int UPW, bool YT>
-static void upwind_div2d_u(const DevParams& P, const double* U, const double* UT, const double* const* xi,
-                           const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
-  raise_smem_limit<k_upwind_div2d<UPW, YT>>(200 * 1024);
+template <int UPW, bool YT, bool MX>
+static void upwind_div2d_u(const DevParams& P, const double* U, const double* UT, const void* const* xi,
+                           const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
+  raise_smem_limit<k_upwind_div2d<UPW, YT, MX>>(200 * 1024);
   dim3 grid(nblk(P.N0, 16), nblk(P.N1, 15));
-  size_t smem = (size_t)P.nvars * (17 * 15 + 16 * 17) * sizeof(double);
-  k_upwind_div2d<UPW, YT><<<grid, 256, smem, s>>>(P, U, UT, xi[0], xi[1], xi[2], xi[3], yi[0], yi[1], yi[2], yi[3],
-                                                   dxinv, rhs, neg);
+  size_t smem = (size_t)P.nvars * (17 * 15 + 16 * 17) * (MX ? sizeof(float) : sizeof(double));
+  k_upwind_div2d<UPW, YT, MX><<<grid, 256, smem, s>>>(P, U, UT, xi[0], xi[1], xi[2], xi[3], yi[0], yi[1], yi[2],
+                                                       yi[3], dxinv, rhs, neg);
 }
-template <bool YT>
-static void upwind_div2d_yt(const DevParams& P, const double* U, const double* UT, const double* const* xi,
-                            const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
+template <bool YT, bool MX>
+static void upwind_div2d_yt(const DevParams& P, const double* U, const double* UT, const void* const* xi,
+                            const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
   switch (P.upwind) {
-    case UPW_ROE: upwind_div2d_u<UPW_ROE, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
-    case UPW_RF: upwind_div2d_u<UPW_RF, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
-    case UPW_RUSANOV: upwind_div2d_u<UPW_RUSANOV, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
-    default: upwind_div2d_u<UPW_LLF, YT>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    case UPW_ROE: upwind_div2d_u<UPW_ROE, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    case UPW_RF: upwind_div2d_u<UPW_RF, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    case UPW_RUSANOV: upwind_div2d_u<UPW_RUSANOV, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    default: upwind_div2d_u<UPW_LLF, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
   }
 }
-void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const double* const* xi,
-                         const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
-  if (UT) upwind_div2d_yt<true>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
-  else upwind_div2d_yt<false>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
+                         const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
+  if (P.mixed) {
+    if (UT) upwind_div2d_yt<true, true>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+    else upwind_div2d_yt<false, true>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+  } else {
+    if (UT) upwind_div2d_yt<true, false>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+    else upwind_div2d_yt<false, false>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+  }
 }
 
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
@@ -824,9 +911,12 @@ void launch_visc_source(const DevParams& P, const double* U, const double* dxinv
   do_chem = do_chem && P.chem;
   if (do_visc) {
     dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
-    k_visc_source<<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem);
+    if (P.mixed) k_visc_source<true><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem);
+    else k_visc_source<false><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem);
   } else if (do_chem) {
-    k_source<<<nblk((long long)P.N0 * P.N1, 256), 256, 0, s>>>(P, U, imap, tdev, cstage, rhs);
+    const unsigned nb = nblk((long long)P.N0 * P.N1, 256);
+    if (P.mixed) k_source<true><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs);
+    else k_source<false><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs);
   }
 }
 

@@ -44,20 +44,26 @@ void launch_update(const DevParams& P, double* u, const double* const* d, const 
                    cudaStream_t s);
 void launch_cfl(const DevParams& P, const double* u, const double* dxinv, unsigned long long* out, cudaStream_t s);
 void launch_flux(const DevParams& P, const double* U, double* F, int dir, cudaStream_t s);
-void launch_weno5(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                  double* fR, int dir, cudaStream_t s);
-// CRWENO5 interface values (crweno.cu); -1 if a line is too long
+// WENO5 interface values; doubles, or floats relative to each line's first
+// value when P.mixed
+void launch_weno5(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                  int dir, cudaStream_t s);
+// CRWENO5 interface values (crweno.cu); -1 if a line is too long.  The
+// interface arrays hold doubles, or floats relative to each line's first
+// value when P.mixed (x-direction lines only).
 int crweno_rows_per_thread(int N);
-int launch_crweno(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
-                  double* fR, int dir, int* err, cudaStream_t s);
+int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                  int dir, int* err, cudaStream_t s);
 // mode 0: rhs = -hyp_x; 1: rhs = -((-rhs) + hyp_y); 2: out = hyp_x; 3: out += hyp_y
-void launch_upwind_div(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
-                       const double* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s);
+// (interface arrays as written by launch_weno5 / launch_crweno; the mixed
+// variant covers the 1D x direction, 2D goes through launch_upwind_div2d)
+void launch_upwind_div(const DevParams& P, const double* U, const void* uL, const void* uR, const void* fL,
+                       const void* fR, const double* dxinv, double* rhs, int dir, int mode, cudaStream_t s);
 // both directions of a 2D hyperbolic term in one pass: xi / yi are the
 // (uL, uR, fL, fR) interface arrays of x and y; y in the transposed layout
 // with cell values from UT when UT is given.  rhs = -hyp (neg) or hyp.
-void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const double* const* xi,
-                         const double* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
+void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
+                         const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
 // rhs += par (if do_visc) then rhs += source (if do_chem)
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
                         const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s);

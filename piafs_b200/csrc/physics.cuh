@@ -266,6 +266,63 @@ __device__ void upwind_flow(const T* uL, const T* uR, const T* fL, const T* fR, 
   }
 }
 
+// Deviation form of upwind_flow for the mixed-precision path.  uL, uR, fL,
+// fR are taken relative to constants shared by both sides of the interface
+// (the reference values of the interface's grid line); uAL / uAR are the
+// absolute interface states (the NS2D characteristic schemes take the Roe
+// average and the eigenvalues from them) and uCL / uCR the absolute
+// cell-centred states.  The flux comes back relative to the same constant as
+// fL and fR.  With fbar = (fL + fR) / 2, every scheme is fI = fbar + R s (or
+// fbar - R |D| L (uR - uL) / 2 for Roe), with s formed from differences of
+// the inputs only, so no O(1) background goes through FP32 rounding before
+// the divergence differences the interface fluxes.  Mathematically equal to
+// upwind_flow on the absolute values.
+template <int MODEL, int UPW, typename T>
+__device__ void upwind_flow_dev(const T* uL, const T* uR, const T* fL, const T* fR, const T* uAL, const T* uAR,
+                                const T* uCL, const T* uCR, T g, int dir, T* fI, T* sp_alpha, int* sp_mode) {
+  typedef Flow<MODEL> F;
+  constexpr int NF = F::NF;
+  if (UPW == UPW_ROE || UPW == UPW_RUSANOV) {   // these are in deviation form already
+    upwind_flow<MODEL, UPW, T>(uL, uR, fL, fR, uCL, uCR, g, dir, fI, sp_alpha, sp_mode);
+    return;
+  }
+  T ua[4], L[4][4], R[4][4], eL[4], eR[4], eC[4], vnL, vnR, vnC;
+  if (MODEL == NS2D) {
+    F::roe_avg(uAL, uAR, g, ua);
+    F::eigvec(ua, g, dir, L, R);
+    vnL = F::eigvals(uAL, g, dir, eL);
+    vnR = F::eigvals(uAR, g, dir, eR);
+    vnC = F::eigvals(ua, g, dir, eC);
+  } else {
+    F::roe_avg(uCL, uCR, g, ua);
+    F::eigvec(ua, g, dir, L, R);
+    vnL = F::eigvals(uCL, g, dir, eL);
+    vnR = F::eigvals(uCR, g, dir, eR);
+    vnC = F::eigvals(ua, g, dir, eC);
+  }
+  T sc[4];
+#pragma unroll
+  for (int a = 0; a < NF; a++) {
+    T df = T(0), du = T(0);
+#pragma unroll
+    for (int b = 0; b < NF; b++) { df += L[a][b] * (fL[b] - fR[b]); du += L[a][b] * (uL[b] - uR[b]); }
+    if (UPW == UPW_RF && eL[a] > T(0) && eC[a] > T(0) && eR[a] > T(0)) sc[a] = T(0.5) * df;
+    else if (UPW == UPW_RF && eL[a] < T(0) && eC[a] < T(0) && eR[a] < T(0)) sc[a] = T(-0.5) * df;
+    else sc[a] = T(0.5) * max3v(absv(eL[a]), absv(eC[a]), absv(eR[a])) * du;
+  }
+#pragma unroll
+  for (int a = 0; a < NF; a++) {
+    T s = T(0);
+#pragma unroll
+    for (int b = 0; b < NF; b++) s += R[a][b] * sc[b];
+    fI[a] = T(0.5) * (fL[a] + fR[a]) + s;
+  }
+  if (UPW == UPW_RF && vnL > T(0) && vnC > T(0) && vnR > T(0)) *sp_mode = 2;
+  else if (UPW == UPW_RF && vnL < T(0) && vnC < T(0) && vnR < T(0)) *sp_mode = 3;
+  else *sp_mode = 1;
+  *sp_alpha = max3v(absv(vnL), absv(vnC), absv(vnR));
+}
+
 template <typename T>
 __device__ __forceinline__ T upwind_species(int mode, T alpha, T uL, T uR, T fL, T fR) {
   if (mode == 0) return T(0.5) * (fL + fR) - alpha * (T(0.5) * (uR - uL));
