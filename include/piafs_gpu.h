@@ -158,6 +158,63 @@ int piafs_gpu_FirstDerivativePar(piafs_gpu_sim* sim, double* Df, const double* f
  * PIAFS_ERR_SINGULAR on a zero pivot like the reference's -1. */
 int piafs_gpu_tridiagLU(double* a, double* b, double* c, double* x, int n, int ns);
 
+/* ---- batched simulations (ensembles and request serving) ----
+ * No counterpart in the reference, whose ensemble mode (OutputSolution.cpp,
+ * one deck per member) runs members one after another.  A batch holds many
+ * independent simulations ("members") resident on the device at once, each
+ * from its own input deck and of its own size, physics and step count, and
+ * advances all of them together: one persistent kernel per Runge-Kutta
+ * stage walks a device-side list of tiles that covers every member, and a
+ * step (the stage kernels plus a small per-step epilogue) is replayed from a
+ * CUDA graph whatever the mix of members.  Members join and leave between
+ * steps (continuous batching).  Supported members: 2D navierstokes2d with or
+ * without photochemistry and viscosity, and 1D euler1d without chemistry,
+ * WENO5 (any weight variant), any upwinding, any explicit RK tableau,
+ * periodic / extrapolate / slip-wall boundaries.  In FP64 a member's result
+ * agrees with the same deck run alone through piafs_gpu_TimeRK to rounding
+ * (relative L2 within 1e-12), and is bit for bit the same whatever other
+ * members share the batch and whenever they join or leave. */
+typedef struct piafs_gpu_batch piafs_gpu_batch;
+typedef struct {
+  int members;                      /* admitted and not yet removed       */
+  int active;                       /* still stepping                     */
+  int tiles;                        /* tiles in the current launch list   */
+  int tile_x, tile_y;               /* tile shape of the 2D stage kernel  */
+  long long steps;                  /* batch steps taken                  */
+  unsigned long long bytes_in_use;  /* member state held on the device    */
+  unsigned long long budget_bytes;  /* 0: no limit                        */
+  int launches_per_step;            /* kernels one batch step launches    */
+} piafs_gpu_batch_info;
+/* hbm_budget_bytes bounds the device memory the members' state may take
+ * (0: no bound); precision is PIAFS_PRECISION_*. */
+int piafs_gpu_batch_create(int precision, unsigned long long hbm_budget_bytes, piafs_gpu_batch** batch);
+void piafs_gpu_batch_destroy(piafs_gpu_batch* batch);
+/* Admit the simulation of the input deck in deck_dir, to run nsteps time
+ * steps (<= 0: the deck's n_iter).  On success *id names the member.  Returns
+ * PIAFS_ERR_MEMORY, with nothing changed, when the budget cannot hold it now,
+ * and PIAFS_ERR_UNSUPPORTED for decks outside the batched path. */
+int piafs_gpu_batch_add(piafs_gpu_batch* batch, const char* deck_dir, int nsteps, int* id);
+/* Advance every active member by up to nsteps steps; a member stops after
+ * its own step count.  Waits for the device. */
+int piafs_gpu_batch_step(piafs_gpu_batch* batch, int nsteps);
+/* Up to cap ids of members that finished since the last call, count in *n. */
+int piafs_gpu_batch_poll(piafs_gpu_batch* batch, int* done, int cap, int* n);
+/* A member's solution (interior points, the layout of the op files) and its
+ * time and step count. */
+int piafs_gpu_batch_get_solution(piafs_gpu_batch* batch, int id, double* u_interior);
+int piafs_gpu_batch_member(piafs_gpu_batch* batch, int id, double* t, int* iter, int* done);
+/* The stage derivative k_stage (TimeRHSFunctionExplicit's rhs) of the
+ * member's last step, interior points in the layout of the op files. */
+int piafs_gpu_batch_get_stage_derivative(piafs_gpu_batch* batch, int id, int stage, double* k_interior);
+/* Release a member's device memory (finished or not). */
+int piafs_gpu_batch_remove(piafs_gpu_batch* batch, int id);
+int piafs_gpu_batch_get_info(piafs_gpu_batch* batch, piafs_gpu_batch_info* info);
+/* Pick the 2D tile shape for the current members by timing each candidate
+ * on a copy-free dry run of one step (the members' state is saved and
+ * restored); tile_x/tile_y report the choice.  Candidates 0 = automatic;
+ * or force a shape with tile_x * tile_y = 256 (32x8, 16x16, 64x4). */
+int piafs_gpu_batch_tune(piafs_gpu_batch* batch, int force_tile_x);
+
 /* ---- diagnostics ----
  * No counterpart in the reference.  y[i] = 1/x[i] (device arrays) computed
  * by the Newton-Raphson reciprocal that the reconstruction and line-solve

@@ -65,6 +65,18 @@ SIGNATURES = {
     "piafs_gpu_tridiagLU": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
     "piafs_gpu_HyperbolicFunction_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "piafs_gpu_reciprocal": (C.c_int, [_vp, _vp, C.c_longlong]),
+    "piafs_gpu_batch_create": (C.c_int, [C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "piafs_gpu_batch_destroy": (None, [_vp]),
+    "piafs_gpu_batch_add": (C.c_int, [_vp, C.c_char_p, C.c_int, C.POINTER(C.c_int)]),
+    "piafs_gpu_batch_step": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_batch_poll": (C.c_int, [_vp, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
+    "piafs_gpu_batch_get_solution": (C.c_int, [_vp, C.c_int, _dp]),
+    "piafs_gpu_batch_member": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int)]),
+    "piafs_gpu_batch_remove": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_batch_get_stage_derivative": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
+    "piafs_gpu_batch_get_info": (C.c_int, [_vp, _vp]),
+    "piafs_gpu_batch_tune": (C.c_int, [_vp, C.c_int]),
 }
 
 
@@ -287,6 +299,95 @@ def hyperbolic_noalloc(params: "HypParams", hyp, u, dxinv, stream: int = 0):
     code = L.piafs_gpu_HyperbolicFunction_noalloc(C.byref(params), _ptr(hyp), _ptr(u), _ptr(dxinv), stream)
     if code != PIAFS_OK:
         raise PiafsError(code, L.piafs_gpu_last_error().decode())
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("members", C.c_int), ("active", C.c_int), ("tiles", C.c_int), ("tile_x", C.c_int),
+        ("tile_y", C.c_int), ("steps", C.c_longlong), ("bytes_in_use", C.c_ulonglong),
+        ("budget_bytes", C.c_ulonglong), ("launches_per_step", C.c_int),
+    ]
+
+    def asdict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Batch:
+    """Many independent simulations resident on the device and advanced
+    together by one persistent kernel per RK stage (piafs_gpu_batch_*)."""
+
+    def __init__(self, precision: str = "fp64", hbm_budget_bytes: int = 0):
+        L = load_library()
+        h = _vp()
+        _check(L.piafs_gpu_batch_create(PRECISION[precision], int(hbm_budget_bytes), C.byref(h)))
+        self._h = h
+        self._shapes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.piafs_gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, deck_dir: str, nsteps: int = 0) -> int:
+        """Admit a member; raises PiafsError (code PIAFS_ERR_MEMORY when the
+        budget cannot hold it now)."""
+        i = C.c_int()
+        _check(_lib.piafs_gpu_batch_add(self._h, os.fsencode(deck_dir), int(nsteps), C.byref(i)))
+        d = deck.read_keyfile(os.path.join(deck_dir, "solver.inp"))
+        size = [int(x) for x in d["size"]]
+        self._shapes[i.value] = (int(np.prod(size)), int(d["nvars"][0]))
+        return i.value
+
+    def step(self, nsteps: int = 1):
+        _check(_lib.piafs_gpu_batch_step(self._h, int(nsteps)))
+
+    def poll(self, cap: int = 4096):
+        buf = (C.c_int * cap)()
+        n = C.c_int()
+        _check(_lib.piafs_gpu_batch_poll(self._h, buf, cap, C.byref(n)))
+        return list(buf[: n.value])
+
+    def solution(self, member: int) -> np.ndarray:
+        npts, nv = self._shapes[member]
+        u = np.empty((npts, nv))
+        _check(_lib.piafs_gpu_batch_get_solution(self._h, int(member), _hp(u)))
+        return u
+
+    def stage_derivative(self, member: int, stage: int) -> np.ndarray:
+        npts, nv = self._shapes[member]
+        k = np.empty((npts, nv))
+        _check(_lib.piafs_gpu_batch_get_stage_derivative(self._h, int(member), int(stage), _hp(k)))
+        return k
+
+    def member(self, member: int) -> dict:
+        t, it, done = C.c_double(), C.c_int(), C.c_int()
+        _check(_lib.piafs_gpu_batch_member(self._h, int(member), C.byref(t), C.byref(it), C.byref(done)))
+        return {"t": t.value, "iter": it.value, "done": bool(done.value)}
+
+    def remove(self, member: int):
+        _check(_lib.piafs_gpu_batch_remove(self._h, int(member)))
+        self._shapes.pop(member, None)
+
+    @property
+    def info(self) -> dict:
+        inf = BatchInfo()
+        _check(_lib.piafs_gpu_batch_get_info(self._h, C.byref(inf)))
+        return inf.asdict()
+
+    def tune(self, tile_x: int = 0):
+        _check(_lib.piafs_gpu_batch_tune(self._h, int(tile_x)))
 
 
 def reciprocal(x, y):

@@ -147,4 +147,24 @@ __device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p
   return w1 * f1 + w2 * f2 + w3 * f3;
 }
 
+// The four WENO5 interface values at one interface (Interp1PrimFifthOrderWENO.c
+// for upw = +1 / -1 on u and f): a[0..5] and b[0..5] are u and f at cells
+// i-3 .. i+2 around interface i; left-biased stencils use cells i-3..i+1,
+// right-biased ones cells i+2..i-2.
+template <typename T>
+__device__ __forceinline__ void weno5_iface(const DevParams& P, const T* a, const T* b, T& uL, T& uR, T& fL,
+                                            T& fR) {
+  const T c1 = T(0.1), c2 = T(0.6), c3 = T(0.3), eps = (T)P.eps;
+  T w1, w2, w3;
+  if (P.no_limiting) { w1 = c1; w2 = c2; w3 = c3; }
+  else weno_weights(P.weno_type, c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
+  uL = weno5_value(w1, w2, w3, a[0], a[1], a[2], a[3], a[4]);
+  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, w1, w2, w3);
+  uR = weno5_value(w1, w2, w3, a[5], a[4], a[3], a[2], a[1]);
+  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, w1, w2, w3);
+  fL = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
+  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
+  fR = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
+}
+
 }  // namespace piafs

@@ -14,6 +14,7 @@
 #include <type_traits>
 #include "kernels.h"
 #include "physics.cuh"
+#include "source.cuh"
 
 namespace piafs {
 
@@ -100,44 +101,9 @@ __global__ void k_bc_zone(DevParams P, double* __restrict__ u, Zone z) {
   int ni = z.ie[0] - z.is[0], nj = z.ie[1] - z.is[1];
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (idx >= (long long)ni * nj) return;
-  int gi[2] = {z.is[0] + (int)(idx % ni), z.is[1] + (int)(idx / ni)};
-  int d = z.dim, b = gi[d] - z.is[d];
-  int src[2] = {gi[0], gi[1]};
-  int Nd = d == 0 ? P.N0 : P.N1;
-  if (z.type == BC_PERIODIC) {
-    // source keeps the zone-relative index in the other dimension
-    if (P.ndims == 2) src[1 - d] = gi[1 - d] - z.is[1 - d];
-    src[d] = z.face == 1 ? b + Nd - P.ghosts : b;
-  } else {
-    src[d] = z.face == 1 ? P.ghosts - 1 - b : Nd - b - 1;
-  }
-  long long p1 = pidx(P, gi[0], gi[1]), p2 = pidx(P, src[0], src[1]);
-  if (z.type == BC_SLIPWALL) {
-    double g = P.bc_gamma, igm1 = 1.0 / (g - 1.0);
-    if (P.ndims == 1) {
-      double rho, uv, e, pr;
-      eu_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], g, rho, uv, e, pr);
-      double ug = 2.0 * z.vel[0] - uv;
-      u[p1] = rho;
-      u[P.ps + p1] = rho * ug;
-      u[2 * P.ps + p1] = igm1 * pr + 0.5 * rho * ug * ug;
-    } else {
-      double rho, uv, vv, e, pr, ug, vg;
-      ns_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], u[3 * P.ps + p2], g, rho, uv, vv, e, pr);
-      if (d == 0) { ug = 2.0 * z.vel[0] - uv; vg = vv; }
-      else        { ug = uv; vg = 2.0 * z.vel[1] - vv; }
-      u[p1] = rho;
-      u[P.ps + p1] = rho * ug;
-      u[2 * P.ps + p1] = rho * vg;
-      u[3 * P.ps + p1] = igm1 * pr + 0.5 * rho * (ug * ug + vg * vg);
-    }
-  } else {
-    for (int v = 0; v < P.nvars; v++) u[v * P.ps + p1] = u[v * P.ps + p2];
-  }
+  const int g0 = z.is[0] + (int)(idx % ni), g1 = z.is[1] + (int)(idx / ni);
+  bc_point(P, z, u, g0, g1, u + pidx(P, g0, g1), P.ps);
 }
-
-// ======================================================================= RK
-// U_s = u + sum_{j<s} (dt a_sj) Udot_j at every point (TimeRK.c:46-57)
 __global__ void k_stage(long long n, double* __restrict__ Us, const double* __restrict__ u,
                         const double* __restrict__ d0, double a0, const double* __restrict__ d1, double a1,
                         const double* __restrict__ d2, double a2, int nterms) {
@@ -223,22 +189,15 @@ __global__ void k_flux(DevParams P, const double* __restrict__ U, double* __rest
   long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= P.npg) return;
   const long long ps = P.ps;
+  double f[4], vn;
   if (MODEL == NS2D) {
-    double rho, vx, vy, e, pr;
-    ns_flowvar(U[p], U[ps + p], U[2 * ps + p], U[3 * ps + p], P.gamma, rho, vx, vy, e, pr);
-    double vn = DIR == 0 ? vx : vy;
-    F[p] = rho * vn;
-    if (DIR == 0) { F[ps + p] = rho * vx * vx + pr; F[2 * ps + p] = rho * vx * vy; }
-    else          { F[ps + p] = rho * vy * vx; F[2 * ps + p] = rho * vy * vy + pr; }
-    F[3 * ps + p] = (e + pr) * vn;
-    for (int m = 4; m < P.nvars; m++) F[m * ps + p] = vn * U[m * ps + p];
+    ns2d_flux(U[p], U[ps + p], U[2 * ps + p], U[3 * ps + p], P.gamma, DIR, f, vn);
+    for (int m = 0; m < 4; m++) F[m * ps + p] = f[m];
+    for (int m = 4; m < P.nvars; m++) F[m * ps + p] = __dmul_rn(vn, U[m * ps + p]);
   } else {
-    double rho, v, e, pr;
-    eu_flowvar(U[p], U[ps + p], U[2 * ps + p], P.gamma, rho, v, e, pr);
-    F[p] = rho * v;
-    F[ps + p] = rho * v * v + pr;
-    F[2 * ps + p] = (e + pr) * v;
-    for (int m = 3; m < P.nvars; m++) F[m * ps + p] = v * U[m * ps + p];
+    euler1d_flux(U[p], U[ps + p], U[2 * ps + p], P.gamma, f, vn);
+    for (int m = 0; m < 3; m++) F[m * ps + p] = f[m];
+    for (int m = 3; m < P.nvars; m++) F[m * ps + p] = __dmul_rn(vn, U[m * ps + p]);
   }
 }
 
@@ -284,20 +243,9 @@ __global__ void k_weno5(DevParams P, const double* __restrict__ U, const double*
   R a[6], b[6];     // cells i-3 .. i+2
 #pragma unroll
   for (int r = 0; r < 6; r++) { a[r] = (R)(u[(r - 3) * st] - ru); b[r] = (R)(f[(r - 3) * st] - rf); }
-  const R c1 = R(0.1), c2 = R(0.6), c3 = R(0.3), eps = (R)P.eps;
-  R w1, w2, w3;
   const long long o = (long long)v * P.pis + q;
   R* uL = (R*)uLv; R* uR = (R*)uRv; R* fL = (R*)fLv; R* fR = (R*)fRv;
-  // left-biased: (m3..p2) = cells i-3..i+1 ; right-biased: cells i+2..i-2
-  if (P.no_limiting) { w1 = c1; w2 = c2; w3 = c3; }
-  else weno_weights(P.weno_type, c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
-  uL[o] = weno5_value(w1, w2, w3, a[0], a[1], a[2], a[3], a[4]);
-  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, w1, w2, w3);
-  uR[o] = weno5_value(w1, w2, w3, a[5], a[4], a[3], a[2], a[1]);
-  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, w1, w2, w3);
-  fL[o] = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
-  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
-  fR[o] = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
+  weno5_iface(P, a, b, uL[o], uR[o], fL[o], fR[o]);
 }
 
 // ============================================================ upwind + div
@@ -510,61 +458,6 @@ __global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double*
 // accumulation rhs += par; rhs += source (TimeRHSFunctionExplicit.c:67-74).
 // Tile: 32 x 8 interior points.  Cross-derivative terms at ghost columns/rows
 // are zero, as the reference computes derivatives on interior lines only.
-template <typename T>
-__device__ __forceinline__ void visc_coeffs(const DevParams& P, T Temp, T& mu, T& kappa) {
-  const T Td = Temp * (T)P.Tref, T0 = (T)P.T0;
-  const T r15 = exp(T(1.5) * log(Td / T0));   // raiseto (math_ops.h:40)
-  mu = r15 * (T0 + (T)P.TS) / (Td + (T)P.TS);
-  kappa = r15 * (T0 + (T)P.TA * exp(-(T)P.TB / T0)) / (Td + (T)P.TA * exp(-(T)P.TB / Td));
-}
-
-// ChemistrySetPhotonDensity (ChemistrySolve.c:18-65) + _ChemistrySetRHS_ /
-// _ChemistrySetQ_ (chemistry.h:30-137) at point p, arithmetic in T, added to
-// the FP64 rhs; the energy slot takes the heating of the last layer.
-template <typename T>
-__device__ void chem_source_point(const DevParams& P, const double* __restrict__ U, long long p,
-                                  double hnu_factor, double imap_p, double* __restrict__ rhs) {
-  const long long ps = P.ps;
-  T n_hnu = (T)(hnu_factor * imap_p / (P.ch_c * P.ch_h * P.ch_nu * P.n_O2));
-  const T k0a = (T)P.k[0], k0b = (T)P.k[1], k1a = (T)P.k[2], k1b = (T)P.k[3], k2a = (T)P.k[4], k2b = (T)P.k[5];
-  const T k3a = (T)P.k[6], k3b = (T)P.k[7], k4 = (T)P.k[8], k5 = (T)P.k[9], k6 = (T)P.k[10];
-  T Q = T(0);
-  for (int iz = 0; iz < P.nz; iz++) {
-    if (iz > 0) {
-      const T damp = T(1) - (T)P.dz * (T)(P.sO3 * P.n_O2) * (T)U[(P.nflow + P.zstride * (iz - 1) + 1) * ps + p];
-      n_hnu = n_hnu * damp;
-    }
-    const int nfv = P.nflow + P.zstride * iz;
-    const T nO2 = (T)U[(nfv + 0) * ps + p], nO3 = (T)U[(nfv + 1) * ps + p], n1D = (T)U[(nfv + 2) * ps + p];
-    const T n1Dg = (T)U[(nfv + 3) * ps + p], n3Su = (T)U[(nfv + 4) * ps + p], n1Sg = (T)U[(nfv + 5) * ps + p];
-    const T nCO2 = (T)U[(nfv + 6) * ps + p];
-    const T sO3 = -(k0a + k0b) * n_hnu * nO3 - (k2a + k2b) * nO3 * n1D - (k3a + k3b) * nO3 * n1Sg
-                  - k5 * nO3 * n3Su - k6 * n1Dg * nO3;
-    const T s1D = k0a * n_hnu * nO3 - (k1a + k1b) * n1D * nO2 - (k2a + k2b) * n1D * nO3 - k4 * n1D * nCO2;
-    const T s1Dg = k0a * n_hnu * nO3 + k5 * nO3 * n3Su - k6 * n1Dg * nO3;
-    const T s3Su = k2a * nO3 * n1D - k5 * nO3 * n3Su;
-    const T s1Sg = k1a * n1D * nO2 - (k3a + k3b) * nO3 * n1Sg;
-    rhs[(nfv + 1) * ps + p] += (double)sO3;
-    rhs[(nfv + 2) * ps + p] += (double)s1D;
-    rhs[(nfv + 3) * ps + p] += (double)s1Dg;
-    rhs[(nfv + 4) * ps + p] += (double)s3Su;
-    rhs[(nfv + 5) * ps + p] += (double)s1Sg;
-    Q = (((T)P.q[0] * k0a + (T)P.q[1] * k0b) * n_hnu * nO3 + ((T)P.q[2] * k1a + (T)P.q[3] * k1b) * nO2 * n1D
-         + ((T)P.q[4] * k2a + (T)P.q[5] * k2b) * nO3 * n1D + ((T)P.q[6] * k3a + (T)P.q[7] * k3b) * nO3 * n1Sg
-         + (T)P.q[8] * k4 * n1D * nCO2 + (T)P.q[9] * k5 * nO3 * n3Su + (T)P.q[10] * k6 * n1Dg * nO3)
-        / ((T)P.chem_gamma - T(1));
-  }
-  rhs[(P.nflow - 1) * ps + p] += (double)Q;
-}
-
-// pulse factor I0 exp(-(t - (t_start+t_pulse))^2 / (2 sigma^2)) or 0 before t_start
-__device__ __forceinline__ double pulse_factor(const DevParams& P, double t) {
-  if (!(t > P.t_start_norm)) return 0.0;
-  const double sigma = P.t_pulse_norm / 2.35482;
-  const double tp = t - (P.t_start_norm + P.t_pulse_norm);
-  return P.I0 * exp(-(tp * tp) / (2 * sigma * sigma));
-}
-
 // MX (mixed precision): velocities and temperature, their differences, the
 // viscous fluxes and the chemistry in FP32; the temperature is held relative
 // to the tile's first point (taken in FP64) so that its differences keep

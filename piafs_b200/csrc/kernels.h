@@ -27,6 +27,51 @@ struct Zone {
   double vel[2];
 };
 
+#ifdef __CUDACC__
+// Boundary values at ghost point (g0, g1) of zone z (BCPeriodic.c,
+// BCExtrapolate.c, BCSlipWall.c): reads the zone's source point of u (SoA
+// planes) and writes the ghost's variables to out[v * ostride] -- all of
+// them, or for a slip wall the flow variables only (the wall leaves the
+// others untouched).  The periodic source keeps the zone-relative index in
+// the other dimension, as the reference does.
+__device__ __forceinline__ void bc_point(const DevParams& P, const Zone& z, const double* u, int g0, int g1,
+                                         double* out, long long ostride) {
+  const int gi[2] = {g0, g1};
+  const int d = z.dim, b = gi[d] - z.is[d];
+  int src[2] = {g0, g1};
+  const int Nd = d == 0 ? P.N0 : P.N1;
+  if (z.type == BC_PERIODIC) {
+    if (P.ndims == 2) src[1 - d] = gi[1 - d] - z.is[1 - d];
+    src[d] = z.face == 1 ? b + Nd - P.ghosts : b;
+  } else {
+    src[d] = z.face == 1 ? P.ghosts - 1 - b : Nd - b - 1;
+  }
+  const long long p2 = pidx(P, src[0], src[1]);
+  if (z.type == BC_SLIPWALL) {
+    const double g = P.bc_gamma, igm1 = 1.0 / (g - 1.0);
+    if (P.ndims == 1) {
+      double rho, uv, e, pr;
+      eu_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], g, rho, uv, e, pr);
+      const double ug = 2.0 * z.vel[0] - uv;
+      out[0] = rho;
+      out[ostride] = rho * ug;
+      out[2 * ostride] = igm1 * pr + 0.5 * rho * ug * ug;
+    } else {
+      double rho, uv, vv, e, pr, ug, vg;
+      ns_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], u[3 * P.ps + p2], g, rho, uv, vv, e, pr);
+      if (d == 0) { ug = 2.0 * z.vel[0] - uv; vg = vv; }
+      else        { ug = uv; vg = 2.0 * z.vel[1] - vv; }
+      out[0] = rho;
+      out[ostride] = rho * ug;
+      out[2 * ostride] = rho * vg;
+      out[3 * ostride] = igm1 * pr + 0.5 * rho * (ug * ug + vg * vg);
+    }
+  } else {
+    for (int v = 0; v < P.nvars; v++) out[v * ostride] = u[v * P.ps + p2];
+  }
+}
+#endif
+
 void launch_aos_to_soa(const double* aos, double* soa, long long npg, int nv, long long ps, cudaStream_t s);
 void launch_soa_to_aos(const double* soa, double* aos, long long npg, int nv, long long ps, cudaStream_t s);
 void launch_soa_to_interior(const DevParams& P, const double* soa, double* out, cudaStream_t s);

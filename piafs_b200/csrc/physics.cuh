@@ -147,6 +147,36 @@ template <> struct Flow<EULER1D> {
   }
 };
 
+// Cell-centred fluxes of the flow variables along dir (NavierStokes2DFlux.c:
+// 24-52, Euler1DFlux.c) and the normal velocity that scales the passive
+// variables (F_m = vn u_m).  Products and sums are rounded operations that the
+// compiler never contracts into a neighbouring FMA, so a flux has the same
+// bits whether it is stored and reloaded (the single-simulation kernels) or
+// consumed in registers (the batched stage kernel).
+__device__ __forceinline__ void ns2d_flux(double u0, double u1, double u2, double u3, double gamma, int dir,
+                                          double* f, double& vn) {
+  double rho, vx, vy, e, pr;
+  ns_flowvar(u0, u1, u2, u3, gamma, rho, vx, vy, e, pr);
+  vn = dir == 0 ? vx : vy;
+  f[0] = __dmul_rn(rho, vn);
+  if (dir == 0) {
+    f[1] = __fma_rn(__dmul_rn(rho, vx), vx, pr);
+    f[2] = __dmul_rn(__dmul_rn(rho, vx), vy);
+  } else {
+    f[1] = __dmul_rn(__dmul_rn(rho, vy), vx);
+    f[2] = __fma_rn(__dmul_rn(rho, vy), vy, pr);
+  }
+  f[3] = __dmul_rn(__dadd_rn(e, pr), vn);
+}
+__device__ __forceinline__ void euler1d_flux(double u0, double u1, double u2, double gamma, double* f, double& vn) {
+  double rho, v, e, pr;
+  eu_flowvar(u0, u1, u2, gamma, rho, v, e, pr);
+  vn = v;
+  f[0] = __dmul_rn(rho, v);
+  f[1] = __fma_rn(__dmul_rn(rho, v), v, pr);
+  f[2] = __dmul_rn(__dadd_rn(e, pr), v);
+}
+
 template <typename T> __device__ __forceinline__ T absv(T a) { return a < T(0) ? -a : a; }
 template <typename T> __device__ __forceinline__ T maxv(T a, T b) { return a > b ? a : b; }
 template <typename T> __device__ __forceinline__ T max3v(T a, T b, T c) { return maxv(maxv(a, b), maxv(b, c)); }

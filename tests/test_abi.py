@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 import piafs_b200
 from conftest import ROOT
 
@@ -48,3 +50,16 @@ def test_unsupported_options_are_rejected(tmp_path):
 
 def test_cli_binary_is_built():
     assert os.access(piafs_b200.CLI_PATH, os.X_OK)
+
+
+def test_batch_entry_points_argument_checks():
+    lib = piafs_b200.load_library()
+    h = ctypes.c_void_p()
+    assert lib.piafs_gpu_batch_create(7, 0, ctypes.byref(h)) == 1
+    assert lib.piafs_gpu_batch_create(0, 0, None) == 1
+    assert lib.piafs_gpu_batch_step(None, 1) == 1
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        # no device: a CUDA error, reported, not a crash
+        assert lib.piafs_gpu_batch_create(0, 0, ctypes.byref(h)) == 4
+        assert lib.piafs_gpu_last_error()

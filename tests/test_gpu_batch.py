@@ -1,0 +1,169 @@
+"""Batched simulations (piafs_gpu_batch_*) against the same decks run alone.
+
+A batch advances many members, of different sizes, physics and step counts,
+with one persistent kernel per Runge-Kutta stage.  Its kernels evaluate the
+expressions of the single-simulation path, but the compiler contracts
+multiply-adds differently in the fused kernel, so a member agrees with its
+deck run alone through piafs_gpu_TimeRK to rounding: the FP64 parity bar
+(relative L2 <= 1e-12 per variable, variables without signal held to it in
+absolute terms).  A tile's arithmetic depends only on its own member, so a
+member's result is bit for bit the same alone in a batch, in any mix, and
+whenever it joins.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from piafs_b200 import Batch, PiafsError, Simulation, cases, deck
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_WENO = ["euler1d_weno5_roe_n1024", "euler1d_weno5_llf_yc_rk4_n128", "ns2d_chem_weno5_llf_48x40",
+               "ns2d_shear_weno5_roe_re200_40x32"]
+
+
+TOL = 1e-12
+NOISE_FLOOR = 1e-6
+
+
+def assert_close(got, ref, what=""):
+    rms = np.sqrt((ref * ref).mean(axis=0))
+    scale = rms.max()
+    worst = 0.0
+    for v in range(ref.shape[1]):
+        d = got[:, v] - ref[:, v]
+        if rms[v] < NOISE_FLOOR * scale:
+            err = np.sqrt((d * d).mean()) / scale
+        else:
+            err = np.sqrt((d * d).sum() / (ref[:, v] ** 2).sum())
+        worst = max(worst, err)
+    assert np.all(np.isfinite(got)) and worst <= TOL, f"{what}: {worst:.2e}"
+
+
+def in_batch_alone(d, steps, tile_x=0):
+    with Batch() as b:
+        if tile_x:
+            b.tune(tile_x)
+        i = b.add(d, steps)
+        b.step(steps)
+        return b.solution(i)
+
+
+def alone(d, steps):
+    with Simulation(d) as s:
+        s.time_rk(steps)
+        return s.solution()
+
+
+def make_mix(root):
+    """Small decks of every member kind, sizes off the tile grid."""
+    out = []
+    for k, (n, ny, amp) in enumerate([(96, 96, 0.7), (64, 160, 1.3), (50, 37, 1.0)]):
+        d = os.path.join(root, f"beam{k}")
+        cases.ns2d_photochem_beam(d, N=n, NY=ny, n_iter=12, scheme="weno5", op_file_format="none",
+                                  dt=0.4 / 2048, beam_amp=amp, seed=k)
+        out.append((d, 12))
+    d = os.path.join(root, "euler300")
+    cases.euler1d_density_wave(d, N=300, n_iter=40, dt=1e-4, scheme="weno5", op_file_format="none")
+    out.append((d, 40))
+    for name in GOLDEN_WENO:
+        d = os.path.join(GOLDEN, name)
+        n = int(deck.read_keyfile(os.path.join(d, "solver.inp"))["n_iter"][0])
+        out.append((d, min(n, 60)))
+    return out
+
+
+def test_batch_members_match_single_runs(tmp_path):
+    mix = make_mix(str(tmp_path))
+    with Batch() as b:
+        ids = [b.add(d, n) for d, n in mix]
+        assert b.info["members"] == len(mix)
+        b.step(max(n for _, n in mix))
+        done = b.poll()
+        assert sorted(done) == sorted(ids)
+        for (d, n), i in zip(mix, ids):
+            m = b.member(i)
+            assert m["iter"] == n and m["done"]
+            got = b.solution(i)
+            assert_close(got, alone(d, n), d)
+            # the mix does not change a member's bits
+            assert np.array_equal(got, in_batch_alone(d, n)), d
+
+
+def test_batch_golden_decks_match_the_reference():
+    """Full-length golden WENO5 runs in one batch against the reference's
+    own output (the FP64 parity bar)."""
+    with Batch() as b:
+        ids = {name: b.add(os.path.join(GOLDEN, name)) for name in GOLDEN_WENO}
+        b.step(1000)
+        for name, i in ids.items():
+            got = b.solution(i)
+            ref = deck.read_op(os.path.join(GOLDEN, name, "ref_final.bin")).u
+            num = np.sqrt(((got - ref) ** 2).sum(axis=0))
+            den = np.sqrt((ref ** 2).sum(axis=0))
+            rel = np.where(den > 1e-15, num / np.maximum(den, 1e-300), num)
+            assert rel.max() <= 1e-12, (name, rel)
+
+
+def test_continuous_batching_join_leave(tmp_path):
+    """Members join while others run and leave when done; each result is bit
+    for bit the result of the member alone in a batch."""
+    mix = make_mix(str(tmp_path))
+    with Batch() as b:
+        first = [b.add(d, n) for d, n in mix[:3]]
+        b.step(5)
+        later = [b.add(d, n) for d, n in mix[3:]]
+        finished = []
+        for _ in range(200):
+            b.step(3)
+            finished += b.poll()
+            if len(finished) == len(mix):
+                break
+        assert sorted(finished) == sorted(first + later)
+        for (d, n), i in zip(mix, first + later):
+            assert np.array_equal(b.solution(i), in_batch_alone(d, n)), d
+        for i in first:
+            b.remove(i)
+        assert b.info["members"] == len(later)
+
+
+@pytest.mark.parametrize("tile_x", [16, 64])
+def test_tile_shapes(tmp_path, tile_x):
+    mix = make_mix(str(tmp_path))[:4]
+    with Batch() as b:
+        b.tune(tile_x)
+        ids = [b.add(d, n) for d, n in mix]
+        b.step(max(n for _, n in mix))
+        assert b.info["tile_x"] == tile_x
+        for (d, n), i in zip(mix, ids):
+            got = b.solution(i)
+            assert_close(got, alone(d, n), d)
+            assert np.array_equal(got, in_batch_alone(d, n, tile_x)), d
+
+
+def test_budget_admission_and_rejections(tmp_path):
+    d = os.path.join(str(tmp_path), "b")
+    cases.ns2d_photochem_beam(d, N=64, n_iter=4, scheme="weno5", op_file_format="none", dt=0.4 / 2048)
+    with Batch(hbm_budget_bytes=1) as b:
+        with pytest.raises(PiafsError) as ex:
+            b.add(d)
+        assert ex.value.code == 7
+    with Batch() as b:
+        i = b.add(d)
+        one = b.info["bytes_in_use"]
+    with Batch(hbm_budget_bytes=int(one * 1.5)) as b:
+        i = b.add(d)
+        with pytest.raises(PiafsError):
+            b.add(d)
+        b.step(4)
+        assert b.poll() == [i]
+        b.remove(i)
+        b.add(d)                      # memory freed: admitted again
+    c = os.path.join(str(tmp_path), "c")
+    cases.ns2d_photochem_beam(c, N=64, n_iter=4, scheme="crweno5", op_file_format="none", dt=0.4 / 2048)
+    with Batch() as b:
+        with pytest.raises(PiafsError) as ex:
+            b.add(c)
+        assert ex.value.code == 3
