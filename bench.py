@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--workload", default="ns2d_photochem", choices=["ns2d_photochem", "euler1d"])
+    ap.add_argument("--workload", default="ns2d_photochem", choices=["ns2d_photochem", "euler1d", "ensemble"])
+    ap.add_argument("--members", type=int, default=256, help="ensemble members")
+    ap.add_argument("--member-steps", type=int, default=100, help="steps per ensemble member")
     ap.add_argument("--n", type=int, default=None, help="grid size (default 2048 / 1024)")
     ap.add_argument("--scheme", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -199,6 +201,102 @@ def cpu_baseline(a):
     return {"value": v, "unit": "pt-stage updates/s", "cores": cores, "kind": kind, "sample": sample}
 
 
+# ----------------------------------------------------------------- ensemble
+def rel_l2_noise_floor(got, ref, floor=1e-6):
+    import numpy as np
+    rms = np.sqrt((ref * ref).mean(axis=0))
+    scale = rms.max()
+    worst = 0.0
+    for v in range(ref.shape[1]):
+        d = got[:, v] - ref[:, v]
+        if rms[v] < floor * scale:
+            e = np.sqrt((d * d).mean()) / scale
+        else:
+            e = np.sqrt((d * d).sum() / (ref[:, v] ** 2).sum())
+        worst = max(worst, float(e))
+    return worst
+
+
+def ensemble_bench(a):
+    """The batched ensemble: every member of cases.ensemble solved (deck read,
+    device set-up, steps, solution back to the host) in one batch, against
+    the same members solved one at a time through Simulation (FP64).  Both
+    are wall-clock times of complete solves on one GPU; the batched step
+    phase is also reported as grid-point RK-stage updates per second."""
+    import numpy as np
+    import torch
+    from piafs_b200 import Batch, Simulation, cases
+
+    torch.cuda.init()
+    n, steps = a.members, a.member_steps
+    tmp = tempfile.mkdtemp(prefix="piafs_ensemble_")
+    try:
+        mem = cases.ensemble(tmp, n=n, steps=steps)
+        sides = [m["side"] for m in mem]
+        npts = sum(s * s for s in sides)
+        # warm the CUDA context and the kernels' modules outside the timing
+        with Batch(precision=a.precision) as B:
+            B.add(mem[0]["dir"], 1)
+            B.step(1)
+        with Simulation(mem[0]["dir"]) as s:
+            s.time_rk(1)
+        torch.cuda.synchronize()
+        # the launch configuration for this class of ensemble (the autotuner,
+        # run once on the full mix; its choice is reused by later ensembles
+        # of the class, so it is timed apart from the solves)
+        t0 = time.perf_counter()
+        with Batch(precision=a.precision) as B:
+            B.add_many([m["dir"] for m in mem], [steps] * n)
+            B.tune()
+            tuned = B.info
+        tune_s = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with Batch(precision=a.precision) as B:
+            B.set_launch(tuned["tile_x"], tuned["tile_y"], tuned["min_ctas_per_sm"])
+            ids = B.add_many([m["dir"] for m in mem], [steps] * n)
+            t1 = time.perf_counter()
+            admit = t1 - t0
+            B.step(steps)
+            t2 = time.perf_counter()
+            sols = [B.solution(i) for i in ids]
+            t3 = time.perf_counter()
+            binfo = B.info
+        batched = t3 - t0
+        worst = 0.0
+        t0 = time.perf_counter()
+        one = []
+        for m in mem:
+            with Simulation(m["dir"]) as s:
+                s.time_rk(steps)
+                one.append(s.solution())
+        single = time.perf_counter() - t0
+        for sb, so in zip(sols, one):
+            worst = max(worst, rel_l2_noise_floor(sb, so))
+        finite = all(bool(np.isfinite(x).all()) for x in sols)
+        units = 3 * steps * npts
+        line = {"metric": "ensemble solves/s", "value": n / batched, "unit": "solves/s", "n_gpus": 1,
+                "higher_is_better": True, "vs_baseline": None,
+                "dtype": "f64" if a.precision == "fp64" else "f32+f64",
+                "data": "synthetic (seeded ensemble decks)",
+                "config": {"workload": f"ensemble_{n}_ns2d_photochem_weno5_llf_ssprk3_{steps}steps",
+                           "members": n, "steps": steps, "sides": [min(sides), max(sides)],
+                           "total_points": npts, "precision": a.precision,
+                           "tile": [binfo["tile_x"], binfo["tile_y"]],
+                           "min_ctas_per_sm": binfo["min_ctas_per_sm"], "tune_s": tune_s,
+                           "launches_per_step": binfo["launches_per_step"]},
+                "batched": {"wall_s": batched, "admit_s": admit,
+                            "step_s": t2 - t1, "pt_stage_updates_per_s": units / (t2 - t1),
+                            "results_s": t3 - t2},
+                "one_at_a_time": {"wall_s": single, "solves_per_s": n / single, "precision": "fp64"},
+                "speedup_vs_one_at_a_time": single / batched,
+                "accuracy": {"max_rel_l2_vs_one_at_a_time": worst}, "finite": finite}
+        print(json.dumps(line))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
 # --------------------------------------------------------------------- main
 def main():
     a = parse()
@@ -207,6 +305,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     n_gpus = max(world, 1)
     metric = "pt-stage updates/s"
+
+    if a.workload == "ensemble" and a.impl == "gpu":
+        return ensemble_bench(a) if rank == 0 else 0
 
     if a.impl == "reference":
         if rank != 0:

@@ -184,6 +184,7 @@ typedef struct {
   unsigned long long bytes_in_use;  /* member state held on the device    */
   unsigned long long budget_bytes;  /* 0: no limit                        */
   int launches_per_step;            /* kernels one batch step launches    */
+  int min_ctas_per_sm;              /* occupancy the stage kernel is built for */
 } piafs_gpu_batch_info;
 /* hbm_budget_bytes bounds the device memory the members' state may take
  * (0: no bound); precision is PIAFS_PRECISION_*. */
@@ -194,6 +195,11 @@ void piafs_gpu_batch_destroy(piafs_gpu_batch* batch);
  * PIAFS_ERR_MEMORY, with nothing changed, when the budget cannot hold it now,
  * and PIAFS_ERR_UNSUPPORTED for decks outside the batched path. */
 int piafs_gpu_batch_add(piafs_gpu_batch* batch, const char* deck_dir, int nsteps, int* id);
+/* piafs_gpu_batch_add for n decks, parsed in parallel by host threads and
+ * admitted in order; nsteps may be NULL (every deck's n_iter).  Stops at the
+ * first failure; *n_added members were admitted, their ids in ids[]. */
+int piafs_gpu_batch_add_many(piafs_gpu_batch* batch, const char* const* deck_dirs, int n, const int* nsteps,
+                             int* ids, int* n_added);
 /* Advance every active member by up to nsteps steps; a member stops after
  * its own step count.  Waits for the device. */
 int piafs_gpu_batch_step(piafs_gpu_batch* batch, int nsteps);
@@ -209,11 +215,17 @@ int piafs_gpu_batch_get_stage_derivative(piafs_gpu_batch* batch, int id, int sta
 /* Release a member's device memory (finished or not). */
 int piafs_gpu_batch_remove(piafs_gpu_batch* batch, int id);
 int piafs_gpu_batch_get_info(piafs_gpu_batch* batch, piafs_gpu_batch_info* info);
-/* Pick the 2D tile shape for the current members by timing each candidate
- * on a copy-free dry run of one step (the members' state is saved and
- * restored); tile_x/tile_y report the choice.  Candidates 0 = automatic;
- * or force a shape with tile_x * tile_y = 256 (32x8, 16x16, 64x4). */
+/* Autotuner: with force_tile_x = 0, time every launch configuration of the
+ * stage kernel (2D tile 32x8, 16x16 or 64x4, each compiled for one or two
+ * CTAs per SM) on the current members -- one warm-up and two timed steps
+ * each, the members' state saved before and restored after every trial --
+ * and keep the fastest; info.tile_x / tile_y / min_ctas_per_sm report it.
+ * A nonzero force_tile_x selects that tile width (one CTA per SM) instead. */
 int piafs_gpu_batch_tune(piafs_gpu_batch* batch, int force_tile_x);
+/* Select a launch configuration directly, e.g. one an earlier tune chose for
+ * the same class of members (tile_x x tile_y = 32x8, 16x16 or 64x4;
+ * min_ctas_per_sm 1 or 2). */
+int piafs_gpu_batch_set_launch(piafs_gpu_batch* batch, int tile_x, int tile_y, int min_ctas_per_sm);
 
 /* ---- diagnostics ----
  * No counterpart in the reference.  y[i] = 1/x[i] (device arrays) computed

@@ -69,6 +69,8 @@ SIGNATURES = {
     "piafs_gpu_batch_destroy": (None, [_vp]),
     "piafs_gpu_batch_add": (C.c_int, [_vp, C.c_char_p, C.c_int, C.POINTER(C.c_int)]),
     "piafs_gpu_batch_step": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_batch_add_many": (C.c_int, [_vp, C.POINTER(C.c_char_p), C.c_int, C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "piafs_gpu_batch_poll": (C.c_int, [_vp, C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int)]),
     "piafs_gpu_batch_get_solution": (C.c_int, [_vp, C.c_int, _dp]),
     "piafs_gpu_batch_member": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_int),
@@ -77,6 +79,7 @@ SIGNATURES = {
     "piafs_gpu_batch_get_stage_derivative": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
     "piafs_gpu_batch_get_info": (C.c_int, [_vp, _vp]),
     "piafs_gpu_batch_tune": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_batch_set_launch": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
 }
 
 
@@ -305,7 +308,7 @@ class BatchInfo(C.Structure):
     _fields_ = [
         ("members", C.c_int), ("active", C.c_int), ("tiles", C.c_int), ("tile_x", C.c_int),
         ("tile_y", C.c_int), ("steps", C.c_longlong), ("bytes_in_use", C.c_ulonglong),
-        ("budget_bytes", C.c_ulonglong), ("launches_per_step", C.c_int),
+        ("budget_bytes", C.c_ulonglong), ("launches_per_step", C.c_int), ("min_ctas_per_sm", C.c_int),
     ]
 
     def asdict(self):
@@ -350,6 +353,20 @@ class Batch:
         self._shapes[i.value] = (int(np.prod(size)), int(d["nvars"][0]))
         return i.value
 
+    def add_many(self, deck_dirs, nsteps=None) -> list:
+        """Admit many members; decks are parsed in parallel host threads."""
+        n = len(deck_dirs)
+        dirs = (C.c_char_p * n)(*[os.fsencode(d) for d in deck_dirs])
+        steps = (C.c_int * n)(*[int(x) for x in nsteps]) if nsteps is not None else None
+        ids = (C.c_int * n)()
+        added = C.c_int()
+        code = _lib.piafs_gpu_batch_add_many(self._h, dirs, n, steps, ids, C.byref(added))
+        for k in range(added.value):
+            d = deck.read_keyfile(os.path.join(deck_dirs[k], "solver.inp"))
+            self._shapes[ids[k]] = (int(np.prod([int(x) for x in d["size"]])), int(d["nvars"][0]))
+        _check(code)
+        return list(ids)
+
     def step(self, nsteps: int = 1):
         _check(_lib.piafs_gpu_batch_step(self._h, int(nsteps)))
 
@@ -387,7 +404,12 @@ class Batch:
         return inf.asdict()
 
     def tune(self, tile_x: int = 0):
+        """Autotune the launch configuration on the current members (tile_x =
+        0), or force a tile width."""
         _check(_lib.piafs_gpu_batch_tune(self._h, int(tile_x)))
+
+    def set_launch(self, tile_x: int, tile_y: int, min_ctas_per_sm: int = 1):
+        _check(_lib.piafs_gpu_batch_set_launch(self._h, int(tile_x), int(tile_y), int(min_ctas_per_sm)))
 
 
 def reciprocal(x, y):

@@ -228,3 +228,37 @@ def ns2d_density_wave(path: str, N: int = 64, NY: Optional[int] = None, axis: in
                                                            "Pr": 0.72})
     deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, 4))
     return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}
+
+
+def ensemble(root: str, n: int = 256, steps: int = 100, seed: int = 1, side_range=(64, 512),
+             dt: float = 0.4 / 2048, op_file_format: str = "none"):
+    """The batched-ensemble workload: ``n`` independent 2D photochemical
+    Navier-Stokes members (``ns2d_photochem_beam`` decks) with grid sides
+    drawn log-uniformly in ``side_range`` and rounded to multiples of 32, beam
+    amplitude U(0.5, 1.5), beam 1/e radius U(0.02, 0.1) and Re log-uniform in
+    [1e3, 1e5] (realised through the beam half-angle, Re ~ 1/sin(theta));
+    WENO5, LLF, SSPRK3, ``steps`` steps.  The normalised heating pulse
+    shortens as 1/Re (the half-angle sets the acoustic time scale), and
+    explicit viscosity bounds dt by the diffusion number, so each member takes
+    dt = min(0.4 dx, dt_2048 * 1e4 / Re, 0.1 Re dx^2) with dx = 1/side: CFL
+    0.4, capped at the pulse resolution of the 2048^2 workload at Re = 1e4
+    (dt_2048 = 0.4/2048, about 35 steps per pulse width) and at a diffusion
+    number nu dt / dx^2 of about 0.2 for the thermal diffusivity
+    gamma / (Pr Re).  Member k's field noise uses seed 1000 * seed + k."""
+    rng = np.random.default_rng(seed)
+    lo, hi = side_range
+    out = []
+    for k in range(n):
+        side = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) / 32.0)) * 32
+        side = min(max(side, 32 * math.ceil(lo / 32)), hi)
+        amp = float(rng.uniform(0.5, 1.5))
+        radius = float(rng.uniform(0.02, 0.1))
+        Re = float(math.exp(rng.uniform(math.log(1e3), math.log(1e5))))
+        theta = math.asin(min(1.0, math.sin(THETA_RE_1E4) * 1e4 / Re))
+        d = os.path.join(root, f"member{k:04d}")
+        mdt = min(0.4 / side, dt * 1e4 / Re, 0.1 * Re / (side * side))
+        ns2d_photochem_beam(d, N=side, n_iter=steps, scheme="weno5", seed=1000 * seed + k, beam_amp=amp,
+                            beam_radius=radius, theta=theta, Re=Re, dt=mdt, op_file_format=op_file_format)
+        out.append({"dir": d, "side": side, "beam_amp": amp, "beam_radius": radius, "Re": Re, "steps": steps,
+                    "dt": mdt})
+    return out

@@ -31,7 +31,9 @@
 // except for one-stage schemes, which write buffer 0 and swap it with u.
 #include <algorithm>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -49,9 +51,9 @@ using namespace piafs;
 
 namespace {
 
-constexpr int BT = 256;          // threads of the stage kernel
+constexpr int BT = 512;          // threads of the stage kernel
 constexpr int H = 3;             // halo (WENO5 stencil half-width)
-constexpr int T1 = 256;          // points of a 1D tile
+constexpr int T1 = 512;          // points of a 1D tile
 
 // Host-written description of one member.
 struct BMember {
@@ -83,76 +85,74 @@ struct BState {
 // Value of every variable at tile point (i, j) of stage state S: interior
 // points from memory, edge ghosts (exactly one index outside the domain, at
 // most 3 deep) from the last boundary zone that covers them, other points 0
-// (corners; never used by the stencils).
+// (corners; never used by the stencils).  A slip wall sets the flow variables
+// and leaves the others as they are in memory, as the boundary kernel does.
 __device__ __forceinline__ void load_point(const BMember& M, const double* S, int i, int j, double* out,
                                            int ostride) {
   const DevParams& P = M.P;
   const bool xin = i >= 0 && i < P.N0, yin = j >= 0 && j < P.N1;
   const int nv = P.nvars;
-  if (xin && yin) {
-    const long long p = pidx(P, i, j);
-    for (int v = 0; v < nv; v++) out[v * ostride] = S[v * P.ps + p];
-    return;
-  }
-  const bool edge = (yin && i >= -P.ghosts && i < P.N0 + P.ghosts) ||
-                    (P.ndims == 2 && xin && j >= -P.ghosts && j < P.N1 + P.ghosts);
-  if (!edge) {
+  const bool edge = !(xin && yin) && ((yin && i >= -P.ghosts && i < P.N0 + P.ghosts) ||
+                                      (P.ndims == 2 && xin && j >= -P.ghosts && j < P.N1 + P.ghosts));
+  if (!(xin && yin) && !edge) {
     for (int v = 0; v < nv; v++) out[v * ostride] = 0.0;
     return;
   }
-  // memory value first (what a slip wall leaves untouched), then the zone
   const long long p = pidx(P, i, j);
   for (int v = 0; v < nv; v++) out[v * ostride] = S[v * P.ps + p];
+  if (!edge) return;
   for (int zi = M.nzones - 1; zi >= 0; zi--) {
     const Zone& z = M.zones[zi];
     if (i >= z.is[0] && i < z.ie[0] && j >= z.is[1] && j < z.ie[1]) {
-      double tmp[32];
-      bc_point(P, z, S, i, j, tmp, 1);
-      const int nw = z.type == BC_SLIPWALL ? (P.ndims == 2 ? 4 : 3) : nv;
-      for (int v = 0; v < nw; v++) out[v * ostride] = tmp[v];
+      bc_point(P, z, S, i, j, out, ostride);
       return;
     }
   }
 }
 
-// Upwind flux of every variable at the interface between the cells at smem
-// offsets cell(r) = base + (r - 3) * st (r = 0..5 for cells i-3..i+2) of the
-// tile state sU ([v][...], plane stride vs); result to so[v * sstride].
-template <int MODEL, int UPW>
-__device__ __forceinline__ void iface_flux(const DevParams& P, const double* sU, int vs, int base, int st, int dir,
-                                           double* so, int sstride) {
+// Cell-centred fluxes of every variable at a tile cell (ns2d_flux /
+// euler1d_flux, passive variables vn u_m) into f[m * fstride]; vn returned.
+template <int MODEL>
+__device__ __forceinline__ double cell_flux(const DevParams& P, const double* sU, int vs, int c, int dir, double* f,
+                                            int fstride) {
   constexpr int NF = Flow<MODEL>::NF;
-  double fc[4][6], vn[6];
+  double fl[4] = {0.0, 0.0, 0.0, 0.0}, vn;
+  if (MODEL == NS2D) ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, dir, fl, vn);
+  else euler1d_flux(sU[c], sU[vs + c], sU[2 * vs + c], P.gamma, fl, vn);
 #pragma unroll
-  for (int r = 0; r < 6; r++) {
-    const int c = base + (r - 3) * st;
-    double f[4] = {0.0, 0.0, 0.0, 0.0}, w;
-    if (MODEL == NS2D) ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, dir, f, w);
-    else euler1d_flux(sU[c], sU[vs + c], sU[2 * vs + c], P.gamma, f, w);
+  for (int m = 0; m < NF; m++) f[m * fstride] = fl[m];
+  for (int m = NF; m < P.nvars; m++) f[m * fstride] = __dmul_rn(vn, sU[m * vs + c]);
+  return vn;
+}
+
+// The four WENO5 values of one variable at one interface: u at u[(r-3)*ust]
+// and its flux at f[(r-3)*fst] for the cells r = 0..5 (i-3..i+2).
+__device__ __forceinline__ void iface_weno(const DevParams& P, const double* u, int ust, const double* f, int fst,
+                                           double& uL, double& uR, double& fL, double& fR) {
+  double a[6], b[6];
 #pragma unroll
-    for (int m = 0; m < NF; m++) fc[m][r] = f[m];
-    vn[r] = w;
-  }
-  double uL[4], uR[4], fL[4], fR[4], ucl[4], ucr[4], fi[4], spa;
-  int spm;
+  for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * ust]; b[r] = f[(r - 3) * fst]; }
+  weno5_iface(P, a, b, uL, uR, fL, fR);
+}
+
+// Characteristic / scalar upwinding of the flow variables at one interface
+// from their stored WENO values rec[k * rs + m] (k: uL, uR, fL, fR) and the
+// cell states left / right (ucl, ucr at stride vs); flux to so[m * sstride],
+// passive-variable scheme data to *spa / *spm.
+template <int MODEL, int UPW>
+__device__ __noinline__ void iface_upwind_flow(const DevParams& P, const double* rec, int rs, const double* ucl,
+                                               const double* ucr, int vs, int dir, double* so, int sstride,
+                                               double* spa, int* spm) {
+  constexpr int NF = Flow<MODEL>::NF;
+  double uL[4], uR[4], fL[4], fR[4], cl[4], cr[4], fi[4];
 #pragma unroll
   for (int m = 0; m < NF; m++) {
-    double a[6];
-#pragma unroll
-    for (int r = 0; r < 6; r++) a[r] = sU[m * vs + base + (r - 3) * st];
-    weno5_iface(P, a, fc[m], uL[m], uR[m], fL[m], fR[m]);
-    ucl[m] = a[2]; ucr[m] = a[3];
+    uL[m] = rec[m]; uR[m] = rec[rs + m]; fL[m] = rec[2 * rs + m]; fR[m] = rec[3 * rs + m];
+    cl[m] = ucl[m * vs]; cr[m] = ucr[m * vs];
   }
-  upwind_flow<MODEL, UPW, double>(uL, uR, fL, fR, ucl, ucr, P.gamma, dir, fi, &spa, &spm);
+  upwind_flow<MODEL, UPW, double>(uL, uR, fL, fR, cl, cr, P.gamma, dir, fi, spa, spm);
 #pragma unroll
   for (int m = 0; m < NF; m++) so[m * sstride] = fi[m];
-  for (int m = NF; m < P.nvars; m++) {
-    double a[6], b[6], l, r, fl, fr;
-#pragma unroll
-    for (int q = 0; q < 6; q++) { a[q] = sU[m * vs + base + (q - 3) * st]; b[q] = __dmul_rn(vn[q], a[q]); }
-    weno5_iface(P, a, b, l, r, fl, fr);
-    so[m * sstride] = upwind_species(spm, spa, l, r, fl, fr);
-  }
 }
 
 // the Runge-Kutta part of stage s at point p with stage derivatives k
@@ -178,48 +178,129 @@ __device__ __forceinline__ void rk_point(const BMember& M, const BState& Sd, int
 }
 
 // ------------------------------------------------------------- 2D tile
-// shared memory (doubles): sU [nv][TY+6][TX+6], sFx [nv][TY][TX+1],
-// sFy [nv][TX][TY+2], Q [3][TY+2][TX+2], viscous fluxes [3][TY][TX+1] and
-// [3][TY+1][TX]
+// One tile of TX x TY points, worked by BT threads in phases separated by
+// barriers, each phase a list of small items so that every thread stays light
+// (many warps per SM):
+//   load        the stage state on the tile + 3-cell halo (boundary ghosts on
+//               the fly)
+//   per direction d = x, y:
+//     fluxes    cell-centred fluxes of every variable at the stencil cells
+//     flow WENO WENO5 values of the flow variables, item = (interface, var)
+//     upwind    characteristic/scalar upwinding, item = interface
+//     passive   WENO5 + scalar upwinding of a passive variable, item =
+//               (interface, var)
+//   viscous     Q, viscous face fluxes (k_visc_source on the tile)
+//   point       stage derivative, chemistry, Runge-Kutta combination
+// Shared memory (doubles): sU [nv][HY][HX]; interface fluxes fx [nv][NXI]
+// and fy [nv][NYI]; a work region reused by the directions and then by the
+// viscous phase: cell fluxes [nv][NC], flow WENO values [4][4][NI], passive
+// speed [NI] and scheme [NI] (ints).
 template <int TX, int TY>
-__host__ __device__ constexpr long long smem2d(int nv) {
-  return (long long)nv * ((TY + 2 * H) * (TX + 2 * H) + TY * (TX + 1) + TX * (TY + 2)) +
-         3LL * (TY + 2) * (TX + 2) + 3LL * TY * (TX + 1) + 3LL * (TY + 1) * TX;
-}
+struct Tile2D {
+  static constexpr int HX = TX + 6, HY = TY + 6;
+  static constexpr int NXI = TY * (TX + 1), NYI = TX * (TY + 1);
+  static constexpr int NI = NXI > NYI ? NXI : NYI;
+  static constexpr int NCX = TY * HX, NCY = TX * HY;            // stencil cells per direction
+  static constexpr int NC = NCX > NCY ? NCX : NCY;
+  static constexpr int VISC = 3 * (TY + 2) * (TX + 2) + 3 * TY * (TX + 1) + 3 * (TY + 1) * TX;
+  __host__ __device__ static constexpr long long work(int nv) {
+    return (long long)nv * NC + 16LL * NI + 2LL * NI > VISC ? (long long)nv * NC + 16LL * NI + 2LL * NI : VISC;
+  }
+  __host__ __device__ static constexpr long long smem(int nv) {
+    return (long long)nv * (HX * HY + NXI + NYI) + work(nv);
+  }
+};
+template <int TX, int TY>
+__host__ __device__ constexpr long long smem2d(int nv) { return Tile2D<TX, TY>::smem(nv); }
 
 template <int TX, int TY, int UPW>
-__device__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, double* smem) {
+__device__ __noinline__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, double* smem) {
+  typedef Tile2D<TX, TY> T;
+  constexpr int HX = T::HX, HY = T::HY, NXI = T::NXI, NYI = T::NYI, NI = T::NI;
   const DevParams& P = M.P;
-  constexpr int HX = TX + 2 * H, HY = TY + 2 * H, LX = TX + 1, LY = TY + 2;
   const int nv = P.nvars, N0 = P.N0, N1 = P.N1;
   const int i0 = tx * TX, j0 = ty * TY;
   const double* S = s == 0 ? Sd.u : ((s - 1) % 2 == 0 ? M.X : M.Y);
-  const int vs = HX * HY;
+  constexpr int vs = HX * HY;
   double* sU = smem;
-  double* sFx = sU + nv * vs;
-  double* sFy = sFx + nv * TY * LX;
-  double* sQ = sFy + nv * TX * LY;              // [3][TY+2][TX+2]
-  double* sVx = sQ + 3 * (TY + 2) * (TX + 2);   // [3][TY][TX+1]
-  double* sVy = sVx + 3 * TY * (TX + 1);        // [3][TY+1][TX]
+  double* fx = sU + nv * vs;                   // [m][jj * (TX+1) + ii]
+  double* fy = fx + nv * NXI;                  // [m][ii * (TY+1) + jj]
+  double* wk = fy + nv * NYI;                  // work region
+  double* cf = wk;                             // cell fluxes [m][NC]
+  double* rec = cf + nv * T::NC;               // flow WENO values [k][m][NI]
+  double* spa = rec + 16 * NI;                 // passive speed [NI]
+  int* spm = (int*)(spa + NI);                 // passive scheme [NI]
   const int tid = threadIdx.x;
   for (int e = tid; e < vs; e += BT) load_point(M, S, i0 - H + e % HX, j0 - H + e / HX, sU + e, vs);
   __syncthreads();
-  // x interfaces (TX+1 per tile row)
-  for (int e = tid; e < LX * TY; e += BT) {
-    const int ii = e % LX, jj = e / LX, i = i0 + ii, j = j0 + jj;
-    if (i > N0 || j >= N1) continue;
-    iface_flux<NS2D, UPW>(P, sU, vs, (jj + H) * HX + ii + H, 1, 0, sFx + jj * LX + ii, TY * LX);
+  constexpr int NF = 4;
+  const int np = nv - NF;
+#pragma unroll 1
+  for (int d = 0; d < 2; d++) {
+    // stencil cells of direction d: x: rows jj, columns a = 0..HX-1; y:
+    // columns ii, rows b = 0..HY-1; cell c's smem offset
+    const int ncell = d == 0 ? T::NCX : T::NCY;
+    const int ni = d == 0 ? NXI : NYI;
+    for (int e = tid; e < ncell; e += BT) {
+      const int c = d == 0 ? (e / HX + H) * HX + e % HX : (e % HY) * HX + e / HY + H;
+      cell_flux<NS2D>(P, sU, vs, c, d, cf + e, T::NC);
+    }
+    __syncthreads();
+    // interface f of direction d: line l, position k along the line; its
+    // cell i (right of the interface) in smem and in the cell-flux array
+    auto geo = [&](int f, int& base, int& ust, int& fbase, bool& ok) {
+      if (d == 0) {
+        const int ii = f % (TX + 1), jj = f / (TX + 1);
+        ok = i0 + ii <= N0 && j0 + jj < N1;
+        base = (jj + H) * HX + ii + H; ust = 1; fbase = jj * HX + ii + H;
+      } else {
+        const int jj = f % (TY + 1), ii = f / (TY + 1);
+        ok = j0 + jj <= N1 && i0 + ii < N0;
+        base = (jj + H) * HX + ii + H; ust = HX; fbase = ii * HY + jj + H;
+      }
+    };
+    for (int e = tid; e < NF * ni; e += BT) {
+      const int m = e / ni, f = e % ni;
+      int base, ust, fbase; bool ok;
+      geo(f, base, ust, fbase, ok);
+      if (!ok) continue;
+      iface_weno(P, sU + m * vs + base, ust, cf + m * T::NC + fbase, 1, rec[(0 * NF + m) * NI + f],
+                 rec[(1 * NF + m) * NI + f], rec[(2 * NF + m) * NI + f], rec[(3 * NF + m) * NI + f]);
+    }
+    __syncthreads();
+    double* fo = d == 0 ? fx : fy;
+    for (int f = tid; f < ni; f += BT) {
+      int base, ust, fbase; bool ok;
+      geo(f, base, ust, fbase, ok);
+      if (!ok) continue;
+      // rec[k][m][f] with stride NI between variables: gather into the layout
+      // iface_upwind_flow reads (k * rs + m), rs = 4
+      double r16[16];
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+#pragma unroll
+        for (int m = 0; m < NF; m++) r16[k * NF + m] = rec[(k * NF + m) * NI + f];
+      iface_upwind_flow<NS2D, UPW>(P, r16, NF, sU + base - ust, sU + base, vs, d, fo + f, ni, spa + f, spm + f);
+    }
+    __syncthreads();
+    for (int e = tid; e < np * ni; e += BT) {
+      const int m = NF + e / ni, f = e % ni;
+      int base, ust, fbase; bool ok;
+      geo(f, base, ust, fbase, ok);
+      if (!ok) continue;
+      double l, r, fl, fr;
+      iface_weno(P, sU + m * vs + base, ust, cf + m * T::NC + fbase, 1, l, r, fl, fr);
+      fo[m * ni + f] = upwind_species(spm[f], spa[f], l, r, fl, fr);
+    }
+    __syncthreads();
   }
-  // y interfaces (TY+1 per tile column)
-  for (int e = tid; e < TX * (TY + 1); e += BT) {
-    const int ii = e % TX, jj = e / TX, i = i0 + ii, j = j0 + jj;
-    if (j > N1 || i >= N0) continue;
-    iface_flux<NS2D, UPW>(P, sU, vs, (jj + H) * HX + ii + H, HX, 1, sFy + ii * LY + jj, TX * LY);
-  }
-  // viscous fluxes (k_visc_source on this tile)
+  // viscous fluxes (k_visc_source on this tile), in the work region
   const bool visc = P.viscous != 0;
+  constexpr int QX = TX + 2, QY = TY + 2, FX = TX + 1, FY = TY + 1;
+  double* sQ = wk;                              // [3][QY][QX]
+  double* sVx = sQ + 3 * QY * QX;               // [3][TY][FX]
+  double* sVy = sVx + 3 * TY * FX;              // [3][FY][TX]
   if (visc) {
-    constexpr int QX = TX + 2, QY = TY + 2, FX = TX + 1, FY = TY + 1;
     for (int e = tid; e < QX * QY; e += BT) {
       const int a = e % QX, b = e / QX;
       const int i = i0 - 1 + a, j = j0 - 1 + b;
@@ -269,23 +350,24 @@ __device__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty
         f[0] = tyx; f[FY * TX] = tyy; f[2 * FY * TX] = uc * tyx + vc * tyy + kre * Ty;
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
   // stage derivative and the Runge-Kutta combination, one point per thread
+  if (tid >= TX * TY) return;
   const int pi = tid % TX, pj = tid / TX, i = i0 + pi, j = j0 + pj;
-  if (pj >= TY || i >= N0 || j >= N1) return;
+  if (i >= N0 || j >= N1) return;
   const long long p = pidx(P, i, j);
   const long long ps = P.ps;
   double* ks = M.k[s];
   const double dxi = M.dxinv[P.ghosts + i], dyi = M.dxinv[P.W0 + P.ghosts + j];
+  constexpr int LX = TX + 1, LY = TY + 1;
   for (int m = 0; m < nv; m++) {
-    const double hx = dxi * (sFx[m * TY * LX + pj * LX + pi + 1] - sFx[m * TY * LX + pj * LX + pi]);
-    const double hy = dyi * (sFy[m * TX * LY + pi * LY + pj + 1] - sFy[m * TX * LY + pi * LY + pj]);
+    const double hx = dxi * (fx[m * NXI + pj * LX + pi + 1] - fx[m * NXI + pj * LX + pi]);
+    const double hy = dyi * (fy[m * NYI + pi * LY + pj + 1] - fy[m * NYI + pi * LY + pj]);
     const double h = hx + hy;
     ks[m * ps + p] = -h;
   }
   if (visc) {
-    constexpr int FX = TX + 1, FY = TY + 1;
 #pragma unroll
     for (int m = 0; m < 3; m++) {
       const double par = dxi * (sVx[m * TY * FX + pj * FX + pi + 1] - sVx[m * TY * FX + pj * FX + pi]) +
@@ -301,29 +383,57 @@ __device__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty
 }
 
 // ------------------------------------------------------------- 1D tile
-// shared memory (doubles): sU [nv][T1+6], sF [nv][T1+1]
-__host__ __device__ constexpr long long smem1d(int nv) { return (long long)nv * ((T1 + 2 * H) + (T1 + 1)); }
+// shared memory (doubles): sU [nv][T1+6], cell fluxes [nv][T1+6], interface
+// fluxes [nv][T1+1], flow WENO values [4][3][T1+1], passive speed and scheme
+__host__ __device__ constexpr long long smem1d(int nv) {
+  return (long long)nv * (2 * (T1 + 2 * H) + (T1 + 1)) + 14LL * (T1 + 1);
+}
 
 template <int UPW>
-__device__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double* smem) {
+__device__ __noinline__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double* smem) {
   const DevParams& P = M.P;
-  constexpr int HX = T1 + 2 * H, LX = T1 + 1;
+  constexpr int HX = T1 + 2 * H, LX = T1 + 1, NF = 3;
   const int nv = P.nvars, N0 = P.N0;
   const int i0 = tx * T1;
   const double* S = s == 0 ? Sd.u : ((s - 1) % 2 == 0 ? M.X : M.Y);
   double* sU = smem;
-  double* sF = sU + nv * HX;
+  double* cf = sU + nv * HX;                 // [m][HX]
+  double* sF = cf + nv * HX;                 // [m][LX]
+  double* rec = sF + nv * LX;                // [k][m][LX]
+  double* spa = rec + 12 * LX;
+  int* spm = (int*)(spa + LX);
   const int tid = threadIdx.x;
   for (int e = tid; e < HX; e += BT) load_point(M, S, i0 - H + e, 0, sU + e, HX);
   __syncthreads();
-  for (int e = tid; e < LX; e += BT) {
-    const int i = i0 + e;
-    if (i > N0) continue;
-    iface_flux<EULER1D, UPW>(P, sU, HX, e + H, 1, 0, sF + e, LX);
+  for (int e = tid; e < HX; e += BT) cell_flux<EULER1D>(P, sU, HX, e, 0, cf + e, HX);
+  __syncthreads();
+  for (int e = tid; e < NF * LX; e += BT) {
+    const int m = e / LX, f = e % LX;
+    if (i0 + f > N0) continue;
+    iface_weno(P, sU + m * HX + f + H, 1, cf + m * HX + f + H, 1, rec[(0 * NF + m) * LX + f],
+               rec[(1 * NF + m) * LX + f], rec[(2 * NF + m) * LX + f], rec[(3 * NF + m) * LX + f]);
+  }
+  __syncthreads();
+  for (int f = tid; f < LX; f += BT) {
+    if (i0 + f > N0) continue;
+    double r12[12];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+#pragma unroll
+      for (int m = 0; m < NF; m++) r12[k * NF + m] = rec[(k * NF + m) * LX + f];
+    iface_upwind_flow<EULER1D, UPW>(P, r12, NF, sU + f + H - 1, sU + f + H, HX, 0, sF + f, LX, spa + f, spm + f);
+  }
+  __syncthreads();
+  for (int e = tid; e < (nv - NF) * LX; e += BT) {
+    const int m = NF + e / LX, f = e % LX;
+    if (i0 + f > N0) continue;
+    double l, r, fl, fr;
+    iface_weno(P, sU + m * HX + f + H, 1, cf + m * HX + f + H, 1, l, r, fl, fr);
+    sF[m * LX + f] = upwind_species(spm[f], spa[f], l, r, fl, fr);
   }
   __syncthreads();
   const int i = i0 + tid;
-  if (i >= N0) return;
+  if (tid >= T1 || i >= N0) return;
   const long long p = pidx(P, i, 0);
   double* ks = M.k[s];
   const double dxi = M.dxinv[P.ghosts + i];
@@ -335,8 +445,8 @@ __device__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double
 }
 
 // --------------------------------------------------------------- kernels
-template <int TX, int TY>
-__global__ void __launch_bounds__(BT) k_batch_stage(const BMember* __restrict__ mem, const BState* __restrict__ st,
+template <int TX, int TY, int MINB>
+__global__ void __launch_bounds__(BT, MINB) k_batch_stage(const BMember* __restrict__ mem, const BState* __restrict__ st,
                                                     const int* __restrict__ tile_member,
                                                     const int* __restrict__ ntiles, int s) {
   extern __shared__ double smem[];
@@ -403,8 +513,34 @@ int nfail(int code, const std::string& m) { return piafs::set_last_error(code, m
     if (e_ != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
   } while (0)
 
-struct TileShape { int tx, ty; };
-constexpr TileShape kShapes[3] = {{32, 8}, {16, 16}, {64, 4}};
+// Launch configurations the tuner chooses from: tile shape and the minimum
+// CTAs per SM the compiler is asked to fit (2 trades registers for spills).
+struct TileShape { int tx, ty, minb; };
+constexpr int kNumShapes = 3;
+constexpr TileShape kShapes[kNumShapes] = {{16, 16, 1}, {32, 8, 1}, {64, 4, 1}};
+
+template <int TX, int TY, int MINB>
+struct StageOps {
+  static long long smem(int nv) { return std::max(smem2d<TX, TY>(nv), smem1d(nv)) * (long long)sizeof(double); }
+  static cudaError_t attr(long long bytes) {
+    return cudaFuncSetAttribute(k_batch_stage<TX, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  }
+  static int per_sm(long long bytes) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<TX, TY, MINB>, BT, bytes) != cudaSuccess) n = 0;
+    return n;
+  }
+  static void launch(int grid, long long bytes, cudaStream_t st, const BMember* m, const BState* s, const int* tl,
+                     const int* nt, int stage) {
+    k_batch_stage<TX, TY, MINB><<<grid, BT, bytes, st>>>(m, s, tl, nt, stage);
+  }
+};
+#define PIAFS_SHAPE_SWITCH(idx, CALL)                      \
+  switch (idx) {                                           \
+    case 0: { typedef StageOps<16, 16, 1> Ops; CALL; } break; \
+    case 1: { typedef StageOps<32, 8, 1> Ops; CALL; } break;  \
+    default: { typedef StageOps<64, 4, 1> Ops; CALL; } break; \
+  }
 
 }  // namespace
 
@@ -433,40 +569,16 @@ struct piafs_gpu_batch {
 namespace {
 
 long long smem_bytes(int shape, int nv) {
-  long long d2 = 0;
-  switch (shape) {
-    case 0: d2 = smem2d<32, 8>(nv); break;
-    case 1: d2 = smem2d<16, 16>(nv); break;
-    default: d2 = smem2d<64, 4>(nv); break;
-  }
-  return std::max(d2, smem1d(nv)) * (long long)sizeof(double);
-}
-
-template <int TX, int TY>
-cudaError_t launch_stage_shape(piafs_gpu_batch* B, int grid, int s) {
-  const long long sm = smem_bytes(B->shape, B->max_nv);
-  k_batch_stage<TX, TY><<<grid, BT, sm, B->stream>>>(B->dmem, B->dstate, B->dtiles, B->dntiles, s);
-  return cudaGetLastError();
-}
-
-cudaError_t set_smem_attr(int shape, long long bytes) {
-  switch (shape) {
-    case 0: return cudaFuncSetAttribute(k_batch_stage<32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    case 1: return cudaFuncSetAttribute(k_batch_stage<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    default: return cudaFuncSetAttribute(k_batch_stage<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  }
+  long long r = 0;
+  PIAFS_SHAPE_SWITCH(shape, r = Ops::smem(nv));
+  return r;
 }
 
 int persistent_grid(piafs_gpu_batch* B) {
   const long long sm = smem_bytes(B->shape, std::max(B->max_nv, 1));
   int per_sm = 0;
-  cudaError_t e;
-  switch (B->shape) {
-    case 0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_stage<32, 8>, BT, sm); break;
-    case 1: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_stage<16, 16>, BT, sm); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_stage<64, 4>, BT, sm); break;
-  }
-  if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+  PIAFS_SHAPE_SWITCH(B->shape, per_sm = Ops::per_sm(sm));
+  if (per_sm < 1) per_sm = 1;
   return per_sm * B->num_sms;
 }
 
@@ -548,16 +660,17 @@ int capture_graph(piafs_gpu_batch* B) {
     return PIAFS_OK;
   if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
   const long long sm = smem_bytes(B->shape, B->max_nv);
-  BCK(set_smem_attr(B->shape, sm));
+  {
+    cudaError_t ea = cudaSuccess;
+    PIAFS_SHAPE_SWITCH(B->shape, ea = Ops::attr(sm));
+    BCK(ea);
+  }
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int s = 0; s < B->max_stages && e == cudaSuccess; s++) {
-    switch (B->shape) {
-      case 0: e = launch_stage_shape<32, 8>(B, grid, s); break;
-      case 1: e = launch_stage_shape<16, 16>(B, grid, s); break;
-      default: e = launch_stage_shape<64, 4>(B, grid, s); break;
-    }
+    PIAFS_SHAPE_SWITCH(B->shape, Ops::launch(grid, sm, B->stream, B->dmem, B->dstate, B->dtiles, B->dntiles, s));
+    e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
     k_batch_epilogue<<<(B->cap + 127) / 128, 128, 0, B->stream>>>(B->dmem, B->dstate, B->cap, B->dstatus);
@@ -576,70 +689,25 @@ int capture_graph(piafs_gpu_batch* B) {
 
 }  // namespace
 
-extern "C" {
-
-int piafs_gpu_batch_create(int precision, unsigned long long budget, piafs_gpu_batch** out) {
-  if (!out) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
-  *out = nullptr;
-  if (precision != PIAFS_PRECISION_FP64 && precision != PIAFS_PRECISION_MIXED)
-    return nfail(PIAFS_ERR_ARGUMENT, "precision must be PIAFS_PRECISION_FP64 or PIAFS_PRECISION_MIXED");
-  if (precision == PIAFS_PRECISION_MIXED)
-    return nfail(PIAFS_ERR_UNSUPPORTED, "the batched path runs FP64 members in this build");
-  auto* B = new piafs_gpu_batch();
-  B->precision = precision;
-  B->budget = budget;
-  cudaError_t e = cudaGetDevice(&B->device);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&B->num_sms, cudaDevAttrMultiProcessorCount, B->device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMallocAsync(&B->dntiles, sizeof(int), B->stream);
-  if (e == cudaSuccess) {
-    // keep freed member memory in the pool instead of returning it to the driver
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, B->device) == cudaSuccess) {
-      unsigned long long thr = ~0ull;
-      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
-  }
-  if (e != cudaSuccess) {
-    if (B->stream) cudaStreamDestroy(B->stream);
-    delete B;
-    return nfail(PIAFS_ERR_CUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
-  }
-  if (int r = grow_slots(B, 16)) { delete B; return r; }
-  *out = B;
-  return PIAFS_OK;
-}
-
-void piafs_gpu_batch_destroy(piafs_gpu_batch* B) {
-  if (!B) return;
-  cudaStreamSynchronize(B->stream);
-  if (B->graph) cudaGraphExecDestroy(B->graph);
-  for (auto& m : B->members)
-    if (m.block) cudaFreeAsync(m.block, B->stream);
-  if (B->dmem) cudaFreeAsync(B->dmem, B->stream);
-  if (B->dstate) cudaFreeAsync(B->dstate, B->stream);
-  if (B->dstatus) cudaFreeAsync(B->dstatus, B->stream);
-  if (B->dtiles) cudaFreeAsync(B->dtiles, B->stream);
-  if (B->dntiles) cudaFreeAsync(B->dntiles, B->stream);
-  cudaStreamSynchronize(B->stream);
-  if (B->hstatus) cudaFreeHost(B->hstatus);
-  cudaStreamDestroy(B->stream);
-  delete B;
-}
-
-int piafs_gpu_batch_add(piafs_gpu_batch* B, const char* deck_dir, int nsteps, int* id) {
-  if (!B || !deck_dir || !id) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
-  HostMember hm;
-  std::string err;
+namespace {
+// Parse and check one member's deck (host only; safe to run in parallel).
+int parse_member(const char* deck_dir, HostMember& hm, DevParams& P, std::string& err) {
   int r = read_deck(deck_dir, hm.deck, err);
-  DevParams P;
   if (!r) r = make_params(hm.deck, P, err);
-  if (r) return nfail(r, err);
+  if (r) return r;
+  if (P.scheme != WENO5) { err = "batched members use hyp_space_scheme weno5"; return PIAFS_ERR_UNSUPPORTED; }
+  if (!((P.ndims == 2 && P.model == NS2D) || (P.ndims == 1 && P.model == EULER1D && !P.chem))) {
+    err = "batched members are 2D navierstokes2d or 1D euler1d without chemistry";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if (P.nvars > 32) { err = "batched members have at most 32 variables"; return PIAFS_ERR_UNSUPPORTED; }
+  return 0;
+}
+}  // namespace
+
+namespace {
+int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, int* id) {
   const Deck& d = hm.deck;
-  if (P.scheme != WENO5) return nfail(PIAFS_ERR_UNSUPPORTED, "batched members use hyp_space_scheme weno5");
-  if (!((P.ndims == 2 && P.model == NS2D) || (P.ndims == 1 && P.model == EULER1D && !P.chem)))
-    return nfail(PIAFS_ERR_UNSUPPORTED, "batched members are 2D navierstokes2d or 1D euler1d without chemistry");
-  if (P.nvars > 32) return nfail(PIAFS_ERR_UNSUPPORTED, "batched members have at most 32 variables");
   {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B->device);
@@ -722,6 +790,94 @@ int piafs_gpu_batch_add(piafs_gpu_batch* B, const char* deck_dir, int nsteps, in
   *id = slot;
   return PIAFS_OK;
 }
+}  // namespace
+
+extern "C" {
+
+int piafs_gpu_batch_create(int precision, unsigned long long budget, piafs_gpu_batch** out) {
+  if (!out) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
+  if (precision != PIAFS_PRECISION_FP64 && precision != PIAFS_PRECISION_MIXED)
+    return nfail(PIAFS_ERR_ARGUMENT, "precision must be PIAFS_PRECISION_FP64 or PIAFS_PRECISION_MIXED");
+  if (precision == PIAFS_PRECISION_MIXED)
+    return nfail(PIAFS_ERR_UNSUPPORTED, "the batched path runs FP64 members in this build");
+  auto* B = new piafs_gpu_batch();
+  B->precision = precision;
+  B->budget = budget;
+  cudaError_t e = cudaGetDevice(&B->device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&B->num_sms, cudaDevAttrMultiProcessorCount, B->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMallocAsync(&B->dntiles, sizeof(int), B->stream);
+  if (e == cudaSuccess) {
+    // keep freed member memory in the pool instead of returning it to the driver
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, B->device) == cudaSuccess) {
+      unsigned long long thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
+  if (e != cudaSuccess) {
+    if (B->stream) cudaStreamDestroy(B->stream);
+    delete B;
+    return nfail(PIAFS_ERR_CUDA, std::string("batch set-up: ") + cudaGetErrorString(e));
+  }
+  if (int r = grow_slots(B, 16)) { delete B; return r; }
+  *out = B;
+  return PIAFS_OK;
+}
+
+void piafs_gpu_batch_destroy(piafs_gpu_batch* B) {
+  if (!B) return;
+  cudaStreamSynchronize(B->stream);
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  for (auto& m : B->members)
+    if (m.block) cudaFreeAsync(m.block, B->stream);
+  if (B->dmem) cudaFreeAsync(B->dmem, B->stream);
+  if (B->dstate) cudaFreeAsync(B->dstate, B->stream);
+  if (B->dstatus) cudaFreeAsync(B->dstatus, B->stream);
+  if (B->dtiles) cudaFreeAsync(B->dtiles, B->stream);
+  if (B->dntiles) cudaFreeAsync(B->dntiles, B->stream);
+  cudaStreamSynchronize(B->stream);
+  if (B->hstatus) cudaFreeHost(B->hstatus);
+  cudaStreamDestroy(B->stream);
+  delete B;
+}
+
+
+int piafs_gpu_batch_add(piafs_gpu_batch* B, const char* deck_dir, int nsteps, int* id) {
+  if (!B || !deck_dir || !id) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
+  HostMember hm;
+  DevParams P;
+  std::string err;
+  if (int r = parse_member(deck_dir, hm, P, err)) return nfail(r, err);
+  return admit_member(B, std::move(hm), P, nsteps, id);
+}
+
+int piafs_gpu_batch_add_many(piafs_gpu_batch* B, const char* const* deck_dirs, int n, const int* nsteps, int* ids,
+                             int* n_added) {
+  if (!B || (n > 0 && (!deck_dirs || !ids)) || n < 0 || !n_added) return nfail(PIAFS_ERR_ARGUMENT, "bad argument");
+  *n_added = 0;
+  std::vector<HostMember> hms(n);
+  std::vector<DevParams> Ps(n);
+  std::vector<std::string> errs(n);
+  std::vector<int> rcs(n, 0);
+  // decks are parsed by a pool of host threads, then admitted in order
+  const int nt = std::max(1, std::min<int>(n, (int)std::thread::hardware_concurrency()));
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  for (int w = 0; w < nt; w++)
+    pool.emplace_back([&]() {
+      for (int k = next++; k < n; k = next++) rcs[k] = parse_member(deck_dirs[k], hms[k], Ps[k], errs[k]);
+    });
+  for (auto& th : pool) th.join();
+  for (int k = 0; k < n; k++) {
+    if (rcs[k]) return nfail(rcs[k], std::string(deck_dirs[k]) + ": " + errs[k]);
+    if (int r = admit_member(B, std::move(hms[k]), Ps[k], nsteps ? nsteps[k] : 0, ids + k)) return r;
+    *n_added = k + 1;
+  }
+  return PIAFS_OK;
+}
+
 
 int piafs_gpu_batch_step(piafs_gpu_batch* B, int nsteps) {
   if (!B || nsteps < 0) return nfail(PIAFS_ERR_ARGUMENT, "bad argument");
@@ -829,6 +985,7 @@ int piafs_gpu_batch_get_info(piafs_gpu_batch* B, piafs_gpu_batch_info* info) {
   info->bytes_in_use = B->used;
   info->budget_bytes = B->budget;
   info->launches_per_step = B->max_stages + 1;
+  info->min_ctas_per_sm = kShapes[B->shape].minb;
   return PIAFS_OK;
 }
 
@@ -836,14 +993,94 @@ int piafs_gpu_batch_tune(piafs_gpu_batch* B, int force_tile_x) {
   if (!B) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
   if (force_tile_x) {
     int k = -1;
-    for (int i = 0; i < 3; i++)
+    for (int i = 0; i < kNumShapes && k < 0; i++)
       if (kShapes[i].tx == force_tile_x) k = i;
     if (k < 0) return nfail(PIAFS_ERR_ARGUMENT, "tile_x must be 32, 16 or 64");
     B->shape = k;
     B->dirty = true;
     return PIAFS_OK;
   }
-  return nfail(PIAFS_ERR_UNSUPPORTED, "automatic tuning is not available in this build");
+  // Time every launch configuration on the current members (one warm-up
+  // step, then two timed steps each) and keep the fastest.  The members'
+  // solution, clocks and step counts are saved before and restored after
+  // every trial, so tuning leaves the batch as it found it.
+  if (B->dirty) if (int r = sync_tables(B)) return r;
+  if (B->ntiles == 0) return PIAFS_OK;
+  std::vector<BState> saved(B->cap);
+  BCK(cudaMemcpyAsync(saved.data(), B->dstate, (size_t)B->cap * sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
+  BCK(cudaStreamSynchronize(B->stream));
+  std::vector<std::pair<double*, size_t>> copies;   // (device copy, doubles) per member slot
+  copies.resize(B->members.size(), {nullptr, 0});
+  cudaError_t e = cudaSuccess;
+  for (size_t i = 0; i < B->members.size() && e == cudaSuccess; i++) {
+    const HostMember& hm = B->members[i];
+    if (!hm.used) continue;
+    const size_t n = (size_t)hm.bm.P.nvars * hm.bm.P.ps;
+    e = cudaMallocAsync((void**)&copies[i].first, n * sizeof(double), B->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(copies[i].first, saved[i].u, n * sizeof(double), cudaMemcpyDeviceToDevice, B->stream);
+    copies[i].second = n;
+  }
+  auto restore = [&]() -> cudaError_t {
+    cudaError_t r = cudaSuccess;
+    for (size_t i = 0; i < copies.size() && r == cudaSuccess; i++)
+      if (copies[i].first)
+        r = cudaMemcpyAsync(saved[i].u, copies[i].first, copies[i].second * sizeof(double),
+                            cudaMemcpyDeviceToDevice, B->stream);
+    if (r == cudaSuccess)
+      r = cudaMemcpyAsync(B->dstate, saved.data(), (size_t)B->cap * sizeof(BState), cudaMemcpyHostToDevice,
+                          B->stream);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(B->stream);
+    return r;
+  };
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B->device);
+  const int keep = B->shape;
+  int best = keep;
+  float best_ms = 1e30f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  for (int c = 0; c < kNumShapes && e == cudaSuccess; c++) {
+    if (smem_bytes(c, B->max_nv) > optin) continue;
+    B->shape = c;
+    B->dirty = true;
+    if (int r = sync_tables(B)) { e = cudaErrorUnknown; (void)r; break; }
+    if (int r = capture_graph(B)) { e = cudaErrorUnknown; (void)r; break; }
+    e = cudaGraphLaunch(B->graph, B->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, B->stream);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) e = cudaGraphLaunch(B->graph, B->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, B->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess && ms < best_ms) { best_ms = ms; best = c; }
+    if (e == cudaSuccess) e = restore();
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (auto& cp : copies)
+    if (cp.first) cudaFreeAsync(cp.first, B->stream);
+  cudaStreamSynchronize(B->stream);
+  B->shape = e == cudaSuccess ? best : keep;
+  B->dirty = true;
+  if (e != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string("tuning: ") + cudaGetErrorString(e));
+  return sync_tables(B);
+}
+
+int piafs_gpu_batch_set_launch(piafs_gpu_batch* B, int tile_x, int tile_y, int minb) {
+  if (!B) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
+  for (int i = 0; i < kNumShapes; i++)
+    if (kShapes[i].tx == tile_x && kShapes[i].ty == tile_y && kShapes[i].minb == minb) {
+      int optin = 0;
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B->device);
+      if (smem_bytes(i, B->max_nv) > optin)
+        return nfail(PIAFS_ERR_UNSUPPORTED, "this tile does not fit the members' variables in shared memory");
+      B->shape = i;
+      B->dirty = true;
+      return PIAFS_OK;
+    }
+  return nfail(PIAFS_ERR_ARGUMENT, "no such launch configuration");
 }
 
 }  // extern "C"

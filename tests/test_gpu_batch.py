@@ -167,3 +167,27 @@ def test_budget_admission_and_rejections(tmp_path):
         with pytest.raises(PiafsError) as ex:
             b.add(c)
         assert ex.value.code == 3
+
+
+def test_autotuner_restores_state_and_picks_a_config(tmp_path):
+    mix = make_mix(str(tmp_path))[:5]
+    with Batch() as b:
+        ids = b.add_many([d for d, _ in mix], [n for _, n in mix])
+        b.step(3)
+        before = [b.solution(i) for i in ids]
+        iters = [b.member(i)["iter"] for i in ids]
+        b.tune()
+        assert [b.member(i)["iter"] for i in ids] == iters
+        for i, u in zip(ids, before):
+            assert np.array_equal(b.solution(i), u)
+        info = b.info
+        assert info["tile_x"] * info["tile_y"] == 256 and info["min_ctas_per_sm"] in (1, 2)
+        b.step(200)
+        for (d, n), i in zip(mix, ids):
+            assert_close(b.solution(i), alone(d, n), d)
+        # the same configuration set explicitly gives the same bits
+        with Batch() as c:
+            c.set_launch(info["tile_x"], info["tile_y"], info["min_ctas_per_sm"])
+            j = c.add(mix[0][0], mix[0][1])
+            c.step(mix[0][1])
+            assert np.array_equal(c.solution(j), b.solution(ids[0]))
