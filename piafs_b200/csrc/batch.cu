@@ -51,9 +51,7 @@ using namespace piafs;
 
 namespace {
 
-constexpr int BT = 512;          // threads of the stage kernel
 constexpr int H = 3;             // halo (WENO5 stencil half-width)
-constexpr int T1 = 512;          // points of a 1D tile
 
 // Host-written description of one member.
 struct BMember {
@@ -136,18 +134,18 @@ __device__ __forceinline__ void iface_weno(const DevParams& P, const double* u, 
 }
 
 // Characteristic / scalar upwinding of the flow variables at one interface
-// from their stored WENO values rec[k * rs + m] (k: uL, uR, fL, fR) and the
-// cell states left / right (ucl, ucr at stride vs); flux to so[m * sstride],
+// from their WENO values rec[k * ks + m * ms] (k: uL, uR, fL, fR) and the cell
+// states left / right (ucl, ucr at stride vs); flux to so[m * sstride],
 // passive-variable scheme data to *spa / *spm.
 template <int MODEL, int UPW>
-__device__ __noinline__ void iface_upwind_flow(const DevParams& P, const double* rec, int rs, const double* ucl,
-                                               const double* ucr, int vs, int dir, double* so, int sstride,
-                                               double* spa, int* spm) {
+__device__ __noinline__ void iface_upwind_flow(const DevParams& P, const double* rec, int ks, int ms,
+                                               const double* ucl, const double* ucr, int vs, int dir, double* so,
+                                               int sstride, double* spa, int* spm) {
   constexpr int NF = Flow<MODEL>::NF;
   double uL[4], uR[4], fL[4], fR[4], cl[4], cr[4], fi[4];
 #pragma unroll
   for (int m = 0; m < NF; m++) {
-    uL[m] = rec[m]; uR[m] = rec[rs + m]; fL[m] = rec[2 * rs + m]; fR[m] = rec[3 * rs + m];
+    uL[m] = rec[m * ms]; uR[m] = rec[ks + m * ms]; fL[m] = rec[2 * ks + m * ms]; fR[m] = rec[3 * ks + m * ms];
     cl[m] = ucl[m * vs]; cr[m] = ucr[m * vs];
   }
   upwind_flow<MODEL, UPW, double>(uL, uR, fL, fR, cl, cr, P.gamma, dir, fi, spa, spm);
@@ -179,44 +177,42 @@ __device__ __forceinline__ void rk_point(const BMember& M, const BState& Sd, int
 
 // ------------------------------------------------------------- 2D tile
 // One tile of TX x TY points, worked by BT threads in phases separated by
-// barriers, each phase a list of small items so that every thread stays light
-// (many warps per SM):
-//   load        the stage state on the tile + 3-cell halo (boundary ghosts on
-//               the fly)
-//   per direction d = x, y:
-//     fluxes    cell-centred fluxes of every variable at the stencil cells
-//     flow WENO WENO5 values of the flow variables, item = (interface, var)
-//     upwind    characteristic/scalar upwinding, item = interface
-//     passive   WENO5 + scalar upwinding of a passive variable, item =
-//               (interface, var)
-//   viscous     Q, viscous face fluxes (k_visc_source on the tile)
-//   point       stage derivative, chemistry, Runge-Kutta combination
-// Shared memory (doubles): sU [nv][HY][HX]; interface fluxes fx [nv][NXI]
-// and fy [nv][NYI]; a work region reused by the directions and then by the
-// viscous phase: cell fluxes [nv][NC], flow WENO values [4][4][NI], passive
-// speed [NI] and scheme [NI] (ints).
+// barriers; each phase is a list of small items over both directions, so
+// every thread stays light and the phases stay balanced:
+//   load     the stage state on the tile + 3-cell halo (boundary ghosts on
+//            the fly)
+//   fluxes   flow-variable fluxes and the normal velocity at every stencil
+//            cell of either direction
+//   WENO     WENO5 values of the flow variables, item = (interface, var)
+//   upwind   characteristic/scalar upwinding, item = interface
+//   passive  WENO5 + scalar upwinding of a passive variable (flux vn u_m),
+//            item = (interface, var)
+//   viscous  Q, viscous face fluxes (k_visc_source on the tile)
+//   point    stage derivative, chemistry, Runge-Kutta combination
+// Interfaces are numbered x first (f < NXI: row jj, position ii) then y.
+// Shared memory (doubles): sU [nv][HY][HX]; interface fluxes fx [nv][NXI] and
+// fy [nv][NYI]; a work region, reused by the viscous phase: cell data
+// [5][NCX] + [5][NCY], WENO values [4][4][NXI+NYI], passive speed and scheme
+// [NXI+NYI] each.
 template <int TX, int TY>
 struct Tile2D {
   static constexpr int HX = TX + 6, HY = TY + 6;
-  static constexpr int NXI = TY * (TX + 1), NYI = TX * (TY + 1);
-  static constexpr int NI = NXI > NYI ? NXI : NYI;
+  static constexpr int NXI = TY * (TX + 1), NYI = TX * (TY + 1), NI = NXI + NYI;
   static constexpr int NCX = TY * HX, NCY = TX * HY;            // stencil cells per direction
-  static constexpr int NC = NCX > NCY ? NCX : NCY;
   static constexpr int VISC = 3 * (TY + 2) * (TX + 2) + 3 * TY * (TX + 1) + 3 * (TY + 1) * TX;
-  __host__ __device__ static constexpr long long work(int nv) {
-    return (long long)nv * NC + 16LL * NI + 2LL * NI > VISC ? (long long)nv * NC + 16LL * NI + 2LL * NI : VISC;
-  }
+  static constexpr int WORK0 = 5 * (NCX + NCY) + 16 * NI + 2 * NI;
+  static constexpr int WORK = WORK0 > VISC ? WORK0 : VISC;
   __host__ __device__ static constexpr long long smem(int nv) {
-    return (long long)nv * (HX * HY + NXI + NYI) + work(nv);
+    return (long long)nv * (HX * HY + NXI + NYI) + WORK;
   }
 };
 template <int TX, int TY>
 __host__ __device__ constexpr long long smem2d(int nv) { return Tile2D<TX, TY>::smem(nv); }
 
-template <int TX, int TY, int UPW>
+template <int TX, int TY, int UPW, int BT>
 __device__ __noinline__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, double* smem) {
   typedef Tile2D<TX, TY> T;
-  constexpr int HX = T::HX, HY = T::HY, NXI = T::NXI, NYI = T::NYI, NI = T::NI;
+  constexpr int HX = T::HX, HY = T::HY, NXI = T::NXI, NYI = T::NYI, NI = T::NI, NCX = T::NCX, NCY = T::NCY;
   const DevParams& P = M.P;
   const int nv = P.nvars, N0 = P.N0, N1 = P.N1;
   const int i0 = tx * TX, j0 = ty * TY;
@@ -226,74 +222,77 @@ __device__ __noinline__ void tile2d(const BMember& M, const BState& Sd, int s, i
   double* fx = sU + nv * vs;                   // [m][jj * (TX+1) + ii]
   double* fy = fx + nv * NXI;                  // [m][ii * (TY+1) + jj]
   double* wk = fy + nv * NYI;                  // work region
-  double* cf = wk;                             // cell fluxes [m][NC]
-  double* rec = cf + nv * T::NC;               // flow WENO values [k][m][NI]
-  double* spa = rec + 16 * NI;                 // passive speed [NI]
-  int* spm = (int*)(spa + NI);                 // passive scheme [NI]
+  double* cx = wk;                             // [5][NCX]: 4 flow fluxes + vn, x cells
+  double* cy = cx + 5 * NCX;                   // [5][NCY]
+  double* rec = cy + 5 * NCY;                  // [k][m][NI]
+  double* spa = rec + 16 * NI;                 // [NI]
+  int* spm = (int*)(spa + NI);                 // [NI]
   const int tid = threadIdx.x;
   for (int e = tid; e < vs; e += BT) load_point(M, S, i0 - H + e % HX, j0 - H + e / HX, sU + e, vs);
   __syncthreads();
-  constexpr int NF = 4;
-  const int np = nv - NF;
-#pragma unroll 1
-  for (int d = 0; d < 2; d++) {
-    // stencil cells of direction d: x: rows jj, columns a = 0..HX-1; y:
-    // columns ii, rows b = 0..HY-1; cell c's smem offset
-    const int ncell = d == 0 ? T::NCX : T::NCY;
-    const int ni = d == 0 ? NXI : NYI;
-    for (int e = tid; e < ncell; e += BT) {
-      const int c = d == 0 ? (e / HX + H) * HX + e % HX : (e % HY) * HX + e / HY + H;
-      cell_flux<NS2D>(P, sU, vs, c, d, cf + e, T::NC);
-    }
-    __syncthreads();
-    // interface f of direction d: line l, position k along the line; its
-    // cell i (right of the interface) in smem and in the cell-flux array
-    auto geo = [&](int f, int& base, int& ust, int& fbase, bool& ok) {
-      if (d == 0) {
-        const int ii = f % (TX + 1), jj = f / (TX + 1);
-        ok = i0 + ii <= N0 && j0 + jj < N1;
-        base = (jj + H) * HX + ii + H; ust = 1; fbase = jj * HX + ii + H;
-      } else {
-        const int jj = f % (TY + 1), ii = f / (TY + 1);
-        ok = j0 + jj <= N1 && i0 + ii < N0;
-        base = (jj + H) * HX + ii + H; ust = HX; fbase = ii * HY + jj + H;
-      }
-    };
-    for (int e = tid; e < NF * ni; e += BT) {
-      const int m = e / ni, f = e % ni;
-      int base, ust, fbase; bool ok;
-      geo(f, base, ust, fbase, ok);
-      if (!ok) continue;
-      iface_weno(P, sU + m * vs + base, ust, cf + m * T::NC + fbase, 1, rec[(0 * NF + m) * NI + f],
-                 rec[(1 * NF + m) * NI + f], rec[(2 * NF + m) * NI + f], rec[(3 * NF + m) * NI + f]);
-    }
-    __syncthreads();
-    double* fo = d == 0 ? fx : fy;
-    for (int f = tid; f < ni; f += BT) {
-      int base, ust, fbase; bool ok;
-      geo(f, base, ust, fbase, ok);
-      if (!ok) continue;
-      // rec[k][m][f] with stride NI between variables: gather into the layout
-      // iface_upwind_flow reads (k * rs + m), rs = 4
-      double r16[16];
+  // cell data: x cells (row jj, column a): c = (jj+H)*HX + a; y cells
+  // (column ii, row b): c = b*HX + ii + H
+  for (int e = tid; e < NCX + NCY; e += BT) {
+    const bool xd = e < NCX;
+    const int g = xd ? e : e - NCX;
+    const int c = xd ? (g / HX + H) * HX + g % HX : (g % HY) * HX + g / HY + H;
+    double f[4], vn;
+    ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, xd ? 0 : 1, f, vn);
+    double* o = xd ? cx + g : cy + g;
+    const int st = xd ? NCX : NCY;
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-#pragma unroll
-        for (int m = 0; m < NF; m++) r16[k * NF + m] = rec[(k * NF + m) * NI + f];
-      iface_upwind_flow<NS2D, UPW>(P, r16, NF, sU + base - ust, sU + base, vs, d, fo + f, ni, spa + f, spm + f);
-    }
-    __syncthreads();
-    for (int e = tid; e < np * ni; e += BT) {
-      const int m = NF + e / ni, f = e % ni;
-      int base, ust, fbase; bool ok;
-      geo(f, base, ust, fbase, ok);
-      if (!ok) continue;
-      double l, r, fl, fr;
-      iface_weno(P, sU + m * vs + base, ust, cf + m * T::NC + fbase, 1, l, r, fl, fr);
-      fo[m * ni + f] = upwind_species(spm[f], spa[f], l, r, fl, fr);
-    }
-    __syncthreads();
+    for (int m = 0; m < 4; m++) o[m * st] = f[m];
+    o[4 * st] = vn;
   }
+  __syncthreads();
+  // geometry of interface f: its cell i (right of the interface) in sU
+  // (base, stride ust along the line), in the cell data (cb, plane cst) and
+  // whether it is inside the member
+  auto geo = [&](int f, int& base, int& ust, const double*& cd, int& cst, int& dir) -> bool {
+    if (f < NXI) {
+      const int ii = f % (TX + 1), jj = f / (TX + 1);
+      base = (jj + H) * HX + ii + H; ust = 1; cd = cx + jj * HX + ii + H; cst = NCX; dir = 0;
+      return i0 + ii <= N0 && j0 + jj < N1;
+    }
+    const int g = f - NXI, jj = g % (TY + 1), ii = g / (TY + 1);
+    base = (jj + H) * HX + ii + H; ust = HX; cd = cy + ii * HY + jj + H; cst = NCY; dir = 1;
+    return j0 + jj <= N1 && i0 + ii < N0;
+  };
+  for (int e = tid; e < 4 * NI; e += BT) {
+    const int m = e / NI, f = e % NI;
+    int base, ust, cst, dir;
+    const double* cd;
+    if (!geo(f, base, ust, cd, cst, dir)) continue;
+    iface_weno(P, sU + m * vs + base, ust, cd + m * cst, 1, rec[(0 * 4 + m) * NI + f], rec[(1 * 4 + m) * NI + f],
+               rec[(2 * 4 + m) * NI + f], rec[(3 * 4 + m) * NI + f]);
+  }
+  __syncthreads();
+  for (int f = tid; f < NI; f += BT) {
+    int base, ust, cst, dir;
+    const double* cd;
+    if (!geo(f, base, ust, cd, cst, dir)) continue;
+    double* so = f < NXI ? fx + f : fy + (f - NXI);
+    iface_upwind_flow<NS2D, UPW>(P, rec + f, 4 * NI, NI, sU + base - ust, sU + base, vs, dir, so,
+                                 f < NXI ? NXI : NYI, spa + f, spm + f);
+  }
+  __syncthreads();
+  const int np = nv - 4;
+  for (int e = tid; e < np * NI; e += BT) {
+    const int m = 4 + e / NI, f = e % NI;
+    int base, ust, cst, dir;
+    const double* cd;
+    if (!geo(f, base, ust, cd, cst, dir)) continue;
+    const double* u = sU + m * vs + base;
+    const double* vn = cd + 4 * cst;
+    double a[6], b[6], l, r, fl, fr;
+#pragma unroll
+    for (int q = 0; q < 6; q++) { a[q] = u[(q - 3) * ust]; b[q] = __dmul_rn(vn[q - 3], a[q]); }
+    weno5_iface(P, a, b, l, r, fl, fr);
+    const double h = upwind_species(spm[f], spa[f], l, r, fl, fr);
+    if (f < NXI) fx[m * NXI + f] = h;
+    else fy[m * NYI + f - NXI] = h;
+  }
+  __syncthreads();
   // viscous fluxes (k_visc_source on this tile), in the work region
   const bool visc = P.viscous != 0;
   constexpr int QX = TX + 2, QY = TY + 2, FX = TX + 1, FY = TY + 1;
@@ -383,14 +382,17 @@ __device__ __noinline__ void tile2d(const BMember& M, const BState& Sd, int s, i
 }
 
 // ------------------------------------------------------------- 1D tile
-// shared memory (doubles): sU [nv][T1+6], cell fluxes [nv][T1+6], interface
-// fluxes [nv][T1+1], flow WENO values [4][3][T1+1], passive speed and scheme
+// A 1D tile has T1 points, one per thread.  Shared memory (doubles): sU
+// [nv][T1+6], cell fluxes [nv][T1+6], interface fluxes [nv][T1+1], flow WENO
+// values [4][3][T1+1], passive speed and scheme
+template <int T1>
 __host__ __device__ constexpr long long smem1d(int nv) {
   return (long long)nv * (2 * (T1 + 2 * H) + (T1 + 1)) + 14LL * (T1 + 1);
 }
 
-template <int UPW>
+template <int UPW, int BT>
 __device__ __noinline__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double* smem) {
+  constexpr int T1 = BT;
   const DevParams& P = M.P;
   constexpr int HX = T1 + 2 * H, LX = T1 + 1, NF = 3;
   const int nv = P.nvars, N0 = P.N0;
@@ -416,12 +418,8 @@ __device__ __noinline__ void tile1d(const BMember& M, const BState& Sd, int s, i
   __syncthreads();
   for (int f = tid; f < LX; f += BT) {
     if (i0 + f > N0) continue;
-    double r12[12];
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-#pragma unroll
-      for (int m = 0; m < NF; m++) r12[k * NF + m] = rec[(k * NF + m) * LX + f];
-    iface_upwind_flow<EULER1D, UPW>(P, r12, NF, sU + f + H - 1, sU + f + H, HX, 0, sF + f, LX, spa + f, spm + f);
+    iface_upwind_flow<EULER1D, UPW>(P, rec + f, NF * LX, LX, sU + f + H - 1, sU + f + H, HX, 0, sF + f, LX,
+                                    spa + f, spm + f);
   }
   __syncthreads();
   for (int e = tid; e < (nv - NF) * LX; e += BT) {
@@ -445,10 +443,11 @@ __device__ __noinline__ void tile1d(const BMember& M, const BState& Sd, int s, i
 }
 
 // --------------------------------------------------------------- kernels
-template <int TX, int TY, int MINB>
-__global__ void __launch_bounds__(BT, MINB) k_batch_stage(const BMember* __restrict__ mem, const BState* __restrict__ st,
-                                                    const int* __restrict__ tile_member,
-                                                    const int* __restrict__ ntiles, int s) {
+template <int TX, int TY, int BT, int MINB>
+__global__ void __launch_bounds__(BT, MINB) k_batch_stage(const BMember* __restrict__ mem,
+                                                          const BState* __restrict__ st,
+                                                          const int* __restrict__ tile_member,
+                                                          const int* __restrict__ ntiles, int s) {
   extern __shared__ double smem[];
   const int nt = *ntiles;
   for (int g = blockIdx.x; g < nt; g += gridDim.x) {
@@ -460,17 +459,17 @@ __global__ void __launch_bounds__(BT, MINB) k_batch_stage(const BMember* __restr
     if (M.P.ndims == 2) {
       const int tx = local % M.tnx, ty = local / M.tnx;
       switch (M.P.upwind) {
-        case UPW_ROE: tile2d<TX, TY, UPW_ROE>(M, Sd, s, tx, ty, smem); break;
-        case UPW_RF: tile2d<TX, TY, UPW_RF>(M, Sd, s, tx, ty, smem); break;
-        case UPW_LLF: tile2d<TX, TY, UPW_LLF>(M, Sd, s, tx, ty, smem); break;
-        default: tile2d<TX, TY, UPW_RUSANOV>(M, Sd, s, tx, ty, smem); break;
+        case UPW_ROE: tile2d<TX, TY, UPW_ROE, BT>(M, Sd, s, tx, ty, smem); break;
+        case UPW_RF: tile2d<TX, TY, UPW_RF, BT>(M, Sd, s, tx, ty, smem); break;
+        case UPW_LLF: tile2d<TX, TY, UPW_LLF, BT>(M, Sd, s, tx, ty, smem); break;
+        default: tile2d<TX, TY, UPW_RUSANOV, BT>(M, Sd, s, tx, ty, smem); break;
       }
     } else {
       switch (M.P.upwind) {
-        case UPW_ROE: tile1d<UPW_ROE>(M, Sd, s, local, smem); break;
-        case UPW_RF: tile1d<UPW_RF>(M, Sd, s, local, smem); break;
-        case UPW_LLF: tile1d<UPW_LLF>(M, Sd, s, local, smem); break;
-        default: tile1d<UPW_RUSANOV>(M, Sd, s, local, smem); break;
+        case UPW_ROE: tile1d<UPW_ROE, BT>(M, Sd, s, local, smem); break;
+        case UPW_RF: tile1d<UPW_RF, BT>(M, Sd, s, local, smem); break;
+        case UPW_LLF: tile1d<UPW_LLF, BT>(M, Sd, s, local, smem); break;
+        default: tile1d<UPW_RUSANOV, BT>(M, Sd, s, local, smem); break;
       }
     }
     __syncthreads();   // shared memory is reused by the next tile
@@ -513,33 +512,41 @@ int nfail(int code, const std::string& m) { return piafs::set_last_error(code, m
     if (e_ != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
   } while (0)
 
-// Launch configurations the tuner chooses from: tile shape and the minimum
-// CTAs per SM the compiler is asked to fit (2 trades registers for spills).
-struct TileShape { int tx, ty, minb; };
-constexpr int kNumShapes = 3;
-constexpr TileShape kShapes[kNumShapes] = {{16, 16, 1}, {32, 8, 1}, {64, 4, 1}};
+// Launch configurations the tuner chooses from: 2D tile shape, threads per
+// CTA (also the points of a 1D tile) and the CTAs per SM the compiler is
+// asked to fit; 256-thread tiles are small enough for two CTAs per SM.
+struct TileShape { int tx, ty, nt, minb; };
+constexpr int kNumShapes = 5;
+constexpr TileShape kShapes[kNumShapes] = {
+    {16, 16, 512, 1}, {32, 8, 512, 1}, {16, 8, 256, 2}, {32, 4, 256, 2}, {8, 16, 256, 2}};
 
-template <int TX, int TY, int MINB>
+template <int TX, int TY, int NT, int MINB>
 struct StageOps {
-  static long long smem(int nv) { return std::max(smem2d<TX, TY>(nv), smem1d(nv)) * (long long)sizeof(double); }
+  static long long smem(int nv) {
+    return std::max(smem2d<TX, TY>(nv), smem1d<NT>(nv)) * (long long)sizeof(double);
+  }
   static cudaError_t attr(long long bytes) {
-    return cudaFuncSetAttribute(k_batch_stage<TX, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return cudaFuncSetAttribute(k_batch_stage<TX, TY, NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bytes);
   }
   static int per_sm(long long bytes) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<TX, TY, MINB>, BT, bytes) != cudaSuccess) n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<TX, TY, NT, MINB>, NT, bytes) != cudaSuccess)
+      n = 0;
     return n;
   }
   static void launch(int grid, long long bytes, cudaStream_t st, const BMember* m, const BState* s, const int* tl,
                      const int* nt, int stage) {
-    k_batch_stage<TX, TY, MINB><<<grid, BT, bytes, st>>>(m, s, tl, nt, stage);
+    k_batch_stage<TX, TY, NT, MINB><<<grid, NT, bytes, st>>>(m, s, tl, nt, stage);
   }
 };
-#define PIAFS_SHAPE_SWITCH(idx, CALL)                      \
-  switch (idx) {                                           \
-    case 0: { typedef StageOps<16, 16, 1> Ops; CALL; } break; \
-    case 1: { typedef StageOps<32, 8, 1> Ops; CALL; } break;  \
-    default: { typedef StageOps<64, 4, 1> Ops; CALL; } break; \
+#define PIAFS_SHAPE_SWITCH(idx, CALL)                              \
+  switch (idx) {                                                   \
+    case 0: { typedef StageOps<16, 16, 512, 1> Ops; CALL; } break; \
+    case 1: { typedef StageOps<32, 8, 512, 1> Ops; CALL; } break;  \
+    case 2: { typedef StageOps<16, 8, 256, 2> Ops; CALL; } break;  \
+    case 3: { typedef StageOps<32, 4, 256, 2> Ops; CALL; } break;  \
+    default: { typedef StageOps<8, 16, 256, 2> Ops; CALL; } break; \
   }
 
 }  // namespace
@@ -586,7 +593,7 @@ int persistent_grid(piafs_gpu_batch* B) {
 void member_tiles(const piafs_gpu_batch* B, BMember& m) {
   const TileShape ts = kShapes[B->shape];
   if (m.P.ndims == 2) { m.tnx = (m.P.N0 + ts.tx - 1) / ts.tx; m.tny = (m.P.N1 + ts.ty - 1) / ts.ty; }
-  else { m.tnx = (m.P.N0 + T1 - 1) / T1; m.tny = 1; }
+  else { m.tnx = (m.P.N0 + ts.nt - 1) / ts.nt; m.tny = 1; }
 }
 
 // rebuild the tile list over the members still stepping and upload the
@@ -1071,7 +1078,7 @@ int piafs_gpu_batch_tune(piafs_gpu_batch* B, int force_tile_x) {
 int piafs_gpu_batch_set_launch(piafs_gpu_batch* B, int tile_x, int tile_y, int minb) {
   if (!B) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
   for (int i = 0; i < kNumShapes; i++)
-    if (kShapes[i].tx == tile_x && kShapes[i].ty == tile_y && kShapes[i].minb == minb) {
+    if (kShapes[i].tx == tile_x && kShapes[i].ty == tile_y && kShapes[i].minb == minb) {   // shapes are unique
       int optin = 0;
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B->device);
       if (smem_bytes(i, B->max_nv) > optin)

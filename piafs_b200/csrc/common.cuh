@@ -69,49 +69,6 @@ __device__ __forceinline__ void eu_flowvar(T rho_in, T ru, T e_in, T gamma, T& r
   P = (e - T(0.5) * rho * v * v) * (gamma - T(1));
 }
 
-// --------------------------------------------------------------- WENO weights
-// Nonlinear weights of the fifth-order WENO family for one stencil
-// (m3,m2,m1,p1,p2) and optimal weights (c1,c2,c3).  Jiang-Shu, mapped
-// (Henrick-Aslam-Powers), Borges (WENO-Z) and Yamaleev-Carpenter variants as
-// selected in weno.inp (interpolation.h:255-545).  The Jiang-Shu weights are
-// normalised with a single reciprocal: w_k = c_k prod_{m!=k} q_m / sum, with
-// q_m = (beta_m + eps)^2, which equals c_k/q_k / sum_m c_m/q_m.
-template <typename T>
-__device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T m2, T m1, T p1,
-                                             T p2, T eps, T& w1, T& w2, T& w3) {
-  const T t1312 = T(13.0 / 12.0), q4 = T(0.25);
-  T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
-  T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
-  T d3 = m1 - T(2) * p1 + p2, e3 = T(3) * m1 - T(4) * p1 + p2;
-  T b1 = t1312 * d1 * d1 + q4 * e1 * e1;
-  T b2 = t1312 * d2 * d2 + q4 * e2 * e2;
-  T b3 = t1312 * d3 * d3 + q4 * e3 * e3;
-  if (type == W_JS || type == W_MAPPED) {
-    T s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
-    T q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
-    T a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
-    T inv = T(1) / (a1 + a2 + a3);
-    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
-    if (type == W_MAPPED) {
-      T x1 = w1, x2 = w2, x3 = w3;
-      T n1 = x1 * (c1 + c1 * c1 - T(3) * c1 * x1 + x1 * x1), d1m = (c1 * c1 + x1 * (T(1) - T(2) * c1));
-      T n2 = x2 * (c2 + c2 * c2 - T(3) * c2 * x2 + x2 * x2), d2m = (c2 * c2 + x2 * (T(1) - T(2) * c2));
-      T n3 = x3 * (c3 + c3 * c3 - T(3) * c3 * x3 + x3 * x3), d3m = (c3 * c3 + x3 * (T(1) - T(2) * c3));
-      T A1 = n1 / d1m, A2 = n2 / d2m, A3 = n3 / d3m;
-      T inv2 = T(1) / (A1 + A2 + A3);
-      w1 = A1 * inv2; w2 = A2 * inv2; w3 = A3 * inv2;
-    }
-    return;
-  }
-  T tau;
-  if (type == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
-  else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = t * t; }
-  T r1 = tau / (b1 + eps), r2 = tau / (b2 + eps), r3 = tau / (b3 + eps);
-  T a1 = c1 * (T(1) + r1 * r1), a2 = c2 * (T(1) + r2 * r2), a3 = c3 * (T(1) + r3 * r3);
-  T inv = T(1) / (a1 + a2 + a3);
-  w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
-}
-
 // Reciprocal 1/x of a finite, nonzero, normal x whose reciprocal is normal.
 // Newton-Raphson iteration for f(y) = 1/y - x, y <- y + y (1 - x y), each
 // step squaring the relative error (P. Markstein, "Computation of elementary
@@ -136,6 +93,51 @@ __device__ __forceinline__ float rcp_nr(float x) {
   return y;
 }
 #endif
+
+// --------------------------------------------------------------- WENO weights
+// Nonlinear weights of the fifth-order WENO family for one stencil
+// (m3,m2,m1,p1,p2) and optimal weights (c1,c2,c3).  Jiang-Shu, mapped
+// (Henrick-Aslam-Powers), Borges (WENO-Z) and Yamaleev-Carpenter variants as
+// selected in weno.inp (interpolation.h:255-545).  The Jiang-Shu weights are
+// normalised with a single reciprocal: w_k = c_k prod_{m!=k} q_m / sum, with
+// q_m = (beta_m + eps)^2, which equals c_k/q_k / sum_m c_m/q_m.  Quotients use
+// rcp_nr (Newton-Raphson reciprocal), so weights agree with the reference's
+// divisions to rounding.
+template <typename T>
+__device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T m2, T m1, T p1,
+                                             T p2, T eps, T& w1, T& w2, T& w3) {
+  const T t1312 = T(13.0 / 12.0), q4 = T(0.25);
+  T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
+  T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
+  T d3 = m1 - T(2) * p1 + p2, e3 = T(3) * m1 - T(4) * p1 + p2;
+  T b1 = t1312 * d1 * d1 + q4 * e1 * e1;
+  T b2 = t1312 * d2 * d2 + q4 * e2 * e2;
+  T b3 = t1312 * d3 * d3 + q4 * e3 * e3;
+  if (type == W_JS || type == W_MAPPED) {
+    T s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
+    T q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
+    T a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
+    T inv = rcp_nr(a1 + a2 + a3);
+    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+    if (type == W_MAPPED) {
+      T x1 = w1, x2 = w2, x3 = w3;
+      T n1 = x1 * (c1 + c1 * c1 - T(3) * c1 * x1 + x1 * x1), d1m = (c1 * c1 + x1 * (T(1) - T(2) * c1));
+      T n2 = x2 * (c2 + c2 * c2 - T(3) * c2 * x2 + x2 * x2), d2m = (c2 * c2 + x2 * (T(1) - T(2) * c2));
+      T n3 = x3 * (c3 + c3 * c3 - T(3) * c3 * x3 + x3 * x3), d3m = (c3 * c3 + x3 * (T(1) - T(2) * c3));
+      T A1 = n1 * rcp_nr(d1m), A2 = n2 * rcp_nr(d2m), A3 = n3 * rcp_nr(d3m);
+      T inv2 = rcp_nr(A1 + A2 + A3);
+      w1 = A1 * inv2; w2 = A2 * inv2; w3 = A3 * inv2;
+    }
+    return;
+  }
+  T tau;
+  if (type == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
+  else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = t * t; }
+  T r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
+  T a1 = c1 * (T(1) + r1 * r1), a2 = c2 * (T(1) + r2 * r2), a3 = c3 * (T(1) + r3 * r3);
+  T inv = rcp_nr(a1 + a2 + a3);
+  w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+}
 
 // 3-point candidate values of explicit WENO5 (Interp1PrimFifthOrderWENO.c:144-146)
 template <typename T>

@@ -129,7 +129,7 @@ def test_continuous_batching_join_leave(tmp_path):
         assert b.info["members"] == len(later)
 
 
-@pytest.mark.parametrize("tile_x", [16, 64])
+@pytest.mark.parametrize("tile_x", [16, 32, 8])
 def test_tile_shapes(tmp_path, tile_x):
     mix = make_mix(str(tmp_path))[:4]
     with Batch() as b:
