@@ -227,6 +227,51 @@ int piafs_gpu_batch_tune(piafs_gpu_batch* batch, int force_tile_x);
  * min_ctas_per_sm 1 or 2). */
 int piafs_gpu_batch_set_launch(piafs_gpu_batch* batch, int tile_x, int tile_y, int min_ctas_per_sm);
 
+/* ---- request serving ----
+ * No counterpart in the reference.  A request is a solve described by its
+ * parameters instead of an input deck on disk: the library writes the deck
+ * in memory (the decks of the package's case generators, cases.py) and
+ * generates the initial fields on the device, so a stream of requests needs
+ * no file traffic.  Kinds: the 1D Euler density wave (rho = 1 + amp
+ * sin(2 pi x), u = 1, p = 1, gamma 1.4, periodic, WENO5, Roe, SSPRK3) and the
+ * 2D photochemical beam (quiescent O2/O3 gas, density noise of amplitude
+ * `noise` from `seed`, Gaussian beam map of amplitude `amp` and 1/e radius
+ * `beam_radius`, Re through the beam half-angle, periodic x, slip walls y,
+ * WENO5, LLF, SSPRK3). */
+enum { PIAFS_REQUEST_EULER1D_WAVE = 1, PIAFS_REQUEST_NS2D_BEAM = 2 };
+typedef struct {
+  int kind;                 /* PIAFS_REQUEST_*                                */
+  int n;                    /* grid points (1D) or grid side (2D, square)     */
+  int nsteps;               /* time steps                                     */
+  double dt;                /* time step                                      */
+  double amp;               /* density-wave (1D) or beam (2D) amplitude       */
+  double beam_radius;       /* 2D                                             */
+  double Re;                /* 2D                                             */
+  double noise;             /* 2D                                             */
+  unsigned long long seed;  /* 2D                                             */
+} piafs_gpu_request;
+int piafs_gpu_batch_add_request(piafs_gpu_batch* batch, const piafs_gpu_request* req, int* id);
+/* Sum of a member's solution over interior points and variables, reduced on
+ * the device in a fixed order (the same bits every time for the same state). */
+int piafs_gpu_batch_checksum(piafs_gpu_batch* batch, int id, double* sum);
+typedef struct {
+  double arrival_s;         /* from the trace                                 */
+  double admitted_s;        /* admission time, seconds from the trace start   */
+  double finished_s;        /* result ready (retired), seconds from the start */
+  int steps;
+  double checksum;          /* piafs_gpu_batch_checksum of the final state    */
+} piafs_gpu_serve_result;
+/* Replay a request trace in real time with continuous batching: request k
+ * arrives at arrival_s[k] (seconds from the start, nondecreasing); arrived
+ * requests are admitted in arrival order while the HBM budget holds them
+ * (a request that does not fit waits, and so do the ones behind it); between
+ * admission rounds all resident requests advance steps_per_round steps
+ * together; a finished request's checksum is taken and its memory released
+ * at once.  Returns when every request has finished; latency of request k
+ * is out[k].finished_s - out[k].arrival_s. */
+int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s, int n, int precision,
+                          unsigned long long hbm_budget_bytes, int steps_per_round, piafs_gpu_serve_result* out);
+
 /* ---- diagnostics ----
  * No counterpart in the reference.  y[i] = 1/x[i] (device arrays) computed
  * by the Newton-Raphson reciprocal that the reconstruction and line-solve

@@ -80,6 +80,9 @@ SIGNATURES = {
     "piafs_gpu_batch_get_info": (C.c_int, [_vp, _vp]),
     "piafs_gpu_batch_tune": (C.c_int, [_vp, C.c_int]),
     "piafs_gpu_batch_set_launch": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    "piafs_gpu_batch_add_request": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+    "piafs_gpu_batch_checksum": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
+    "piafs_gpu_serve_trace": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_ulonglong, C.c_int, _vp]),
 }
 
 
@@ -304,6 +307,38 @@ def hyperbolic_noalloc(params: "HypParams", hyp, u, dxinv, stream: int = 0):
         raise PiafsError(code, L.piafs_gpu_last_error().decode())
 
 
+REQUEST_EULER1D_WAVE, REQUEST_NS2D_BEAM = 1, 2
+
+
+class Request(C.Structure):
+    """A parameter-described solve (piafs_gpu_request)."""
+    _fields_ = [
+        ("kind", C.c_int), ("n", C.c_int), ("nsteps", C.c_int), ("dt", C.c_double), ("amp", C.c_double),
+        ("beam_radius", C.c_double), ("Re", C.c_double), ("noise", C.c_double), ("seed", C.c_ulonglong),
+    ]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("arrival_s", C.c_double), ("admitted_s", C.c_double), ("finished_s", C.c_double),
+                ("steps", C.c_int), ("checksum", C.c_double)]
+
+
+def serve_trace(requests, arrivals, precision: str = "fp64", hbm_budget_bytes: int = 0, steps_per_round: int = 4):
+    """Replay a request trace in real time through the continuous-batching
+    serving loop (piafs_gpu_serve_trace); returns a list of dicts per request
+    (arrival, admission, finish in seconds from the start, steps, checksum)."""
+    L = load_library()
+    n = len(requests)
+    reqs = (Request * n)(*requests)
+    arr = (C.c_double * n)(*[float(x) for x in arrivals])
+    out = (ServeResult * n)()
+    code = L.piafs_gpu_serve_trace(reqs, arr, n, PRECISION[precision], int(hbm_budget_bytes), int(steps_per_round),
+                                   out)
+    if code != PIAFS_OK:
+        raise PiafsError(code, L.piafs_gpu_last_error().decode())
+    return [{name: getattr(r, name) for name, _ in ServeResult._fields_} for r in out]
+
+
 class BatchInfo(C.Structure):
     _fields_ = [
         ("members", C.c_int), ("active", C.c_int), ("tiles", C.c_int), ("tile_x", C.c_int),
@@ -366,6 +401,18 @@ class Batch:
             self._shapes[ids[k]] = (int(np.prod([int(x) for x in d["size"]])), int(d["nvars"][0]))
         _check(code)
         return list(ids)
+
+    def add_request(self, req: "Request") -> int:
+        i = C.c_int()
+        _check(_lib.piafs_gpu_batch_add_request(self._h, C.byref(req), C.byref(i)))
+        npts = req.n if req.kind == REQUEST_EULER1D_WAVE else req.n * req.n
+        self._shapes[i.value] = (npts, 3 if req.kind == REQUEST_EULER1D_WAVE else 11)
+        return i.value
+
+    def checksum(self, member: int) -> float:
+        s = C.c_double()
+        _check(_lib.piafs_gpu_batch_checksum(self._h, int(member), C.byref(s)))
+        return s.value
 
     def step(self, nsteps: int = 1):
         _check(_lib.piafs_gpu_batch_step(self._h, int(nsteps)))

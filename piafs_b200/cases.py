@@ -262,3 +262,34 @@ def ensemble(root: str, n: int = 256, steps: int = 100, seed: int = 1, side_rang
         out.append({"dir": d, "side": side, "beam_amp": amp, "beam_radius": radius, "Re": Re, "steps": steps,
                     "dt": mdt})
     return out
+
+
+def serving_trace(n: int = 10000, rate: float = 2000.0, frac_1d: float = 0.7, seed_arrivals: int = 2,
+                  seed_params: int = 3, n1d=(256, 8192), side2d=(64, 1024), steps=(50, 500)):
+    """The request-serving workload: ``n`` requests arriving as a Poisson
+    process of ``rate`` requests/s (seed 2).  A fraction ``frac_1d`` are 1D
+    Euler density waves (N log-uniform in ``n1d``, amplitude U(0.05, 0.3),
+    dt = 0.1/N as in the 1024-point case), the rest 2D photochemical beams
+    (side log-uniform in ``side2d``, beam parameters and dt as in
+    ``ensemble``, density noise 1e-6); each runs a uniform number of SSPRK3
+    steps in ``steps`` (parameters: seed 3).  Returns (requests, arrivals):
+    dicts with the fields of piafs_gpu_request, and arrival times in seconds."""
+    ra = np.random.default_rng(seed_arrivals)
+    arrivals = np.cumsum(ra.exponential(1.0 / rate, size=n))
+    rp = np.random.default_rng(seed_params)
+    reqs = []
+    for k in range(n):
+        nsteps = int(rp.integers(steps[0], steps[1] + 1))
+        if rp.uniform() < frac_1d:
+            N = int(round(math.exp(rp.uniform(math.log(n1d[0]), math.log(n1d[1])))))
+            reqs.append({"kind": 1, "n": N, "nsteps": nsteps, "dt": 0.1 / N, "amp": float(rp.uniform(0.05, 0.3)),
+                         "beam_radius": 0.0, "Re": 0.0, "noise": 0.0, "seed": 0})
+        else:
+            side = int(round(math.exp(rp.uniform(math.log(side2d[0]), math.log(side2d[1])))))
+            amp = float(rp.uniform(0.5, 1.5))
+            radius = float(rp.uniform(0.02, 0.1))
+            Re = float(math.exp(rp.uniform(math.log(1e3), math.log(1e5))))
+            dt = min(0.4 / side, (0.4 / 2048) * 1e4 / Re, 0.1 * Re / (side * side))
+            reqs.append({"kind": 2, "n": side, "nsteps": nsteps, "dt": dt, "amp": amp, "beam_radius": radius,
+                         "Re": Re, "noise": 1e-6, "seed": 1000003 * seed_params + k})
+    return reqs, arrivals

@@ -32,6 +32,9 @@
 #include <algorithm>
 #include <cstring>
 #include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
 #include <mutex>
 #include <thread>
 #include <string>
@@ -494,6 +497,82 @@ __global__ void k_batch_epilogue(const BMember* __restrict__ mem, BState* __rest
   status[2 * m + 1] = S.active;
 }
 
+// ------------------------------------------------------- request fields
+// SplitMix64 (Steele, Lea and Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014): a counter-based stream, value k of seed s.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Initial fields of a request (interior points; ghosts stay zero), the
+// fields of the package's case generators: 1D density wave and 2D
+// photochemical beam (see piafs_gpu_request).
+__global__ void k_request_init(DevParams P, int kind, double amp, double radius, double noise,
+                               unsigned long long seed, double* __restrict__ u, double* __restrict__ imap) {
+  const long long n = (long long)P.N0 * P.N1;
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int i = (int)(k % P.N0), j = (int)(k / P.N0);
+  const long long p = pidx(P, i, j), ps = P.ps;
+  const double g = P.gamma;
+  if (kind == PIAFS_REQUEST_EULER1D_WAVE) {
+    const double x = (double)i / P.N0;
+    const double rho = 1.0 + amp * sin(2.0 * 3.141592653589793 * x);
+    u[p] = rho;
+    u[ps + p] = rho;
+    u[2 * ps + p] = 1.0 / (g - 1.0) + 0.5 * rho;
+    return;
+  }
+  const double x = (i + 0.5) / P.N0, y = (j + 0.5) / P.N1;
+  const double r01 = (double)(splitmix64(seed * 0x100000001B3ull + (unsigned long long)k) >> 11) * 0x1.0p-53;
+  const double rho = 1.0 + noise * (2.0 * r01 - 1.0);
+  const double pr = 1.0 / g;
+  u[p] = rho;
+  u[ps + p] = 0.0;
+  u[2 * ps + p] = 0.0;
+  u[3 * ps + p] = pr / (g - 1.0);
+  for (int v = 4; v < P.nvars; v++) u[v * ps + p] = 0.0;
+  for (int iz = 0; (P.chem ? iz < P.nz : false) && 4 + P.zstride * iz + 1 < P.nvars; iz++) {
+    u[(4 + P.zstride * iz) * ps + p] = 1.0;          // O2 (normalised)
+    u[(5 + P.zstride * iz) * ps + p] = 0.005;        // O3 = f_O3 / f_O2
+  }
+  if (imap) {
+    const double dx = x - 0.5, dy = y - 0.5;
+    imap[p] = amp * exp(-(dx * dx + dy * dy) / (radius * radius));
+  }
+}
+
+// Deterministic sum of a member's interior solution: per-block partial sums
+// in a fixed tree order, then one block over the partials in index order.
+constexpr int CS_THREADS = 256, CS_BLOCKS = 256;
+__global__ void k_checksum_partial(DevParams P, const double* __restrict__ u, double* __restrict__ part) {
+  __shared__ double sh[CS_THREADS];
+  const long long n = (long long)P.N0 * P.N1 * P.nvars;
+  double acc = 0.0;
+  for (long long e = blockIdx.x * (long long)CS_THREADS + threadIdx.x; e < n; e += (long long)CS_BLOCKS * CS_THREADS) {
+    const long long pt = e / P.nvars;
+    const int v = (int)(e - pt * P.nvars);
+    acc += u[v * P.ps + pidx(P, (int)(pt % P.N0), (int)(pt / P.N0))];
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = CS_THREADS / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+__global__ void k_checksum_final(const double* __restrict__ part, double* __restrict__ out) {
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int b = 0; b < CS_BLOCKS; b++) s += part[b];
+    *out = s;
+  }
+}
+
 // ------------------------------------------------------------- host side
 struct HostMember {
   bool used = false;
@@ -713,7 +792,8 @@ int parse_member(const char* deck_dir, HostMember& hm, DevParams& P, std::string
 }  // namespace
 
 namespace {
-int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, int* id) {
+int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, int* id,
+                 const piafs_gpu_request* req = nullptr) {
   const Deck& d = hm.deck;
   {
     int optin = 0;
@@ -724,7 +804,7 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   P.mixed = 0;
   const int ns = d.nstages;
   const size_t planes = (size_t)P.nvars * P.ps;
-  const size_t ndx = d.dxinv.size(), nim = d.imap.size();
+  const size_t ndx = d.dxinv.size(), nim = req ? (P.chem ? (size_t)P.npg : 0) : d.imap.size();
   const size_t bytes = ((3 + ns) * planes + ndx + nim) * sizeof(double);
   if (B->budget && B->used + bytes > B->budget)
     return nfail(PIAFS_ERR_MEMORY, "the batch's device memory budget cannot hold this member now");
@@ -758,16 +838,30 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   }
   bm.nsteps = nsteps > 0 ? nsteps : d.n_iter;
   // upload: initial state (AoS with ghosts) into u, X and Y (the ghost
-  // entries of the stage buffers must hold what the state's ghosts hold)
+  // entries of the stage buffers must hold what the state's ghosts hold);
+  // a request's fields are generated on the device instead
   double* stage = nullptr;
-  e = cudaMallocAsync((void**)&stage, d.u0.size() * sizeof(double), B->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(stage, d.u0.data(), d.u0.size() * sizeof(double), cudaMemcpyHostToDevice, B->stream);
-  if (e == cudaSuccess) { launch_aos_to_soa(stage, u, P.npg, P.nvars, P.ps, B->stream); e = cudaGetLastError(); }
+  if (req) {
+    e = cudaMemsetAsync(u, 0, planes * sizeof(double), B->stream);
+    if (e == cudaSuccess && nim) e = cudaMemsetAsync(im, 0, nim * sizeof(double), B->stream);
+    if (e == cudaSuccess) {
+      const long long npt = (long long)P.N0 * P.N1;
+      k_request_init<<<(unsigned)((npt + 255) / 256), 256, 0, B->stream>>>(
+          P, req->kind, req->amp, req->beam_radius, req->noise, req->seed, u, nim ? im : nullptr);
+      e = cudaGetLastError();
+    }
+  } else {
+    e = cudaMallocAsync((void**)&stage, d.u0.size() * sizeof(double), B->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(stage, d.u0.data(), d.u0.size() * sizeof(double), cudaMemcpyHostToDevice, B->stream);
+    if (e == cudaSuccess) { launch_aos_to_soa(stage, u, P.npg, P.nvars, P.ps, B->stream); e = cudaGetLastError(); }
+  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(bm.X, u, planes * sizeof(double), cudaMemcpyDeviceToDevice, B->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(bm.Y, u, planes * sizeof(double), cudaMemcpyDeviceToDevice, B->stream);
   for (int k = 0; k < ns && e == cudaSuccess; k++) e = cudaMemsetAsync(bm.k[k], 0, planes * sizeof(double), B->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(dx, d.dxinv.data(), ndx * sizeof(double), cudaMemcpyHostToDevice, B->stream);
-  if (e == cudaSuccess && nim) e = cudaMemcpyAsync(im, d.imap.data(), nim * sizeof(double), cudaMemcpyHostToDevice, B->stream);
+  if (e == cudaSuccess && nim && !req)
+    e = cudaMemcpyAsync(im, d.imap.data(), nim * sizeof(double), cudaMemcpyHostToDevice, B->stream);
   BState st{};
   st.u = u; st.X = bm.X; st.t = d.restart_iter * d.dt; st.iter = 0; st.active = bm.nsteps > 0 ? 1 : 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(B->dstate + slot, &st, sizeof(BState), cudaMemcpyHostToDevice, B->stream);
@@ -797,6 +891,62 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   *id = slot;
   return PIAFS_OK;
 }
+}  // namespace
+
+namespace {
+
+std::string fmt17(double v) {
+  char b[64];
+  std::snprintf(b, sizeof(b), "%.17g", v);
+  return b;
+}
+
+// The in-memory deck of a request: the key files the package's case
+// generators write for the same parameters (cases.euler1d_density_wave,
+// cases.ns2d_photochem_beam) and the interior grid.
+int request_deck(const piafs_gpu_request& q, DeckMemory& m, std::string& err) {
+  if (q.n < 8 || q.nsteps < 1 || !(q.dt > 0.0)) { err = "request: bad size, step count or dt"; return PIAFS_ERR_ARGUMENT; }
+  const std::string n = std::to_string(q.n), ns = std::to_string(q.nsteps);
+  if (q.kind == PIAFS_REQUEST_EULER1D_WAVE) {
+    m.files["solver.inp"] =
+        "begin\n ndims 1\n nvars 3\n size " + n + "\n ghost 3\n n_iter " + ns +
+        "\n time_scheme rk\n time_scheme_type ssprk3\n hyp_space_scheme weno5\n hyp_interp_type components\n"
+        " dt " + fmt17(q.dt) + "\n screen_op_iter " + ns + "\n file_op_iter " + ns +
+        "\n op_file_format none\n ip_file_type binary\n op_overwrite no\n model euler1d\nend\n";
+    m.files["boundary.inp"] = "2\nperiodic 0 1 0 0\nperiodic 0 -1 0 0\n";
+    m.files["physics.inp"] = "begin\n gamma 1.4\n upwinding roe\nend\n";
+    m.grid.resize(q.n);
+    for (int i = 0; i < q.n; i++) m.grid[i] = (double)i / q.n;
+    return 0;
+  }
+  if (q.kind == PIAFS_REQUEST_NS2D_BEAM) {
+    if (!(q.Re > 0.0) || !(q.beam_radius > 0.0)) { err = "request: Re and beam_radius must be positive"; return PIAFS_ERR_ARGUMENT; }
+    // Re ~ 1/sin(theta): theta = 4.2117e-5 rad gives Re = 1e4
+    const double s = std::sin(4.2117e-5) * 1e4 / q.Re;
+    const double theta = std::asin(s < 1.0 ? s : 1.0);
+    m.files["solver.inp"] =
+        "begin\n ndims 2\n nvars 11\n size " + n + " " + n + "\n ghost 3\n n_iter " + ns +
+        "\n time_scheme rk\n time_scheme_type ssprk3\n hyp_space_scheme weno5\n hyp_interp_type components\n"
+        " par_space_scheme 2\n dt " + fmt17(q.dt) + "\n screen_op_iter " + ns + "\n file_op_iter " + ns +
+        "\n op_file_format none\n ip_file_type binary\n op_overwrite no\n model navierstokes2d\nend\n";
+    m.files["boundary.inp"] =
+        "4\nperiodic 0 1 0 0 -1e+99 1e+99\nperiodic 0 -1 0 0 -1e+99 1e+99\n"
+        "slip-wall 1 1 -1e+99 1e+99 0 0\n 0 0\nslip-wall 1 -1 -1e+99 1e+99 0 0\n 0 0\n";
+    m.files["physics.inp"] = "begin\n gamma 1.4\n upwinding llf-char\n Pr 0.72\n Re " + fmt17(q.Re) +
+                             "\n include_chemistry yes\n write_output no\nend\n";
+    m.files["chemistry.inp"] = "begin\n theta " + fmt17(theta) + "\nend\n";
+    m.grid.resize(2 * (size_t)q.n);
+    for (int i = 0; i < q.n; i++) m.grid[i] = m.grid[q.n + i] = (i + 0.5) / q.n;
+    return 0;
+  }
+  err = "request: unknown kind";
+  return PIAFS_ERR_ARGUMENT;
+}
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 }  // namespace
 
 extern "C" {
@@ -1088,6 +1238,107 @@ int piafs_gpu_batch_set_launch(piafs_gpu_batch* B, int tile_x, int tile_y, int m
       return PIAFS_OK;
     }
   return nfail(PIAFS_ERR_ARGUMENT, "no such launch configuration");
+}
+
+int piafs_gpu_batch_add_request(piafs_gpu_batch* B, const piafs_gpu_request* req, int* id) {
+  if (!B || !req || !id) return nfail(PIAFS_ERR_ARGUMENT, "null argument");
+  DeckMemory mem;
+  std::string err;
+  if (int r = request_deck(*req, mem, err)) return nfail(r, err);
+  HostMember hm;
+  DevParams P;
+  int r = read_deck_memory(mem, hm.deck, err);
+  if (!r) r = make_params(hm.deck, P, err);
+  if (r) return nfail(r, err);
+  return admit_member(B, std::move(hm), P, req->nsteps, id, req);
+}
+
+int piafs_gpu_batch_checksum(piafs_gpu_batch* B, int id, double* sum) {
+  if (!B || !sum || id < 0 || id >= (int)B->members.size() || !B->members[id].used)
+    return nfail(PIAFS_ERR_ARGUMENT, "no such member");
+  const DevParams& P = B->members[id].bm.P;
+  BState st;
+  BCK(cudaMemcpyAsync(&st, B->dstate + id, sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
+  double* part = nullptr;
+  BCK(cudaMallocAsync((void**)&part, (CS_BLOCKS + 1) * sizeof(double), B->stream));
+  BCK(cudaStreamSynchronize(B->stream));
+  k_checksum_partial<<<CS_BLOCKS, CS_THREADS, 0, B->stream>>>(P, st.u, part);
+  k_checksum_final<<<1, 32, 0, B->stream>>>(part, part + CS_BLOCKS);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sum, part + CS_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, B->stream);
+  cudaFreeAsync(part, B->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string("checksum: ") + cudaGetErrorString(e));
+  return PIAFS_OK;
+}
+
+int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s, int n, int precision,
+                          unsigned long long budget, int steps_per_round, piafs_gpu_serve_result* out) {
+  if (n < 0 || (n > 0 && (!reqs || !arrival_s || !out)) || steps_per_round < 1)
+    return nfail(PIAFS_ERR_ARGUMENT, "bad argument");
+  for (int k = 1; k < n; k++)
+    if (arrival_s[k] < arrival_s[k - 1]) return nfail(PIAFS_ERR_ARGUMENT, "arrival times must be nondecreasing");
+  piafs_gpu_batch* B = nullptr;
+  if (int r = piafs_gpu_batch_create(precision, budget, &B)) return r;
+  std::vector<int> slot_req;     // member id -> request index
+  int next = 0, finished = 0, rc = PIAFS_OK;
+  const double t0 = now_s();
+  for (int k = 0; k < n; k++) {
+    out[k].arrival_s = arrival_s[k];
+    out[k].admitted_s = out[k].finished_s = -1.0;
+    out[k].steps = 0;
+    out[k].checksum = 0.0;
+  }
+  std::vector<int> done(4096);
+  while (finished < n && rc == PIAFS_OK) {
+    // admission: arrived requests in order, while the budget holds them
+    double t = now_s() - t0;
+    while (next < n && arrival_s[next] <= t) {
+      int id = -1;
+      const int r = piafs_gpu_batch_add_request(B, reqs + next, &id);
+      if (r == PIAFS_ERR_MEMORY) {
+        piafs_gpu_batch_info bi;
+        if ((rc = piafs_gpu_batch_get_info(B, &bi))) break;
+        if (bi.members == 0)   // alone it does not fit: it never will
+          rc = nfail(PIAFS_ERR_MEMORY, "a request needs more device memory than the whole HBM budget");
+        break;
+      }
+      if (r) { rc = r; break; }
+      if ((int)slot_req.size() <= id) slot_req.resize(id + 1, -1);
+      slot_req[id] = next;
+      out[next].admitted_s = now_s() - t0;
+      next++;
+      t = now_s() - t0;
+    }
+    if (rc) break;
+    piafs_gpu_batch_info info;
+    if ((rc = piafs_gpu_batch_get_info(B, &info))) break;
+    if (info.active > 0) {
+      if ((rc = piafs_gpu_batch_step(B, steps_per_round))) break;
+    } else if (info.members == 0) {
+      if (next >= n) break;
+      // nothing resident: wait for the next arrival
+      std::this_thread::sleep_for(std::chrono::duration<double>(std::min(std::max(arrival_s[next] - t, 0.0), 1e-3)));
+      continue;
+    }
+    // retire finished requests
+    int nd = 0;
+    if ((rc = piafs_gpu_batch_poll(B, done.data(), (int)done.size(), &nd))) break;
+    for (int q = 0; q < nd && rc == PIAFS_OK; q++) {
+      const int id = done[q], k = slot_req[id];
+      double cs = 0.0, tm = 0.0;
+      int it = 0, dn = 0;
+      rc = piafs_gpu_batch_checksum(B, id, &cs);
+      if (!rc) rc = piafs_gpu_batch_member(B, id, &tm, &it, &dn);
+      if (!rc) rc = piafs_gpu_batch_remove(B, id);
+      out[k].checksum = cs;
+      out[k].steps = it;
+      out[k].finished_s = now_s() - t0;
+      finished++;
+    }
+  }
+  piafs_gpu_batch_destroy(B);
+  return rc;
 }
 
 }  // extern "C"

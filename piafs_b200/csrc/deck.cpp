@@ -14,7 +14,24 @@ namespace piafs {
 
 namespace {
 
+// In-memory deck of read_deck_memory (this thread, for the duration of the
+// call): key files by name, the interior grid, no field files.
+thread_local const DeckMemory* tl_mem = nullptr;
+
+std::string base_name(const std::string& path) {
+  const size_t k = path.find_last_of('/');
+  return k == std::string::npos ? path : path.substr(k + 1);
+}
+
 bool read_tokens(const std::string& path, std::vector<std::string>& toks) {
+  if (tl_mem) {
+    auto it = tl_mem->files.find(base_name(path));
+    if (it == tl_mem->files.end()) return false;
+    std::istringstream f(it->second);
+    std::string t;
+    while (f >> t) toks.push_back(t);
+    return true;
+  }
   std::ifstream f(path);
   if (!f) return false;
   std::string t;
@@ -348,8 +365,15 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
   const int g = d.ghosts;
   const bool ascii = d.ip_file_type == "ascii";
   std::vector<double> xs, field;
-  if (int r = read_field(dir + "/initial.inp", d, d.nvars, ascii, xs, field, found, err)) return r;
-  if (!found) { err = "initial solution file not found"; return PIAFS_ERR_INPUT; }
+  if (tl_mem) {
+    long long nx = 0;
+    for (int s : d.size) nx += s;
+    if ((long long)tl_mem->grid.size() != nx) { err = "in-memory deck: grid size mismatch"; return PIAFS_ERR_INPUT; }
+    xs = tl_mem->grid;
+  } else {
+    if (int r = read_field(dir + "/initial.inp", d, d.nvars, ascii, xs, field, found, err)) return r;
+    if (!found) { err = "initial solution file not found"; return PIAFS_ERR_INPUT; }
+  }
   d.grid = xs;
   d.x.clear();
   d.dxinv.clear();
@@ -363,6 +387,12 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
   }
   const int N0 = d.size[0], N1 = d.ndims == 2 ? d.size[1] : 1;
   const int W0 = N0 + 2 * g, W1 = d.ndims == 2 ? N1 + 2 * g : 1, g1 = d.ndims == 2 ? g : 0;
+  if (tl_mem) {
+    // fields are generated by the caller
+    d.u0.clear();
+    d.imap.clear();
+    goto boundaries;
+  }
   d.u0.assign((size_t)W0 * W1 * d.nvars, 0.0);
   for (int j = 0; j < N1; j++)
     for (int i = 0; i < N0; i++)
@@ -384,6 +414,7 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
         d.imap[(size_t)(i + g) + (size_t)W0 * (j + g1)] = val;
       }
   }
+boundaries:
   // boundary.inp (InitializeBoundaries.c:82-150, CalculateLocalExtent :296-378)
   std::vector<std::string> t;
   if (!read_tokens(dir + "/boundary.inp", t) || t.empty()) {
@@ -429,6 +460,13 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
     d.zones.push_back(z);
   }
   return 0;
+}
+
+int read_deck_memory(const DeckMemory& m, Deck& d, std::string& err) {
+  tl_mem = &m;
+  const int r = read_deck("<memory>", d, err);
+  tl_mem = nullptr;
+  return r;
 }
 
 int make_params(const Deck& d, DevParams& P, std::string& err) {

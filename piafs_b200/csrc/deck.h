@@ -6,6 +6,7 @@
 // model/chemistry initialisers) and produces the flat parameters, grid,
 // initial state and boundary zones the device path consumes.
 #pragma once
+#include <map>
 #include <string>
 #include <vector>
 #include "common.cuh"
@@ -50,6 +51,15 @@ struct Deck {
 // Parse the deck in `dir`.  Returns 0 on success, otherwise a PIAFS_ERR_*
 // code with a message in `err`.
 int read_deck(const std::string& dir, Deck& d, std::string& err);
+// A deck held in memory: the key files (solver.inp, boundary.inp,
+// physics.inp, chemistry.inp, weno.inp) by name and the interior grid
+// (coordinates of each dimension, concatenated).  read_deck_memory parses it
+// like read_deck and leaves u0 and imap empty for the caller to generate.
+struct DeckMemory {
+  std::map<std::string, std::string> files;
+  std::vector<double> grid;
+};
+int read_deck_memory(const DeckMemory& m, Deck& d, std::string& err);
 // Flat device parameters from a parsed deck.
 int make_params(const Deck& d, DevParams& P, std::string& err);
 // Write an op_*.bin file (WriteBinary.c:37-93) from the interior AoS field.

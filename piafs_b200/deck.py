@@ -25,15 +25,27 @@ from typing import Dict, List, Optional, Sequence
 import numpy as np
 
 
+def _num(v) -> str:
+    """A value as the reference's fscanf reads it: floats (numpy ones too) in
+    shortest round-trip form, integers plainly, anything else as str."""
+    if isinstance(v, (bool, np.bool_)):
+        return str(v)
+    if isinstance(v, (int, np.integer)):
+        return str(int(v))
+    if isinstance(v, (float, np.floating)):
+        return repr(float(v))
+    return str(v)
+
+
 def write_keyfile(path: str, items: Dict[str, object]) -> None:
     """Write a ``begin ... end`` keyword file, one ``key value`` per line."""
     with open(path, "w") as f:
         f.write("begin\n")
         for k, v in items.items():
             if isinstance(v, (list, tuple)):
-                v = " ".join(str(a) for a in v)
-            elif isinstance(v, float):
-                v = repr(v)
+                v = " ".join(_num(a) for a in v)
+            else:
+                v = _num(v)
             f.write(f"  {k:<20s} {v}\n")
         f.write("end\n")
 
