@@ -54,7 +54,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--workload", default="ns2d_photochem", choices=["ns2d_photochem", "euler1d", "ensemble"])
+    ap.add_argument("--workload", default="ns2d_photochem",
+                    choices=["ns2d_photochem", "euler1d", "ensemble", "serving"])
+    ap.add_argument("--requests", type=int, default=1000, help="serving requests (the stream's first n)")
+    ap.add_argument("--hbm-budget-gb", type=float, default=120.0)
     ap.add_argument("--members", type=int, default=256, help="ensemble members")
     ap.add_argument("--member-steps", type=int, default=100, help="steps per ensemble member")
     ap.add_argument("--n", type=int, default=None, help="grid size (default 2048 / 1024)")
@@ -297,6 +300,45 @@ def ensemble_bench(a):
     return 0
 
 
+# ------------------------------------------------------------------ serving
+def serving_bench(a):
+    """The request stream of cases.serving_trace (Poisson arrivals at 2000
+    requests/s, 70% 1D Euler / 30% 2D photochemical, 50-500 steps), its first
+    --requests requests replayed in real time through the continuous-batching
+    serving loop under the HBM budget.  Latency = result ready - arrival."""
+    import numpy as np
+    import torch
+    from piafs_b200 import Request, serve_trace, cases
+
+    torch.cuda.init()
+    reqs, arr = cases.serving_trace(n=a.requests)
+    rq = [Request(**r) for r in reqs]
+    # warm the context and the kernels
+    serve_trace(rq[:2], [0.0, 0.0], precision=a.precision)
+    budget = int(a.hbm_budget_gb * 1e9)
+    t0 = time.perf_counter()
+    res = serve_trace(rq, list(arr), precision=a.precision, hbm_budget_bytes=budget, steps_per_round=4)
+    wall = time.perf_counter() - t0
+    lat = np.array([r["finished_s"] - r["arrival_s"] for r in res])
+    wait = np.array([r["admitted_s"] - r["arrival_s"] for r in res])
+    units = sum(3 * q["nsteps"] * (q["n"] if q["kind"] == 1 else q["n"] ** 2) for q in reqs)
+    span = max(r["finished_s"] for r in res) - min(r["arrival_s"] for r in res)
+    line = {"metric": "served solves/s", "value": len(res) / span, "unit": "solves/s", "n_gpus": 1,
+            "higher_is_better": True, "vs_baseline": None,
+            "dtype": "f64" if a.precision == "fp64" else "f32+f64", "data": "synthetic (seeded request stream)",
+            "config": {"workload": f"serving_{len(res)}req_poisson2000_70pct1d_30pct2d_50to500steps",
+                       "requests": len(res), "rate_per_s": 2000.0, "precision": a.precision,
+                       "hbm_budget_gb": a.hbm_budget_gb, "steps_per_round": 4,
+                       "pt_stage_updates": units},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "queue_wait_s": {"p50": float(np.percentile(wait, 50)), "p99": float(np.percentile(wait, 99))},
+            "makespan_s": span, "wall_s": wall, "pt_stage_updates_per_s": units / span,
+            "finite": bool(all(np.isfinite(r["checksum"]) for r in res))}
+    print(json.dumps(line))
+    return 0
+
+
 # --------------------------------------------------------------------- main
 def main():
     a = parse()
@@ -308,6 +350,8 @@ def main():
 
     if a.workload == "ensemble" and a.impl == "gpu":
         return ensemble_bench(a) if rank == 0 else 0
+    if a.workload == "serving" and a.impl == "gpu":
+        return serving_bench(a) if rank == 0 else 0
 
     if a.impl == "reference":
         if rank != 0:

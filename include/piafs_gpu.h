@@ -212,6 +212,9 @@ int piafs_gpu_batch_member(piafs_gpu_batch* batch, int id, double* t, int* iter,
 /* The stage derivative k_stage (TimeRHSFunctionExplicit's rhs) of the
  * member's last step, interior points in the layout of the op files. */
 int piafs_gpu_batch_get_stage_derivative(piafs_gpu_batch* batch, int id, int stage, double* k_interior);
+/* A member's state buffers with ghosts, reference layout: which = 0 the
+ * solution, 1 and 2 the two stage-state buffers of its last step. */
+int piafs_gpu_batch_get_buffer(piafs_gpu_batch* batch, int id, int which, double* u_ghosted);
 /* Release a member's device memory (finished or not). */
 int piafs_gpu_batch_remove(piafs_gpu_batch* batch, int id);
 int piafs_gpu_batch_get_info(piafs_gpu_batch* batch, piafs_gpu_batch_info* info);

@@ -77,6 +77,7 @@ SIGNATURES = {
                                          C.POINTER(C.c_int)]),
     "piafs_gpu_batch_remove": (C.c_int, [_vp, C.c_int]),
     "piafs_gpu_batch_get_stage_derivative": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
+    "piafs_gpu_batch_get_buffer": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
     "piafs_gpu_batch_get_info": (C.c_int, [_vp, _vp]),
     "piafs_gpu_batch_tune": (C.c_int, [_vp, C.c_int]),
     "piafs_gpu_batch_set_launch": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),

@@ -30,6 +30,7 @@
 // tile still reads as halo; the last stage updates u in place (pointwise),
 // except for one-stage schemes, which write buffer 0 and swap it with u.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <chrono>
@@ -213,7 +214,7 @@ template <int TX, int TY>
 __host__ __device__ constexpr long long smem2d(int nv) { return Tile2D<TX, TY>::smem(nv); }
 
 template <int TX, int TY, int UPW, int BT>
-__device__ __noinline__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, double* smem) {
+__device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, double* smem) {
   typedef Tile2D<TX, TY> T;
   constexpr int HX = T::HX, HY = T::HY, NXI = T::NXI, NYI = T::NYI, NI = T::NI, NCX = T::NCX, NCY = T::NCY;
   const DevParams& P = M.P;
@@ -394,7 +395,7 @@ __host__ __device__ constexpr long long smem1d(int nv) {
 }
 
 template <int UPW, int BT>
-__device__ __noinline__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double* smem) {
+__device__ __forceinline__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double* smem) {
   constexpr int T1 = BT;
   const DevParams& P = M.P;
   constexpr int HX = T1 + 2 * H, LX = T1 + 1, NF = 3;
@@ -661,6 +662,11 @@ long long smem_bytes(int shape, int nv) {
 }
 
 int persistent_grid(piafs_gpu_batch* B) {
+  // PIAFS_GPU_BATCH_GRID=n overrides the number of persistent CTAs
+  if (const char* g = std::getenv("PIAFS_GPU_BATCH_GRID")) {
+    const int n = std::atoi(g);
+    if (n > 0) return n;
+  }
   const long long sm = smem_bytes(B->shape, std::max(B->max_nv, 1));
   int per_sm = 0;
   PIAFS_SHAPE_SWITCH(B->shape, per_sm = Ops::per_sm(sm));
@@ -1110,6 +1116,27 @@ int piafs_gpu_batch_get_stage_derivative(piafs_gpu_batch* B, int id, int stage, 
   cudaFreeAsync(tmp, B->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
   if (e != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string("stage derivative: ") + cudaGetErrorString(e));
+  return PIAFS_OK;
+}
+
+int piafs_gpu_batch_get_buffer(piafs_gpu_batch* B, int id, int which, double* out) {
+  if (!B || !out || id < 0 || id >= (int)B->members.size() || !B->members[id].used || which < 0 || which > 2)
+    return nfail(PIAFS_ERR_ARGUMENT, "bad argument");
+  const BMember& bm = B->members[id].bm;
+  BState st;
+  BCK(cudaMemcpyAsync(&st, B->dstate + id, sizeof(BState), cudaMemcpyDeviceToHost, B->stream));
+  BCK(cudaStreamSynchronize(B->stream));
+  const double* src = which == 0 ? st.u : which == 1 ? bm.X : bm.Y;
+  const DevParams& P = bm.P;
+  double* tmp = nullptr;
+  const size_t n = (size_t)P.npg * P.nvars;
+  BCK(cudaMallocAsync((void**)&tmp, n * sizeof(double), B->stream));
+  launch_soa_to_aos(src, tmp, P.npg, P.nvars, P.ps, B->stream);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, B->stream);
+  cudaFreeAsync(tmp, B->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+  if (e != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string("buffer: ") + cudaGetErrorString(e));
   return PIAFS_OK;
 }
 

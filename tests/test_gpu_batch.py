@@ -191,3 +191,32 @@ def test_autotuner_restores_state_and_picks_a_config(tmp_path):
             j = c.add(mix[0][0], mix[0][1])
             c.step(mix[0][1])
             assert np.array_equal(c.solution(j), b.solution(ids[0]))
+
+
+def test_persistent_ctas_walking_many_tiles(tmp_path, monkeypatch):
+    """One persistent CTA walks every tile of members whose sides are not
+    multiples of the tile (partial edge tiles), through all RK stages: the
+    results are those of the full grid of CTAs, bit for bit, and of the
+    single-simulation path to the parity bar."""
+    decks = []
+    for k, (n, ts) in enumerate([(117, "ssprk3"), (100, "22"), (75, "44")]):
+        d = os.path.join(str(tmp_path), f"p{k}")
+        cases.ns2d_photochem_beam(d, N=n, n_iter=3, scheme="weno5", dt=8e-5, time_scheme_type=ts,
+                                  op_file_format="none", seed=k)
+        decks.append(d)
+    e = os.path.join(str(tmp_path), "e")
+    cases.euler1d_density_wave(e, N=1500, n_iter=3, dt=1e-4, scheme="weno5", op_file_format="none")
+    decks.append(e)
+
+    def run():
+        with Batch() as b:
+            ids = [b.add(d, 3) for d in decks]
+            b.step(3)
+            return [b.solution(i) for i in ids]
+
+    full = run()
+    monkeypatch.setenv("PIAFS_GPU_BATCH_GRID", "1")
+    one = run()
+    for d, a, b in zip(decks, full, one):
+        assert np.array_equal(a, b), d
+        assert_close(a, alone(d, 3), d)
