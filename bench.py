@@ -37,6 +37,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BYTES_PER_UNIT = {11: 264, 4: 96, 3: 72}   # 3 * nvars * 8: read U_s, read u_n, write (FP64 state)
+# measured DRAM traffic of one CRWENO5 line-solve launch per interior point
+# (dram__bytes_read + dram__bytes_write, ncu at 1536^2, 11 variables)
+TRAFFIC_PER_POINT = {11: (417.0e6 + 774.2e6) / (1536 * 1536)}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 CPU_SAMPLE_N = 512                          # sample grid of the CPU arms
 # Steps timed back to back from the initial condition before the state is
@@ -470,13 +473,13 @@ def main():
             peaks = json.load(open(pk))
         peak = peaks.get("hbm_gbs", 6650.0)
         achieved = bpu * npts / (phases[dom] / 1e3) / 1e9
+        # DRAM bytes per launch of the dominant kernel from the ncu capture of
+        # k_crweno_pair at 1536^2 (read + write per interior point, scaled by
+        # the points processed); known for the FP64 CRWENO5 line solve only
         traffic = None
-        tf = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
-        if os.path.exists(tf):
-            tj = json.load(open(tf))
-            ent = tj.get(dom)
-            if ent and ent.get("grid") == info["dim"][:info["ndims"]]:
-                traffic = ent["bytes"]
+        if dom.startswith("reconstruct") and a.precision == "fp64" and (a.scheme or "crweno5") == "crweno5" \
+                and info["nvars"] in TRAFFIC_PER_POINT:
+            traffic = TRAFFIC_PER_POINT[info["nvars"]] * npts
         step_ms = ms_max / a.steps
         path_gbs = bpu * units_per_step / (step_ms / 1e3) / 1e9 / 1.0
         roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
