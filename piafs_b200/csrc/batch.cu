@@ -2,24 +2,14 @@
 //
 // The reference runs an ensemble one member after another (one deck each,
 // OutputSolution.cpp).  Here every member lives on the device at once and one
-// persistent kernel per Runge-Kutta stage advances all of them: a CTA walks a
-// device-side list of tiles (tile -> member), and for each tile it
-//   1. loads the stage state on the tile plus a 3-cell halo into shared
-//      memory, computing boundary ghosts on the fly from the member's zones
-//      (bc_point, the rule of the boundary kernels),
-//   2. reconstructs the WENO5 interface values of u and of the cell-centred
-//      flux at every x and y interface of the tile (weno5_iface), upwinds
-//      them (upwind_flow) and forms -dxinv (fI[+1] - fI) in both directions,
-//   3. adds the viscous terms (2D, FirstDerivativeFirstOrder stencils on the
-//      tile) and the photochemical source,
-//   4. writes the stage derivative k_s and the next stage state
-//      U_{s+1} = u + dt sum_j a_{s+1,j} k_j, or at the last stage
-//      u <- u + dt sum_j b_j k_j.
-// The expressions are those of the single-simulation kernels; a member's FP64
-// result agrees with its deck run alone to rounding (the compiler contracts
-// multiply-adds differently in the fused kernel), and it is bit for bit the
-// same whatever other members share the batch, since a tile's arithmetic
-// depends only on its own member.
+// persistent kernel per Runge-Kutta stage advances all of them, a CTA per
+// tile of a device-side tile list (batch_tile.cuh has the stage kernel; the
+// FP64 and the mixed-precision instances are compiled in batch_stage_fp64.cu
+// and batch_stage_mixed.cu).  A member's FP64 result agrees with its deck run
+// alone to rounding (the compiler contracts multiply-adds differently in the
+// fused kernel), and in either precision it is bit for bit the same whatever
+// other members share the batch, since a tile's arithmetic depends only on
+// its own member.
 // A per-step epilogue advances the members' clocks and retires members that
 // reached their step count.  The tile list and the member table are device
 // arrays the host rewrites between steps, so one CUDA graph of a step serves
@@ -43,442 +33,16 @@
 
 #include "../../include/piafs_gpu.h"
 #include "deck.h"
-#include "kernels.h"
-#include "physics.cuh"
-#include "source.cuh"
+#include "batch_tile.cuh"
 
 namespace piafs {
 int set_last_error(int code, const std::string& msg);   // api.cu: piafs_gpu_last_error()
 }
 
 using namespace piafs;
+using namespace piafs::batch;
 
 namespace {
-
-constexpr int H = 3;             // halo (WENO5 stencil half-width)
-
-// Host-written description of one member.
-struct BMember {
-  DevParams P;
-  double* X;                     // stage buffers (ghosted SoA planes)
-  double* Y;
-  double* k[MAX_STAGES];         // stage derivatives
-  const double* dxinv;
-  const double* imap;
-  Zone zones[MAX_ZONES];
-  int nzones;
-  int nstages;
-  double a[MAX_STAGES * MAX_STAGES];   // dt * A, row s = coefficients of stage s
-  double b[MAX_STAGES];                // dt * b
-  double c[MAX_STAGES];
-  int tile_off, tnx, tny;
-  int nsteps;
-};
-// Device-written state of one member.
-struct BState {
-  double* u;                     // solution u_n (swapped with X by one-stage schemes)
-  double* X;
-  double t;
-  int iter;
-  int active;
-};
-
-// ------------------------------------------------------------ ghost values
-// Value of every variable at tile point (i, j) of stage state S: interior
-// points from memory, edge ghosts (exactly one index outside the domain, at
-// most 3 deep) from the last boundary zone that covers them, other points 0
-// (corners; never used by the stencils).  A slip wall sets the flow variables
-// and leaves the others as they are in memory, as the boundary kernel does.
-__device__ __forceinline__ void load_point(const BMember& M, const double* S, int i, int j, double* out,
-                                           int ostride) {
-  const DevParams& P = M.P;
-  const bool xin = i >= 0 && i < P.N0, yin = j >= 0 && j < P.N1;
-  const int nv = P.nvars;
-  const bool edge = !(xin && yin) && ((yin && i >= -P.ghosts && i < P.N0 + P.ghosts) ||
-                                      (P.ndims == 2 && xin && j >= -P.ghosts && j < P.N1 + P.ghosts));
-  if (!(xin && yin) && !edge) {
-    for (int v = 0; v < nv; v++) out[v * ostride] = 0.0;
-    return;
-  }
-  const long long p = pidx(P, i, j);
-  for (int v = 0; v < nv; v++) out[v * ostride] = S[v * P.ps + p];
-  if (!edge) return;
-  for (int zi = M.nzones - 1; zi >= 0; zi--) {
-    const Zone& z = M.zones[zi];
-    if (i >= z.is[0] && i < z.ie[0] && j >= z.is[1] && j < z.ie[1]) {
-      bc_point(P, z, S, i, j, out, ostride);
-      return;
-    }
-  }
-}
-
-// Cell-centred fluxes of every variable at a tile cell (ns2d_flux /
-// euler1d_flux, passive variables vn u_m) into f[m * fstride]; vn returned.
-template <int MODEL>
-__device__ __forceinline__ double cell_flux(const DevParams& P, const double* sU, int vs, int c, int dir, double* f,
-                                            int fstride) {
-  constexpr int NF = Flow<MODEL>::NF;
-  double fl[4] = {0.0, 0.0, 0.0, 0.0}, vn;
-  if (MODEL == NS2D) ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, dir, fl, vn);
-  else euler1d_flux(sU[c], sU[vs + c], sU[2 * vs + c], P.gamma, fl, vn);
-#pragma unroll
-  for (int m = 0; m < NF; m++) f[m * fstride] = fl[m];
-  for (int m = NF; m < P.nvars; m++) f[m * fstride] = __dmul_rn(vn, sU[m * vs + c]);
-  return vn;
-}
-
-// The four WENO5 values of one variable at one interface: u at u[(r-3)*ust]
-// and its flux at f[(r-3)*fst] for the cells r = 0..5 (i-3..i+2).
-__device__ __forceinline__ void iface_weno(const DevParams& P, const double* u, int ust, const double* f, int fst,
-                                           double& uL, double& uR, double& fL, double& fR) {
-  double a[6], b[6];
-#pragma unroll
-  for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * ust]; b[r] = f[(r - 3) * fst]; }
-  weno5_iface(P, a, b, uL, uR, fL, fR);
-}
-
-// Characteristic / scalar upwinding of the flow variables at one interface
-// from their WENO values rec[k * ks + m * ms] (k: uL, uR, fL, fR) and the cell
-// states left / right (ucl, ucr at stride vs); flux to so[m * sstride],
-// passive-variable scheme data to *spa / *spm.
-template <int MODEL, int UPW>
-__device__ __noinline__ void iface_upwind_flow(const DevParams& P, const double* rec, int ks, int ms,
-                                               const double* ucl, const double* ucr, int vs, int dir, double* so,
-                                               int sstride, double* spa, int* spm) {
-  constexpr int NF = Flow<MODEL>::NF;
-  double uL[4], uR[4], fL[4], fR[4], cl[4], cr[4], fi[4];
-#pragma unroll
-  for (int m = 0; m < NF; m++) {
-    uL[m] = rec[m * ms]; uR[m] = rec[ks + m * ms]; fL[m] = rec[2 * ks + m * ms]; fR[m] = rec[3 * ks + m * ms];
-    cl[m] = ucl[m * vs]; cr[m] = ucr[m * vs];
-  }
-  upwind_flow<MODEL, UPW, double>(uL, uR, fL, fR, cl, cr, P.gamma, dir, fi, spa, spm);
-#pragma unroll
-  for (int m = 0; m < NF; m++) so[m * sstride] = fi[m];
-}
-
-// the Runge-Kutta part of stage s at point p with stage derivatives k
-__device__ __forceinline__ void rk_point(const BMember& M, const BState& Sd, int s, long long p, int nv) {
-  const long long ps = M.P.ps;
-  if (s < M.nstages - 1) {
-    double* dst = (s % 2 == 0) ? M.X : M.Y;
-    for (int v = 0; v < nv; v++) {
-      const long long q = v * ps + p;
-      double x = Sd.u[q];
-      for (int j = 0; j <= s; j++) x += M.a[(s + 1) * MAX_STAGES + j] * M.k[j][q];
-      dst[q] = x;
-    }
-  } else {
-    double* dst = M.nstages == 1 ? Sd.X : Sd.u;
-    for (int v = 0; v < nv; v++) {
-      const long long q = v * ps + p;
-      double x = Sd.u[q];
-      for (int j = 0; j < M.nstages; j++) x += M.b[j] * M.k[j][q];
-      dst[q] = x;
-    }
-  }
-}
-
-// ------------------------------------------------------------- 2D tile
-// One tile of TX x TY points, worked by BT threads in phases separated by
-// barriers; each phase is a list of small items over both directions, so
-// every thread stays light and the phases stay balanced:
-//   load     the stage state on the tile + 3-cell halo (boundary ghosts on
-//            the fly)
-//   fluxes   flow-variable fluxes and the normal velocity at every stencil
-//            cell of either direction
-//   WENO     WENO5 values of the flow variables, item = (interface, var)
-//   upwind   characteristic/scalar upwinding, item = interface
-//   passive  WENO5 + scalar upwinding of a passive variable (flux vn u_m),
-//            item = (interface, var)
-//   viscous  Q, viscous face fluxes (k_visc_source on the tile)
-//   point    stage derivative, chemistry, Runge-Kutta combination
-// Interfaces are numbered x first (f < NXI: row jj, position ii) then y.
-// Shared memory (doubles): sU [nv][HY][HX]; interface fluxes fx [nv][NXI] and
-// fy [nv][NYI]; a work region, reused by the viscous phase: cell data
-// [5][NCX] + [5][NCY], WENO values [4][4][NXI+NYI], passive speed and scheme
-// [NXI+NYI] each.
-template <int TX, int TY>
-struct Tile2D {
-  static constexpr int HX = TX + 6, HY = TY + 6;
-  static constexpr int NXI = TY * (TX + 1), NYI = TX * (TY + 1), NI = NXI + NYI;
-  static constexpr int NCX = TY * HX, NCY = TX * HY;            // stencil cells per direction
-  static constexpr int VISC = 3 * (TY + 2) * (TX + 2) + 3 * TY * (TX + 1) + 3 * (TY + 1) * TX;
-  static constexpr int WORK0 = 5 * (NCX + NCY) + 16 * NI + 2 * NI;
-  static constexpr int WORK = WORK0 > VISC ? WORK0 : VISC;
-  __host__ __device__ static constexpr long long smem(int nv) {
-    return (long long)nv * (HX * HY + NXI + NYI) + WORK;
-  }
-};
-template <int TX, int TY>
-__host__ __device__ constexpr long long smem2d(int nv) { return Tile2D<TX, TY>::smem(nv); }
-
-template <int TX, int TY, int UPW, int BT>
-__device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, double* smem) {
-  typedef Tile2D<TX, TY> T;
-  constexpr int HX = T::HX, HY = T::HY, NXI = T::NXI, NYI = T::NYI, NI = T::NI, NCX = T::NCX, NCY = T::NCY;
-  const DevParams& P = M.P;
-  const int nv = P.nvars, N0 = P.N0, N1 = P.N1;
-  const int i0 = tx * TX, j0 = ty * TY;
-  const double* S = s == 0 ? Sd.u : ((s - 1) % 2 == 0 ? M.X : M.Y);
-  constexpr int vs = HX * HY;
-  double* sU = smem;
-  double* fx = sU + nv * vs;                   // [m][jj * (TX+1) + ii]
-  double* fy = fx + nv * NXI;                  // [m][ii * (TY+1) + jj]
-  double* wk = fy + nv * NYI;                  // work region
-  double* cx = wk;                             // [5][NCX]: 4 flow fluxes + vn, x cells
-  double* cy = cx + 5 * NCX;                   // [5][NCY]
-  double* rec = cy + 5 * NCY;                  // [k][m][NI]
-  double* spa = rec + 16 * NI;                 // [NI]
-  int* spm = (int*)(spa + NI);                 // [NI]
-  const int tid = threadIdx.x;
-  for (int e = tid; e < vs; e += BT) load_point(M, S, i0 - H + e % HX, j0 - H + e / HX, sU + e, vs);
-  __syncthreads();
-  // cell data: x cells (row jj, column a): c = (jj+H)*HX + a; y cells
-  // (column ii, row b): c = b*HX + ii + H
-  for (int e = tid; e < NCX + NCY; e += BT) {
-    const bool xd = e < NCX;
-    const int g = xd ? e : e - NCX;
-    const int c = xd ? (g / HX + H) * HX + g % HX : (g % HY) * HX + g / HY + H;
-    double f[4], vn;
-    ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, xd ? 0 : 1, f, vn);
-    double* o = xd ? cx + g : cy + g;
-    const int st = xd ? NCX : NCY;
-#pragma unroll
-    for (int m = 0; m < 4; m++) o[m * st] = f[m];
-    o[4 * st] = vn;
-  }
-  __syncthreads();
-  // geometry of interface f: its cell i (right of the interface) in sU
-  // (base, stride ust along the line), in the cell data (cb, plane cst) and
-  // whether it is inside the member
-  auto geo = [&](int f, int& base, int& ust, const double*& cd, int& cst, int& dir) -> bool {
-    if (f < NXI) {
-      const int ii = f % (TX + 1), jj = f / (TX + 1);
-      base = (jj + H) * HX + ii + H; ust = 1; cd = cx + jj * HX + ii + H; cst = NCX; dir = 0;
-      return i0 + ii <= N0 && j0 + jj < N1;
-    }
-    const int g = f - NXI, jj = g % (TY + 1), ii = g / (TY + 1);
-    base = (jj + H) * HX + ii + H; ust = HX; cd = cy + ii * HY + jj + H; cst = NCY; dir = 1;
-    return j0 + jj <= N1 && i0 + ii < N0;
-  };
-  for (int e = tid; e < 4 * NI; e += BT) {
-    const int m = e / NI, f = e % NI;
-    int base, ust, cst, dir;
-    const double* cd;
-    if (!geo(f, base, ust, cd, cst, dir)) continue;
-    iface_weno(P, sU + m * vs + base, ust, cd + m * cst, 1, rec[(0 * 4 + m) * NI + f], rec[(1 * 4 + m) * NI + f],
-               rec[(2 * 4 + m) * NI + f], rec[(3 * 4 + m) * NI + f]);
-  }
-  __syncthreads();
-  for (int f = tid; f < NI; f += BT) {
-    int base, ust, cst, dir;
-    const double* cd;
-    if (!geo(f, base, ust, cd, cst, dir)) continue;
-    double* so = f < NXI ? fx + f : fy + (f - NXI);
-    iface_upwind_flow<NS2D, UPW>(P, rec + f, 4 * NI, NI, sU + base - ust, sU + base, vs, dir, so,
-                                 f < NXI ? NXI : NYI, spa + f, spm + f);
-  }
-  __syncthreads();
-  const int np = nv - 4;
-  for (int e = tid; e < np * NI; e += BT) {
-    const int m = 4 + e / NI, f = e % NI;
-    int base, ust, cst, dir;
-    const double* cd;
-    if (!geo(f, base, ust, cd, cst, dir)) continue;
-    const double* u = sU + m * vs + base;
-    const double* vn = cd + 4 * cst;
-    double a[6], b[6], l, r, fl, fr;
-#pragma unroll
-    for (int q = 0; q < 6; q++) { a[q] = u[(q - 3) * ust]; b[q] = __dmul_rn(vn[q - 3], a[q]); }
-    weno5_iface(P, a, b, l, r, fl, fr);
-    const double h = upwind_species(spm[f], spa[f], l, r, fl, fr);
-    if (f < NXI) fx[m * NXI + f] = h;
-    else fy[m * NYI + f - NXI] = h;
-  }
-  __syncthreads();
-  // viscous fluxes (k_visc_source on this tile), in the work region
-  const bool visc = P.viscous != 0;
-  constexpr int QX = TX + 2, QY = TY + 2, FX = TX + 1, FY = TY + 1;
-  double* sQ = wk;                              // [3][QY][QX]
-  double* sVx = sQ + 3 * QY * QX;               // [3][TY][FX]
-  double* sVy = sVx + 3 * TY * FX;              // [3][FY][TX]
-  if (visc) {
-    for (int e = tid; e < QX * QY; e += BT) {
-      const int a = e % QX, b = e / QX;
-      const int i = i0 - 1 + a, j = j0 - 1 + b;
-      double uu = 0.0, vv = 0.0, TT = 0.0;
-      const bool xin = i >= 0 && i < N0, yin = j >= 0 && j < N1;
-      if ((xin || yin) && i >= -P.ghosts && i < N0 + P.ghosts && j >= -P.ghosts && j < N1 + P.ghosts) {
-        const int c = (b - 1 + H) * HX + (a - 1 + H);
-        double rho, e_, pr;
-        ns_flowvar(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, rho, uu, vv, e_, pr);
-        TT = P.gamma * pr / rho;
-      }
-      sQ[e] = uu; sQ[QX * QY + e] = vv; sQ[2 * QX * QY + e] = TT;
-    }
-    __syncthreads();
-    const double two_third = 2.0 / 3.0, inv_Re = 1.0 / P.Re, inv_Pr = 1.0 / P.Pr;
-    const double igm1 = 1.0 / (P.gamma - 1.0);
-    const double* su = sQ;
-    const double* sv = sQ + QX * QY;
-    const double* sT = sQ + 2 * QX * QY;
-    for (int e = tid; e < FX * FY; e += BT) {
-      const int a = e % FX, b = e / FX;
-      const int i = i0 - 1 + a, j = j0 - 1 + b;
-      const bool need_x = (b >= 1) && (j < N1) && (i < N0);
-      const bool need_y = (a >= 1) && (i < N0) && (j < N1);
-      if (!need_x && !need_y) continue;
-      const int q = b * QX + a;
-      const double dxi = M.dxinv[P.ghosts + i], dyi = M.dxinv[P.W0 + P.ghosts + j];
-      const bool row_int = (j >= 0 && j < N1), col_int = (i >= 0 && i < N0);
-      const double uc = su[q], vc = sv[q], Tc = sT[q];
-      const double ux = row_int ? dxi * (su[q + 1] - uc) : 0.0;
-      const double vx = row_int ? dxi * (sv[q + 1] - vc) : 0.0;
-      const double Tx = row_int ? dxi * (sT[q + 1] - Tc) : 0.0;
-      const double uy = col_int ? dyi * (su[q + QX] - uc) : 0.0;
-      const double vy = col_int ? dyi * (sv[q + QX] - vc) : 0.0;
-      const double Ty = col_int ? dyi * (sT[q + QX] - Tc) : 0.0;
-      double mu, kappa;
-      visc_coeffs<double>(P, Tc, mu, kappa);
-      const double mre = mu * inv_Re, kre = kappa * inv_Re * igm1 * inv_Pr;
-      if (need_x) {
-        const double txx = two_third * mre * (2.0 * ux - vy), txy = mre * (uy + vx);
-        double* f = sVx + (b - 1) * FX + a;
-        f[0] = txx; f[TY * FX] = txy; f[2 * TY * FX] = uc * txx + vc * txy + kre * Tx;
-      }
-      if (need_y) {
-        const double tyx = mre * (uy + vx), tyy = two_third * mre * (-ux + 2.0 * vy);
-        double* f = sVy + b * TX + (a - 1);
-        f[0] = tyx; f[FY * TX] = tyy; f[2 * FY * TX] = uc * tyx + vc * tyy + kre * Ty;
-      }
-    }
-    __syncthreads();
-  }
-  // stage derivative and the Runge-Kutta combination, one point per thread
-  if (tid >= TX * TY) return;
-  const int pi = tid % TX, pj = tid / TX, i = i0 + pi, j = j0 + pj;
-  if (i >= N0 || j >= N1) return;
-  const long long p = pidx(P, i, j);
-  const long long ps = P.ps;
-  double* ks = M.k[s];
-  const double dxi = M.dxinv[P.ghosts + i], dyi = M.dxinv[P.W0 + P.ghosts + j];
-  constexpr int LX = TX + 1, LY = TY + 1;
-  for (int m = 0; m < nv; m++) {
-    const double hx = dxi * (fx[m * NXI + pj * LX + pi + 1] - fx[m * NXI + pj * LX + pi]);
-    const double hy = dyi * (fy[m * NYI + pi * LY + pj + 1] - fy[m * NYI + pi * LY + pj]);
-    const double h = hx + hy;
-    ks[m * ps + p] = -h;
-  }
-  if (visc) {
-#pragma unroll
-    for (int m = 0; m < 3; m++) {
-      const double par = dxi * (sVx[m * TY * FX + pj * FX + pi + 1] - sVx[m * TY * FX + pj * FX + pi]) +
-                         dyi * (sVy[m * FY * TX + (pj + 1) * TX + pi] - sVy[m * FY * TX + pj * TX + pi]);
-      ks[(m + 1) * ps + p] += par;
-    }
-  }
-  if (P.chem) {
-    const double t = Sd.t + M.c[s] * P.dt;
-    chem_source_point<double>(P, S, p, pulse_factor(P, t), M.imap[p], ks);
-  }
-  rk_point(M, Sd, s, p, nv);
-}
-
-// ------------------------------------------------------------- 1D tile
-// A 1D tile has T1 points, one per thread.  Shared memory (doubles): sU
-// [nv][T1+6], cell fluxes [nv][T1+6], interface fluxes [nv][T1+1], flow WENO
-// values [4][3][T1+1], passive speed and scheme
-template <int T1>
-__host__ __device__ constexpr long long smem1d(int nv) {
-  return (long long)nv * (2 * (T1 + 2 * H) + (T1 + 1)) + 14LL * (T1 + 1);
-}
-
-template <int UPW, int BT>
-__device__ __forceinline__ void tile1d(const BMember& M, const BState& Sd, int s, int tx, double* smem) {
-  constexpr int T1 = BT;
-  const DevParams& P = M.P;
-  constexpr int HX = T1 + 2 * H, LX = T1 + 1, NF = 3;
-  const int nv = P.nvars, N0 = P.N0;
-  const int i0 = tx * T1;
-  const double* S = s == 0 ? Sd.u : ((s - 1) % 2 == 0 ? M.X : M.Y);
-  double* sU = smem;
-  double* cf = sU + nv * HX;                 // [m][HX]
-  double* sF = cf + nv * HX;                 // [m][LX]
-  double* rec = sF + nv * LX;                // [k][m][LX]
-  double* spa = rec + 12 * LX;
-  int* spm = (int*)(spa + LX);
-  const int tid = threadIdx.x;
-  for (int e = tid; e < HX; e += BT) load_point(M, S, i0 - H + e, 0, sU + e, HX);
-  __syncthreads();
-  for (int e = tid; e < HX; e += BT) cell_flux<EULER1D>(P, sU, HX, e, 0, cf + e, HX);
-  __syncthreads();
-  for (int e = tid; e < NF * LX; e += BT) {
-    const int m = e / LX, f = e % LX;
-    if (i0 + f > N0) continue;
-    iface_weno(P, sU + m * HX + f + H, 1, cf + m * HX + f + H, 1, rec[(0 * NF + m) * LX + f],
-               rec[(1 * NF + m) * LX + f], rec[(2 * NF + m) * LX + f], rec[(3 * NF + m) * LX + f]);
-  }
-  __syncthreads();
-  for (int f = tid; f < LX; f += BT) {
-    if (i0 + f > N0) continue;
-    iface_upwind_flow<EULER1D, UPW>(P, rec + f, NF * LX, LX, sU + f + H - 1, sU + f + H, HX, 0, sF + f, LX,
-                                    spa + f, spm + f);
-  }
-  __syncthreads();
-  for (int e = tid; e < (nv - NF) * LX; e += BT) {
-    const int m = NF + e / LX, f = e % LX;
-    if (i0 + f > N0) continue;
-    double l, r, fl, fr;
-    iface_weno(P, sU + m * HX + f + H, 1, cf + m * HX + f + H, 1, l, r, fl, fr);
-    sF[m * LX + f] = upwind_species(spm[f], spa[f], l, r, fl, fr);
-  }
-  __syncthreads();
-  const int i = i0 + tid;
-  if (tid >= T1 || i >= N0) return;
-  const long long p = pidx(P, i, 0);
-  double* ks = M.k[s];
-  const double dxi = M.dxinv[P.ghosts + i];
-  for (int m = 0; m < nv; m++) {
-    const double h = dxi * (sF[m * LX + tid + 1] - sF[m * LX + tid]);
-    ks[m * P.ps + p] = -h;
-  }
-  rk_point(M, Sd, s, p, nv);
-}
-
-// --------------------------------------------------------------- kernels
-template <int TX, int TY, int BT, int MINB>
-__global__ void __launch_bounds__(BT, MINB) k_batch_stage(const BMember* __restrict__ mem,
-                                                          const BState* __restrict__ st,
-                                                          const int* __restrict__ tile_member,
-                                                          const int* __restrict__ ntiles, int s) {
-  extern __shared__ double smem[];
-  const int nt = *ntiles;
-  for (int g = blockIdx.x; g < nt; g += gridDim.x) {
-    const int m = tile_member[g];
-    const BMember& M = mem[m];
-    const BState Sd = st[m];
-    if (!Sd.active || s >= M.nstages) continue;   // uniform over the CTA
-    const int local = g - M.tile_off;
-    if (M.P.ndims == 2) {
-      const int tx = local % M.tnx, ty = local / M.tnx;
-      switch (M.P.upwind) {
-        case UPW_ROE: tile2d<TX, TY, UPW_ROE, BT>(M, Sd, s, tx, ty, smem); break;
-        case UPW_RF: tile2d<TX, TY, UPW_RF, BT>(M, Sd, s, tx, ty, smem); break;
-        case UPW_LLF: tile2d<TX, TY, UPW_LLF, BT>(M, Sd, s, tx, ty, smem); break;
-        default: tile2d<TX, TY, UPW_RUSANOV, BT>(M, Sd, s, tx, ty, smem); break;
-      }
-    } else {
-      switch (M.P.upwind) {
-        case UPW_ROE: tile1d<UPW_ROE, BT>(M, Sd, s, local, smem); break;
-        case UPW_RF: tile1d<UPW_RF, BT>(M, Sd, s, local, smem); break;
-        case UPW_LLF: tile1d<UPW_LLF, BT>(M, Sd, s, local, smem); break;
-        default: tile1d<UPW_RUSANOV, BT>(M, Sd, s, local, smem); break;
-      }
-    }
-    __syncthreads();   // shared memory is reused by the next tile
-  }
-}
 
 // clocks (k_advance_time), step counts, retirement; status[2m] = iter,
 // status[2m+1] = active
@@ -592,43 +156,6 @@ int nfail(int code, const std::string& m) { return piafs::set_last_error(code, m
     if (e_ != cudaSuccess) return nfail(PIAFS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
   } while (0)
 
-// Launch configurations the tuner chooses from: 2D tile shape, threads per
-// CTA (also the points of a 1D tile) and the CTAs per SM the compiler is
-// asked to fit; 256-thread tiles are small enough for two CTAs per SM.
-struct TileShape { int tx, ty, nt, minb; };
-constexpr int kNumShapes = 5;
-constexpr TileShape kShapes[kNumShapes] = {
-    {16, 16, 512, 1}, {32, 8, 512, 1}, {16, 8, 256, 2}, {32, 4, 256, 2}, {8, 16, 256, 2}};
-
-template <int TX, int TY, int NT, int MINB>
-struct StageOps {
-  static long long smem(int nv) {
-    return std::max(smem2d<TX, TY>(nv), smem1d<NT>(nv)) * (long long)sizeof(double);
-  }
-  static cudaError_t attr(long long bytes) {
-    return cudaFuncSetAttribute(k_batch_stage<TX, TY, NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)bytes);
-  }
-  static int per_sm(long long bytes) {
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_stage<TX, TY, NT, MINB>, NT, bytes) != cudaSuccess)
-      n = 0;
-    return n;
-  }
-  static void launch(int grid, long long bytes, cudaStream_t st, const BMember* m, const BState* s, const int* tl,
-                     const int* nt, int stage) {
-    k_batch_stage<TX, TY, NT, MINB><<<grid, NT, bytes, st>>>(m, s, tl, nt, stage);
-  }
-};
-#define PIAFS_SHAPE_SWITCH(idx, CALL)                              \
-  switch (idx) {                                                   \
-    case 0: { typedef StageOps<16, 16, 512, 1> Ops; CALL; } break; \
-    case 1: { typedef StageOps<32, 8, 512, 1> Ops; CALL; } break;  \
-    case 2: { typedef StageOps<16, 8, 256, 2> Ops; CALL; } break;  \
-    case 3: { typedef StageOps<32, 4, 256, 2> Ops; CALL; } break;  \
-    default: { typedef StageOps<8, 16, 256, 2> Ops; CALL; } break; \
-  }
-
 }  // namespace
 
 struct piafs_gpu_batch {
@@ -655,10 +182,10 @@ struct piafs_gpu_batch {
 
 namespace {
 
-long long smem_bytes(int shape, int nv) {
-  long long r = 0;
-  PIAFS_SHAPE_SWITCH(shape, r = Ops::smem(nv));
-  return r;
+bool mixed(const piafs_gpu_batch* B) { return B->precision == PIAFS_PRECISION_MIXED; }
+
+long long smem_bytes(const piafs_gpu_batch* B, int shape, int nv) {
+  return mixed(B) ? StageTable<true>::smem(shape, nv) : StageTable<false>::smem(shape, nv);
 }
 
 int persistent_grid(piafs_gpu_batch* B) {
@@ -667,9 +194,9 @@ int persistent_grid(piafs_gpu_batch* B) {
     const int n = std::atoi(g);
     if (n > 0) return n;
   }
-  const long long sm = smem_bytes(B->shape, std::max(B->max_nv, 1));
+  const long long sm = smem_bytes(B, B->shape, std::max(B->max_nv, 1));
   int per_sm = 0;
-  PIAFS_SHAPE_SWITCH(B->shape, per_sm = Ops::per_sm(sm));
+  per_sm = mixed(B) ? StageTable<true>::per_sm(B->shape, sm) : StageTable<false>::per_sm(B->shape, sm);
   if (per_sm < 1) per_sm = 1;
   return per_sm * B->num_sms;
 }
@@ -751,17 +278,14 @@ int capture_graph(piafs_gpu_batch* B) {
       B->graph_stages == B->max_stages && B->graph_grid == grid)
     return PIAFS_OK;
   if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
-  const long long sm = smem_bytes(B->shape, B->max_nv);
-  {
-    cudaError_t ea = cudaSuccess;
-    PIAFS_SHAPE_SWITCH(B->shape, ea = Ops::attr(sm));
-    BCK(ea);
-  }
+  const long long sm = smem_bytes(B, B->shape, B->max_nv);
+  BCK(mixed(B) ? StageTable<true>::attr(B->shape, sm) : StageTable<false>::attr(B->shape, sm));
   cudaGraph_t g;
   BCK(cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
   for (int s = 0; s < B->max_stages && e == cudaSuccess; s++) {
-    PIAFS_SHAPE_SWITCH(B->shape, Ops::launch(grid, sm, B->stream, B->dmem, B->dstate, B->dtiles, B->dntiles, s));
+    if (mixed(B)) StageTable<true>::launch(B->shape, grid, sm, B->stream, B->dmem, B->dstate, B->dtiles, B->dntiles, s);
+    else StageTable<false>::launch(B->shape, grid, sm, B->stream, B->dmem, B->dstate, B->dtiles, B->dntiles, s);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) {
@@ -804,10 +328,10 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   {
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B->device);
-    if (smem_bytes(B->shape, std::max(B->max_nv, P.nvars)) > optin)
+    if (smem_bytes(B, B->shape, std::max(B->max_nv, P.nvars)) > optin)
       return nfail(PIAFS_ERR_UNSUPPORTED, "too many variables for the batched stage kernel's shared-memory tile");
   }
-  P.mixed = 0;
+  P.mixed = mixed(B) ? 1 : 0;
   const int ns = d.nstages;
   const size_t planes = (size_t)P.nvars * P.ps;
   const size_t ndx = d.dxinv.size(), nim = req ? (P.chem ? (size_t)P.npg : 0) : d.imap.size();
@@ -962,8 +486,6 @@ int piafs_gpu_batch_create(int precision, unsigned long long budget, piafs_gpu_b
   *out = nullptr;
   if (precision != PIAFS_PRECISION_FP64 && precision != PIAFS_PRECISION_MIXED)
     return nfail(PIAFS_ERR_ARGUMENT, "precision must be PIAFS_PRECISION_FP64 or PIAFS_PRECISION_MIXED");
-  if (precision == PIAFS_PRECISION_MIXED)
-    return nfail(PIAFS_ERR_UNSUPPORTED, "the batched path runs FP64 members in this build");
   auto* B = new piafs_gpu_batch();
   B->precision = precision;
   B->budget = budget;
@@ -1179,7 +701,7 @@ int piafs_gpu_batch_tune(piafs_gpu_batch* B, int force_tile_x) {
     int k = -1;
     for (int i = 0; i < kNumShapes && k < 0; i++)
       if (kShapes[i].tx == force_tile_x) k = i;
-    if (k < 0) return nfail(PIAFS_ERR_ARGUMENT, "tile_x must be 32, 16 or 64");
+    if (k < 0) return nfail(PIAFS_ERR_ARGUMENT, "tile_x must be 8, 16 or 32");
     B->shape = k;
     B->dirty = true;
     return PIAFS_OK;
@@ -1226,7 +748,7 @@ int piafs_gpu_batch_tune(piafs_gpu_batch* B, int force_tile_x) {
   if (e == cudaSuccess) e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   for (int c = 0; c < kNumShapes && e == cudaSuccess; c++) {
-    if (smem_bytes(c, B->max_nv) > optin) continue;
+    if (smem_bytes(B, c, B->max_nv) > optin) continue;
     B->shape = c;
     B->dirty = true;
     if (int r = sync_tables(B)) { e = cudaErrorUnknown; (void)r; break; }
@@ -1258,7 +780,7 @@ int piafs_gpu_batch_set_launch(piafs_gpu_batch* B, int tile_x, int tile_y, int m
     if (kShapes[i].tx == tile_x && kShapes[i].ty == tile_y && kShapes[i].minb == minb) {   // shapes are unique
       int optin = 0;
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, B->device);
-      if (smem_bytes(i, B->max_nv) > optin)
+      if (smem_bytes(B, i, B->max_nv) > optin)
         return nfail(PIAFS_ERR_UNSUPPORTED, "this tile does not fit the members' variables in shared memory");
       B->shape = i;
       B->dirty = true;

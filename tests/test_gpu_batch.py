@@ -26,6 +26,25 @@ GOLDEN_WENO = ["euler1d_weno5_roe_n1024", "euler1d_weno5_llf_yc_rk4_n128", "ns2d
 
 TOL = 1e-12
 NOISE_FLOOR = 1e-6
+MIXED_TOL = 1e-5
+# tile shapes of the stage kernel (x, y)
+SHAPES = [(16, 16), (32, 8), (16, 8), (32, 4), (8, 16), (16, 15), (32, 7), (16, 7)]
+
+
+def rel_err(got, ref):
+    """Worst relative L2 over the variables (variables without signal in
+    absolute terms against the largest variable's RMS)."""
+    rms = np.sqrt((ref * ref).mean(axis=0))
+    scale = rms.max()
+    worst = 0.0
+    for v in range(ref.shape[1]):
+        d = got[:, v] - ref[:, v]
+        if rms[v] < NOISE_FLOOR * scale:
+            err = np.sqrt((d * d).mean()) / scale
+        else:
+            err = np.sqrt((d * d).sum() / (ref[:, v] ** 2).sum())
+        worst = max(worst, err)
+    return worst
 
 
 def assert_close(got, ref, what=""):
@@ -42,8 +61,8 @@ def assert_close(got, ref, what=""):
     assert np.all(np.isfinite(got)) and worst <= TOL, f"{what}: {worst:.2e}"
 
 
-def in_batch_alone(d, steps, tile_x=0):
-    with Batch() as b:
+def in_batch_alone(d, steps, tile_x=0, precision="fp64"):
+    with Batch(precision) as b:
         if tile_x:
             b.tune(tile_x)
         i = b.add(d, steps)
@@ -181,7 +200,7 @@ def test_autotuner_restores_state_and_picks_a_config(tmp_path):
         for i, u in zip(ids, before):
             assert np.array_equal(b.solution(i), u)
         info = b.info
-        assert info["tile_x"] * info["tile_y"] == 256 and info["min_ctas_per_sm"] in (1, 2)
+        assert (info["tile_x"], info["tile_y"]) in SHAPES and info["min_ctas_per_sm"] in (1, 2)
         b.step(200)
         for (d, n), i in zip(mix, ids):
             assert_close(b.solution(i), alone(d, n), d)
@@ -220,3 +239,63 @@ def test_persistent_ctas_walking_many_tiles(tmp_path, monkeypatch):
     for d, a, b in zip(decks, full, one):
         assert np.array_equal(a, b), d
         assert_close(a, alone(d, 3), d)
+
+
+def test_mixed_precision_members_track_fp64(tmp_path):
+    """Mixed-precision members (FP32 weights, reconstruction, upwind fluxes,
+    viscous stencils and chemistry on FP64 state and RK accumulation) stay
+    within MIXED_TOL relative L2 of the FP64 single runs, and a member's
+    result is bit for bit the same alone and in the mix."""
+    mix = make_mix(str(tmp_path))
+    with Batch("mixed") as b:
+        ids = [b.add(d, n) for d, n in mix]
+        b.step(max(n for _, n in mix))
+        assert sorted(b.poll()) == sorted(ids)
+        for (d, n), i in zip(mix, ids):
+            got = b.solution(i)
+            assert np.all(np.isfinite(got)), d
+            err = rel_err(got, alone(d, n))
+            print(f"{os.path.basename(d)}: mixed batch vs FP64 rel L2 {err:.2e}")
+            assert err <= MIXED_TOL, (d, err)
+            assert np.array_equal(got, in_batch_alone(d, n, precision="mixed")), d
+
+
+@pytest.mark.parametrize("tile", [(16, 15, 1), (16, 7, 2), (32, 7, 1)])
+def test_balanced_tiles_both_precisions(tmp_path, tile):
+    """The 15- and 7-row tiles (at most one interface per thread) in FP64 and
+    mixed precision, on members whose sides are not multiples of the tile."""
+    mix = make_mix(str(tmp_path))[:4]
+    for prec in ("fp64", "mixed"):
+        with Batch(prec) as b:
+            b.set_launch(*tile)
+            ids = [b.add(d, n) for d, n in mix]
+            b.step(max(n for _, n in mix))
+            assert (b.info["tile_x"], b.info["tile_y"]) == tile[:2]
+            for (d, n), i in zip(mix, ids):
+                got = b.solution(i)
+                if prec == "fp64":
+                    assert_close(got, alone(d, n), d)
+                else:
+                    assert rel_err(got, alone(d, n)) <= MIXED_TOL, d
+
+
+def test_mixed_persistent_ctas_walking_many_tiles(tmp_path, monkeypatch):
+    """Mixed precision with one persistent CTA walking all tiles gives the
+    bits of the full grid of CTAs."""
+    decks = []
+    for k, n in enumerate([117, 75]):
+        d = os.path.join(str(tmp_path), f"p{k}")
+        cases.ns2d_photochem_beam(d, N=n, n_iter=3, scheme="weno5", dt=8e-5, op_file_format="none", seed=k)
+        decks.append(d)
+
+    def run():
+        with Batch("mixed") as b:
+            ids = [b.add(d, 3) for d in decks]
+            b.step(3)
+            return [b.solution(i) for i in ids]
+
+    full = run()
+    monkeypatch.setenv("PIAFS_GPU_BATCH_GRID", "1")
+    one = run()
+    for d, a, c in zip(decks, full, one):
+        assert np.array_equal(a, c), d
