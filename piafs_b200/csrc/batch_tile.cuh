@@ -91,7 +91,22 @@ __device__ __forceinline__ void load_point(const BMember& M, const double* S, in
     return;
   }
   const long long p = pidx(P, i, j);
-  for (int v = 0; v < nv; v++) out[v * ostride] = S[v * P.ps + p];
+  // six loads in flight before their stores (the stores could alias S as far
+  // as the compiler knows, which would serialise the loads)
+  const long long ps = P.ps;
+  for (int v0 = 0; v0 < nv; v0 += 6) {
+    const double* q = S + v0 * ps + p;
+    double* o = out + v0 * ostride;
+    const int r = nv - v0;
+    const double a0 = q[0], a1 = r > 1 ? q[ps] : 0.0, a2 = r > 2 ? q[2 * ps] : 0.0;
+    const double a3 = r > 3 ? q[3 * ps] : 0.0, a4 = r > 4 ? q[4 * ps] : 0.0, a5 = r > 5 ? q[5 * ps] : 0.0;
+    o[0] = a0;
+    if (r > 1) o[ostride] = a1;
+    if (r > 2) o[2 * ostride] = a2;
+    if (r > 3) o[3 * ostride] = a3;
+    if (r > 4) o[4 * ostride] = a4;
+    if (r > 5) o[5 * ostride] = a5;
+  }
   if (!edge) return;
   for (int zi = M.nzones - 1; zi >= 0; zi--) {
     const Zone& z = M.zones[zi];
@@ -210,12 +225,13 @@ __device__ __forceinline__ void rk_point(const BMember& M, const BState& Sd, int
 //            item = (interface, var)
 //   viscous  Q, viscous face fluxes (k_visc_source on the tile)
 //   point    stage derivative, chemistry, Runge-Kutta combination
-// Interfaces are numbered x first (f < NXI: row jj, position ii) then y.
+// Interfaces are numbered x first (f < NXI: row jj, position ii) then y
+// (row jj, column ii), x fastest in both.
 // Shared memory (bytes, regions 16-byte aligned): sU [nv][HY][HX] (FP64);
-// interface fluxes fx [nv][NXI] and fy [nv][NYI] (T); a work region, reused
-// by the viscous phase: cell data [5][NCX] + [5][NCY] (FP64), WENO values
-// [4][4][NI] (T), passive speed (T) and scheme (int) [NI] each.  T is FP64, or
-// FP32 under MX.
+// interface fluxes fx [nv][TY][TX+1] and fy [nv][TY+1][TX] (T); a work
+// region, reused by the viscous phase: cell data [5][TY][HX] + [5][HY][TX]
+// (FP64), WENO values [4][4][NI] (T), passive speed (T) and scheme (int) [NI]
+// each.  T is FP64, or FP32 under MX.
 template <int TX, int TY, bool MX>
 struct Tile2D {
   typedef typename std::conditional<MX, float, double>::type T;
@@ -252,11 +268,25 @@ struct Tile1D {
 };
 
 #ifdef __CUDACC__
+// photochemical source of one layer at a point whose state is u[v * us]
+// (shared memory), added to the point's stage derivative kv[] in registers
+// (the arithmetic and the order of chem_source_point for nz = 1)
+template <typename T>
+__device__ __forceinline__ void chem_source_kv(const DevParams& P, const double* u, int us, double hnu_factor,
+                                               double imap_p, double* kv) {
+  T src[5], Q;
+  chem_layer<T>(P, chem_hnu0<T>(P, hnu_factor, imap_p), (T)u[4 * us], (T)u[5 * us], (T)u[6 * us], (T)u[7 * us],
+                (T)u[8 * us], (T)u[9 * us], (T)u[10 * us], src, Q);
+#pragma unroll
+  for (int k = 0; k < 5; k++) kv[5 + k] += (double)src[k];
+  kv[3] += (double)Q;
+}
+
 template <int TX, int TY, int UPW, int BT, bool MX>
 __device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s, int tx, int ty, char* smem) {
   typedef Tile2D<TX, TY, MX> L;
   typedef typename L::T T;
-  constexpr int HX = L::HX, HY = L::HY, NXI = L::NXI, NI = L::NI, NCX = L::NCX, NCY = L::NCY;
+  constexpr int HX = L::HX, HY = L::HY, NXI = L::NXI, NYI = L::NYI, NI = L::NI, NCX = L::NCX, NCY = L::NCY;
   const DevParams& P = M.P;
   const int nv = P.nvars, N0 = P.N0, N1 = P.N1;
   const int i0 = tx * TX, j0 = ty * TY;
@@ -264,22 +294,22 @@ __device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s
   constexpr int vs = HX * HY;
   double* sU = (double*)smem;
   T* fx = (T*)(smem + L::su_bytes(nv));                  // [m][jj * (TX+1) + ii]
-  T* fy = (T*)((char*)fx + L::fx_bytes(nv));             // [m][ii * (TY+1) + jj]
+  T* fy = (T*)((char*)fx + L::fx_bytes(nv));             // [m][jj * TX + ii]
   char* wk = (char*)fy + L::fy_bytes(nv);                // work region
-  double* cx = (double*)wk;                              // [5][NCX]: 4 flow fluxes + vn, x cells
-  double* cy = cx + 5 * NCX;                             // [5][NCY]
+  double* cx = (double*)wk;                              // [5][NCX]: 4 flow fluxes + vn, x cells [jj][a]
+  double* cy = cx + 5 * NCX;                             // [5][NCY]: y cells [b][ii]
   T* rec = (T*)(wk + L::CELL);                           // [k][m][NI]
   T* spa = (T*)(wk + L::CELL + L::REC);                  // [NI]
   int* spm = (int*)(wk + L::CELL + L::REC + L::SPA);     // [NI]
   const int tid = threadIdx.x;
   for (int e = tid; e < vs; e += BT) load_point(M, S, i0 - H + e % HX, j0 - H + e / HX, sU + e, vs);
   __syncthreads();
-  // cell data: x cells (row jj, column a): c = (jj+H)*HX + a; y cells
-  // (column ii, row b): c = b*HX + ii + H
+  // cell data: x cells (row jj, column a): c = (jj+H)*HX + a, index jj*HX + a;
+  // y cells (row b, column ii): c = b*HX + ii + H, index b*TX + ii
   for (int e = tid; e < NCX + NCY; e += BT) {
     const bool xd = e < NCX;
     const int g = xd ? e : e - NCX;
-    const int c = xd ? (g / HX + H) * HX + g % HX : (g % HY) * HX + g / HY + H;
+    const int c = xd ? (g / HX + H) * HX + g % HX : (g / TX) * HX + g % TX + H;
     double f[4], vn;
     ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, xd ? 0 : 1, f, vn);
     double* o = xd ? cx + g : cy + g;
@@ -290,48 +320,49 @@ __device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s
   }
   __syncthreads();
   // geometry of interface f: its cell i (right of the interface) in sU
-  // (base, stride ust along the line), in the cell data (cd, plane cst), the
-  // line's reference cell (the tile's first interior cell of the row or
-  // column: cref in sU, cdr in the cell data) and whether it is inside the
-  // member
-  auto geo = [&](int f, int& base, int& ust, const double*& cd, int& cst, int& dir, int& cref,
+  // (base, stride ust along the line), in the cell data (cd, plane cst, stride
+  // cls along the line), the line's reference cell (the tile's first interior
+  // cell of the row or column: cref in sU, cdr in the cell data) and whether it
+  // is inside the member.  Consecutive interfaces of either direction are
+  // consecutive in x, so a warp's shared-memory accesses are unit-stride.
+  auto geo = [&](int f, int& base, int& ust, const double*& cd, int& cst, int& cls, int& dir, int& cref,
                  const double*& cdr) -> bool {
     if (f < NXI) {
       const int ii = f % (TX + 1), jj = f / (TX + 1);
-      base = (jj + H) * HX + ii + H; ust = 1; cd = cx + jj * HX + ii + H; cst = NCX; dir = 0;
+      base = (jj + H) * HX + ii + H; ust = 1; cd = cx + jj * HX + ii + H; cst = NCX; cls = 1; dir = 0;
       cref = (jj + H) * HX + H; cdr = cx + jj * HX + H;
       return i0 + ii <= N0 && j0 + jj < N1;
     }
-    const int g = f - NXI, jj = g % (TY + 1), ii = g / (TY + 1);
-    base = (jj + H) * HX + ii + H; ust = HX; cd = cy + ii * HY + jj + H; cst = NCY; dir = 1;
-    cref = H * HX + ii + H; cdr = cy + ii * HY + H;
+    const int g = f - NXI, ii = g % TX, jj = g / TX;
+    base = (jj + H) * HX + ii + H; ust = HX; cd = cy + (jj + H) * TX + ii; cst = NCY; cls = TX; dir = 1;
+    cref = H * HX + ii + H; cdr = cy + H * TX + ii;
     return j0 + jj <= N1 && i0 + ii < N0;
   };
   for (int e = tid; e < 4 * NI; e += BT) {
     const int m = e / NI, f = e % NI;
-    int base, ust, cst, dir, cref;
+    int base, ust, cst, cls, dir, cref;
     const double *cd, *cdr;
-    if (!geo(f, base, ust, cd, cst, dir, cref, cdr)) continue;
+    if (!geo(f, base, ust, cd, cst, cls, dir, cref, cdr)) continue;
     const double ur = MX ? sU[m * vs + cref] : 0.0, fr = MX ? cdr[m * cst] : 0.0;
-    iface_weno<MX>(P, sU + m * vs + base, ust, cd + m * cst, 1, ur, fr, rec[(0 * 4 + m) * NI + f],
+    iface_weno<MX>(P, sU + m * vs + base, ust, cd + m * cst, cls, ur, fr, rec[(0 * 4 + m) * NI + f],
                    rec[(1 * 4 + m) * NI + f], rec[(2 * 4 + m) * NI + f], rec[(3 * 4 + m) * NI + f]);
   }
   __syncthreads();
   for (int f = tid; f < NI; f += BT) {
-    int base, ust, cst, dir, cref;
+    int base, ust, cst, cls, dir, cref;
     const double *cd, *cdr;
-    if (!geo(f, base, ust, cd, cst, dir, cref, cdr)) continue;
+    if (!geo(f, base, ust, cd, cst, cls, dir, cref, cdr)) continue;
     T* so = f < NXI ? fx + f : fy + (f - NXI);
     iface_upwind_flow<NS2D, UPW, MX>(P, rec + f, 4 * NI, NI, sU + base - ust, sU + base, sU + cref, vs, dir, so,
-                                     f < NXI ? NXI : L::NYI, spa + f, spm + f);
+                                     f < NXI ? NXI : NYI, spa + f, spm + f);
   }
   __syncthreads();
   const int np = nv - 4;
   for (int e = tid; e < np * NI; e += BT) {
     const int m = 4 + e / NI, f = e % NI;
-    int base, ust, cst, dir, cref;
+    int base, ust, cst, cls, dir, cref;
     const double *cd, *cdr;
-    if (!geo(f, base, ust, cd, cst, dir, cref, cdr)) continue;
+    if (!geo(f, base, ust, cd, cst, cls, dir, cref, cdr)) continue;
     const double* u = sU + m * vs + base;
     const double* vn = cd + 4 * cst;
     T a[6], b[6], l, r, fl, fr;
@@ -341,16 +372,16 @@ __device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s
       for (int q = 0; q < 6; q++) {
         const double uu = u[(q - 3) * ust];
         a[q] = (T)(uu - ur);
-        b[q] = (T)(__dmul_rn(vn[q - 3], uu) - frf);
+        b[q] = (T)(__dmul_rn(vn[(q - 3) * cls], uu) - frf);
       }
     } else {
 #pragma unroll
-      for (int q = 0; q < 6; q++) { a[q] = u[(q - 3) * ust]; b[q] = __dmul_rn(vn[q - 3], a[q]); }
+      for (int q = 0; q < 6; q++) { a[q] = u[(q - 3) * ust]; b[q] = __dmul_rn(vn[(q - 3) * cls], a[q]); }
     }
     weno5_iface(P, a, b, l, r, fl, fr);
     const T h = upwind_species(spm[f], spa[f], l, r, fl, fr);
     if (f < NXI) fx[m * NXI + f] = h;
-    else fy[m * L::NYI + f - NXI] = h;
+    else fy[m * NYI + f - NXI] = h;
   }
   __syncthreads();
   // viscous fluxes (k_visc_source on this tile), in the work region; MX:
@@ -427,39 +458,68 @@ __device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s
   const long long ps = P.ps;
   double* ks = M.k[s];
   const double dxi = M.dxinv[P.ghosts + i], dyi = M.dxinv[P.W0 + P.ghosts + j];
-  constexpr int LX = TX + 1, LY = TY + 1;
-  for (int m = 0; m < nv; m++) {
+  constexpr int LX = TX + 1;
+  // the stage derivative of one variable: hyperbolic (and viscous) part
+  auto hyp_visc = [&](int m) -> double {
     const T* ax = fx + m * NXI + pj * LX + pi;
-    const T* ay = fy + m * L::NYI + pi * LY + pj;
+    const T* ay = fy + m * NYI + pj * TX + pi;
     double h;
     if (MX) {
-      const T hx = (T)dxi * (ax[1] - ax[0]), hy = (T)dyi * (ay[1] - ay[0]);
+      const T hx = (T)dxi * (ax[1] - ax[0]), hy = (T)dyi * (ay[TX] - ay[0]);
       h = (double)(hx + hy);
     } else {
       const double hx = dxi * (ax[1] - ax[0]);
-      const double hy = dyi * (ay[1] - ay[0]);
+      const double hy = dyi * (ay[TX] - ay[0]);
       h = hx + hy;
     }
-    ks[m * ps + p] = -h;
-  }
-  if (visc) {
-#pragma unroll
-    for (int m = 0; m < 3; m++) {
+    double k = -h;
+    if (visc && m >= 1 && m <= 3) {
+      const int n = m - 1;
       if (MX) {
-        const T par = (T)dxi * (sVx[m * TY * FX + pj * FX + pi + 1] - sVx[m * TY * FX + pj * FX + pi]) +
-                      (T)dyi * (sVy[m * FY * TX + (pj + 1) * TX + pi] - sVy[m * FY * TX + pj * TX + pi]);
-        ks[(m + 1) * ps + p] += (double)par;
+        const T par = (T)dxi * (sVx[n * TY * FX + pj * FX + pi + 1] - sVx[n * TY * FX + pj * FX + pi]) +
+                      (T)dyi * (sVy[n * FY * TX + (pj + 1) * TX + pi] - sVy[n * FY * TX + pj * TX + pi]);
+        k += (double)par;
       } else {
-        const double par = dxi * (sVx[m * TY * FX + pj * FX + pi + 1] - sVx[m * TY * FX + pj * FX + pi]) +
-                           dyi * (sVy[m * FY * TX + (pj + 1) * TX + pi] - sVy[m * FY * TX + pj * TX + pi]);
-        ks[(m + 1) * ps + p] += par;
+        const double par = dxi * (sVx[n * TY * FX + pj * FX + pi + 1] - sVx[n * TY * FX + pj * FX + pi]) +
+                           dyi * (sVy[n * FY * TX + (pj + 1) * TX + pi] - sVy[n * FY * TX + pj * TX + pi]);
+        k += par;
       }
     }
-  }
-  if (P.chem) {
-    const double t = Sd.t + M.c[s] * P.dt;
-    chem_source_point<T>(P, S, p, pulse_factor(P, t), M.imap[p], ks);
-  }
+    return k;
+  };
+  const double t = Sd.t + M.c[s] * P.dt;
+  // Every variable in registers (the common counts: NS2D with one chemistry
+  // layer, 11, and without chemistry, 4): the earlier stages' part of the
+  // Runge-Kutta combination first, all of its loads in flight together, then
+  // this stage's derivative, then the stores.
+  auto fast = [&](auto nvc) {
+    constexpr int NV = decltype(nvc)::value;
+    const int c = (pj + H) * HX + pi + H;                // the point's cell in sU
+    const bool last = s == M.nstages - 1;
+    double xa[NV], kv[NV];
+#pragma unroll
+    for (int m = 0; m < NV; m++) xa[m] = s == 0 ? sU[m * vs + c] : Sd.u[m * ps + p];
+    for (int q = 0; q < s; q++) {
+      const double cq = last ? M.b[q] : M.a[(s + 1) * MAX_STAGES + q];
+      const double* kq = M.k[q] + p;
+      double tq[NV];
+#pragma unroll
+      for (int m = 0; m < NV; m++) tq[m] = kq[m * ps];
+#pragma unroll
+      for (int m = 0; m < NV; m++) xa[m] += cq * tq[m];
+    }
+#pragma unroll
+    for (int m = 0; m < NV; m++) kv[m] = hyp_visc(m);
+    if (NV == 11) chem_source_kv<T>(P, sU + c, vs, pulse_factor(P, t), M.imap[p], kv);
+    const double cs = last ? M.b[s] : M.a[(s + 1) * MAX_STAGES + s];
+    double* dst = last ? (M.nstages == 1 ? Sd.X : Sd.u) : (s % 2 == 0 ? M.X : M.Y);
+#pragma unroll
+    for (int m = 0; m < NV; m++) { ks[m * ps + p] = kv[m]; dst[m * ps + p] = xa[m] + cs * kv[m]; }
+  };
+  if (nv == 11 && P.chem && P.nz == 1) { fast(std::integral_constant<int, 11>()); return; }
+  if (nv == 4 && !P.chem) { fast(std::integral_constant<int, 4>()); return; }
+  for (int m = 0; m < nv; m++) ks[m * ps + p] = hyp_visc(m);
+  if (P.chem) chem_source_point<T>(P, S, p, pulse_factor(P, t), M.imap[p], ks);
   rk_point(M, Sd, s, p, nv);
 }
 
