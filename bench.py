@@ -61,6 +61,8 @@ def parse():
                     choices=["ns2d_photochem", "euler1d", "ensemble", "serving"])
     ap.add_argument("--requests", type=int, default=1000, help="serving requests (the stream's first n)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0)
+    ap.add_argument("--max-resident-points", type=float, default=4e6,
+                    help="serving: grid points resident at once (0: HBM budget only)")
     ap.add_argument("--members", type=int, default=256, help="ensemble members")
     ap.add_argument("--member-steps", type=int, default=100, help="steps per ensemble member")
     ap.add_argument("--n", type=int, default=None, help="grid size (default 2048 / 1024)")
@@ -320,7 +322,9 @@ def serving_bench(a):
     serve_trace(rq[:2], [0.0, 0.0], precision=a.precision)
     budget = int(a.hbm_budget_gb * 1e9)
     t0 = time.perf_counter()
-    res = serve_trace(rq, list(arr), precision=a.precision, hbm_budget_bytes=budget, steps_per_round=4)
+    maxpts = int(a.max_resident_points)
+    res = serve_trace(rq, list(arr), precision=a.precision, hbm_budget_bytes=budget, steps_per_round=4,
+                      max_resident_points=maxpts)
     wall = time.perf_counter() - t0
     lat = np.array([r["finished_s"] - r["arrival_s"] for r in res])
     wait = np.array([r["admitted_s"] - r["arrival_s"] for r in res])
@@ -332,6 +336,7 @@ def serving_bench(a):
             "config": {"workload": f"serving_{len(res)}req_poisson2000_70pct1d_30pct2d_50to500steps",
                        "requests": len(res), "rate_per_s": 2000.0, "precision": a.precision,
                        "hbm_budget_gb": a.hbm_budget_gb, "steps_per_round": 4,
+                       "max_resident_points": maxpts, "admission": "FIFO",
                        "pt_stage_updates": units},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},

@@ -266,14 +266,19 @@ typedef struct {
 } piafs_gpu_serve_result;
 /* Replay a request trace in real time with continuous batching: request k
  * arrives at arrival_s[k] (seconds from the start, nondecreasing); arrived
- * requests are admitted in arrival order while the HBM budget holds them
- * (a request that does not fit waits, and so do the ones behind it); between
- * admission rounds all resident requests advance steps_per_round steps
- * together; a finished request's checksum is taken and its memory released
- * at once.  Returns when every request has finished; latency of request k
- * is out[k].finished_s - out[k].arrival_s. */
+ * requests are admitted in arrival order while the HBM budget holds them and
+ * the resident grid points stay within max_resident_points (0: no bound; a
+ * request is always admitted when nothing is resident); a request that does
+ * not fit waits, and so do the ones behind it.  Between admission rounds all
+ * resident requests advance steps_per_round steps together; a finished
+ * request's checksum is taken and its memory released at once.  The points
+ * bound trades concurrency for latency: every resident request shares the
+ * device, so admitting fewer at a time lets each finish sooner once started.
+ * Returns when every request has finished; latency of request k is
+ * out[k].finished_s - out[k].arrival_s. */
 int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s, int n, int precision,
-                          unsigned long long hbm_budget_bytes, int steps_per_round, piafs_gpu_serve_result* out);
+                          unsigned long long hbm_budget_bytes, unsigned long long max_resident_points,
+                          int steps_per_round, piafs_gpu_serve_result* out);
 
 /* ---- diagnostics ----
  * No counterpart in the reference.  y[i] = 1/x[i] (device arrays) computed

@@ -83,7 +83,7 @@ SIGNATURES = {
     "piafs_gpu_batch_set_launch": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
     "piafs_gpu_batch_add_request": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "piafs_gpu_batch_checksum": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
-    "piafs_gpu_serve_trace": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_ulonglong, C.c_int, _vp]),
+    "piafs_gpu_serve_trace": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, _vp]),
 }
 
 
@@ -324,17 +324,20 @@ class ServeResult(C.Structure):
                 ("steps", C.c_int), ("checksum", C.c_double)]
 
 
-def serve_trace(requests, arrivals, precision: str = "fp64", hbm_budget_bytes: int = 0, steps_per_round: int = 4):
+def serve_trace(requests, arrivals, precision: str = "fp64", hbm_budget_bytes: int = 0, steps_per_round: int = 4,
+                max_resident_points: int = 0):
     """Replay a request trace in real time through the continuous-batching
     serving loop (piafs_gpu_serve_trace); returns a list of dicts per request
-    (arrival, admission, finish in seconds from the start, steps, checksum)."""
+    (arrival, admission, finish in seconds from the start, steps, checksum).
+    max_resident_points bounds the grid points resident at once (0: only the
+    HBM budget bounds admission)."""
     L = load_library()
     n = len(requests)
     reqs = (Request * n)(*requests)
     arr = (C.c_double * n)(*[float(x) for x in arrivals])
     out = (ServeResult * n)()
-    code = L.piafs_gpu_serve_trace(reqs, arr, n, PRECISION[precision], int(hbm_budget_bytes), int(steps_per_round),
-                                   out)
+    code = L.piafs_gpu_serve_trace(reqs, arr, n, PRECISION[precision], int(hbm_budget_bytes),
+                                   int(max_resident_points), int(steps_per_round), out)
     if code != PIAFS_OK:
         raise PiafsError(code, L.piafs_gpu_last_error().decode())
     return [{name: getattr(r, name) for name, _ in ServeResult._fields_} for r in out]

@@ -822,7 +822,8 @@ int piafs_gpu_batch_checksum(piafs_gpu_batch* B, int id, double* sum) {
 }
 
 int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s, int n, int precision,
-                          unsigned long long budget, int steps_per_round, piafs_gpu_serve_result* out) {
+                          unsigned long long budget, unsigned long long max_points, int steps_per_round,
+                          piafs_gpu_serve_result* out) {
   if (n < 0 || (n > 0 && (!reqs || !arrival_s || !out)) || steps_per_round < 1)
     return nfail(PIAFS_ERR_ARGUMENT, "bad argument");
   for (int k = 1; k < n; k++)
@@ -831,6 +832,11 @@ int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s
   if (int r = piafs_gpu_batch_create(precision, budget, &B)) return r;
   std::vector<int> slot_req;     // member id -> request index
   int next = 0, finished = 0, rc = PIAFS_OK;
+  unsigned long long resident = 0;   // grid points of the resident requests
+  auto points = [&](int k) -> unsigned long long {
+    const unsigned long long n1 = (unsigned long long)std::max(reqs[k].n, 0);
+    return reqs[k].kind == PIAFS_REQUEST_NS2D_BEAM ? n1 * n1 : n1;
+  };
   const double t0 = now_s();
   for (int k = 0; k < n; k++) {
     out[k].arrival_s = arrival_s[k];
@@ -843,6 +849,7 @@ int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s
     // admission: arrived requests in order, while the budget holds them
     double t = now_s() - t0;
     while (next < n && arrival_s[next] <= t) {
+      if (max_points && resident > 0 && resident + points(next) > max_points) break;
       int id = -1;
       const int r = piafs_gpu_batch_add_request(B, reqs + next, &id);
       if (r == PIAFS_ERR_MEMORY) {
@@ -855,6 +862,7 @@ int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s
       if (r) { rc = r; break; }
       if ((int)slot_req.size() <= id) slot_req.resize(id + 1, -1);
       slot_req[id] = next;
+      resident += points(next);
       out[next].admitted_s = now_s() - t0;
       next++;
       t = now_s() - t0;
@@ -880,6 +888,7 @@ int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s
       rc = piafs_gpu_batch_checksum(B, id, &cs);
       if (!rc) rc = piafs_gpu_batch_member(B, id, &tm, &it, &dn);
       if (!rc) rc = piafs_gpu_batch_remove(B, id);
+      resident -= points(k);
       out[k].checksum = cs;
       out[k].steps = it;
       out[k].finished_s = now_s() - t0;

@@ -88,3 +88,22 @@ def test_serving_under_a_small_budget():
     # a request larger than the whole budget is refused, not waited on forever
     with pytest.raises(PiafsError):
         serve_trace(reqs[:1], arr[:1], hbm_budget_bytes=16)
+
+
+def test_resident_points_bound():
+    """With the resident grid points bounded, requests are admitted in arrival
+    order as earlier ones finish (never more points resident than the bound,
+    except one request alone), and each result is still its result alone."""
+    reqs, arr = small_trace(30)
+    pts = [q.n if q.kind == 1 else q.n * q.n for q in reqs]
+    bound = 2 * max(pts)
+    res = serve_trace(reqs, arr, steps_per_round=2, max_resident_points=bound)
+    adm = [r["admitted_s"] for r in res]
+    assert adm == sorted(adm)
+    for k, r in enumerate(res):
+        # requests resident at k's admission: admitted no later, finished after
+        live = [j for j in range(len(res)) if res[j]["admitted_s"] <= r["admitted_s"] < res[j]["finished_s"]]
+        assert sum(pts[j] for j in live) <= max(bound, pts[k])
+    for q, r in zip(reqs, res):
+        _, cs = one(q)
+        assert r["checksum"] == cs
