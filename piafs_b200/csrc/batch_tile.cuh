@@ -18,10 +18,10 @@
 // the cell fluxes and the Runge-Kutta combination stay FP64; the WENO
 // weights and values, the upwind fluxes (deviation form), the viscous
 // stencils and the chemistry source are FP32.  Values enter FP32 relative to
-// a reference of their grid line inside the tile (the tile's first interior
-// cell of that row or column, subtracted in FP64), so the O(1) background
-// never goes through FP32 rounding; the divergence differences the interface
-// fluxes along the same line, where the reference cancels.
+// a reference of the tile (the state and fluxes at its first interior cell,
+// subtracted in FP64; 1D: the tile's first cell), so the O(1) background never
+// goes through FP32 rounding; the divergence differences the interface fluxes
+// along grid lines of the tile, where the reference cancels.
 #pragma once
 #include <type_traits>
 
@@ -155,8 +155,8 @@ __device__ __forceinline__ void iface_weno(const DevParams& P, const double* u, 
 // from their WENO values rec[k * ks + m * ms] (k: uL, uR, fL, fR) and the cell
 // states left / right (ucl, ucr at stride vs); flux to so[m * sstride],
 // passive-variable scheme data to *spa / *spm.  MX: rec holds FP32 values
-// relative to the line's reference state uref (stride vs), and the flux comes
-// back relative to the line's reference flux (upwind_flow_dev).
+// relative to the reference state uref (stride vs), and the flux comes back
+// relative to the reference flux (upwind_flow_dev).
 template <int MODEL, int UPW, bool MX>
 __device__ __noinline__ void iface_upwind_flow(const DevParams& P,
                                                const typename std::conditional<MX, float, double>::type* rec, int ks,
@@ -229,9 +229,16 @@ __device__ __forceinline__ void rk_point(const BMember& M, const BState& Sd, int
 // (row jj, column ii), x fastest in both.
 // Shared memory (bytes, regions 16-byte aligned): sU [nv][HY][HX] (FP64);
 // interface fluxes fx [nv][TY][TX+1] and fy [nv][TY+1][TX] (T); a work
-// region, reused by the viscous phase: cell data [5][TY][HX] + [5][HY][TX]
-// (FP64), WENO values [4][4][NI] (T), passive speed (T) and scheme (int) [NI]
-// each.  T is FP64, or FP32 under MX.
+// region, reused by the viscous phase: cell data, WENO values [4][4][NI] (T),
+// passive speed (T) and scheme (int) [NI] each.  T is FP64, or FP32 under MX.
+// FP64 cell data: 4 flow fluxes and vn, [5][TY][HX] for x cells and
+// [5][HY][TX] for y cells.  MX: the state and every cell flux (flow fluxes and
+// the passive fluxes vn u_m) enter FP32 once per cell, relative to the tile's
+// reference values (state, x and y fluxes at the tile's first interior cell,
+// subtracted in FP64): state deviations [nv][HY][HX] and flux deviations
+// [nv][TY][HX] + [nv][HY][TX].  A per-tile constant is constant along every
+// grid line of the tile, so reconstruction and upwinding are unchanged by it
+// and the divergence cancels it.
 template <int TX, int TY, bool MX>
 struct Tile2D {
   typedef typename std::conditional<MX, float, double>::type T;
@@ -240,16 +247,24 @@ struct Tile2D {
   static constexpr int NCX = TY * HX, NCY = TX * HY;            // stencil cells per direction
   static constexpr long long VISC =
       al16((3LL * (TY + 2) * (TX + 2) + 3LL * TY * (TX + 1) + 3LL * (TY + 1) * TX) * (long long)sizeof(T));
-  static constexpr long long CELL = al16(5LL * (NCX + NCY) * 8);
   static constexpr long long REC = al16(16LL * NI * (long long)sizeof(T));
   static constexpr long long SPA = al16((long long)NI * (long long)sizeof(T));
-  static constexpr long long WORK0 = CELL + REC + SPA + al16(4LL * NI);
-  static constexpr long long WORK = WORK0 > VISC ? WORK0 : VISC;
+  // work region: [MX: FP32 state deviations] cell data, WENO values, passive
+  // speed and scheme
+  __host__ __device__ static constexpr long long suf_bytes(int nv) { return MX ? al16(4LL * nv * HX * HY) : 0; }
+  __host__ __device__ static constexpr long long cell_bytes(int nv) {
+    return MX ? al16(4LL * nv * (NCX + NCY)) : al16(5LL * (NCX + NCY) * 8);
+  }
+  __host__ __device__ static constexpr long long work(int nv) {
+    return suf_bytes(nv) + cell_bytes(nv) + REC + SPA + al16(4LL * NI) > VISC
+               ? suf_bytes(nv) + cell_bytes(nv) + REC + SPA + al16(4LL * NI)
+               : VISC;
+  }
   __host__ __device__ static constexpr long long su_bytes(int nv) { return al16((long long)nv * HX * HY * 8); }
   __host__ __device__ static constexpr long long fx_bytes(int nv) { return al16((long long)nv * NXI * sizeof(T)); }
   __host__ __device__ static constexpr long long fy_bytes(int nv) { return al16((long long)nv * NYI * sizeof(T)); }
   __host__ __device__ static constexpr long long smem(int nv) {
-    return su_bytes(nv) + fx_bytes(nv) + fy_bytes(nv) + WORK;
+    return su_bytes(nv) + fx_bytes(nv) + fy_bytes(nv) + work(nv);
   }
 };
 
@@ -296,92 +311,147 @@ __device__ __forceinline__ void tile2d(const BMember& M, const BState& Sd, int s
   T* fx = (T*)(smem + L::su_bytes(nv));                  // [m][jj * (TX+1) + ii]
   T* fy = (T*)((char*)fx + L::fx_bytes(nv));             // [m][jj * TX + ii]
   char* wk = (char*)fy + L::fy_bytes(nv);                // work region
-  double* cx = (double*)wk;                              // [5][NCX]: 4 flow fluxes + vn, x cells [jj][a]
-  double* cy = cx + 5 * NCX;                             // [5][NCY]: y cells [b][ii]
-  T* rec = (T*)(wk + L::CELL);                           // [k][m][NI]
-  T* spa = (T*)(wk + L::CELL + L::REC);                  // [NI]
-  int* spm = (int*)(wk + L::CELL + L::REC + L::SPA);     // [NI]
+  float* sUf = (float*)wk;                               // MX: [nv][HY][HX] state deviations
+  char* cw = wk + L::suf_bytes(nv);
+  double* cx = (double*)cw;                              // FP64: [5][NCX]: 4 flow fluxes + vn, x cells [jj][a]
+  double* cy = cx + 5 * NCX;                             // FP64: [5][NCY]: y cells [b][ii]
+  float* cxf = (float*)cw;                               // MX: [nv][NCX] flux deviations, x cells
+  float* cyf = cxf + nv * NCX;                           // MX: [nv][NCY], y cells
+  T* rec = (T*)(cw + L::cell_bytes(nv));                 // [k][m][NI]
+  T* spa = (T*)((char*)rec + L::REC);                    // [NI]
+  int* spm = (int*)((char*)spa + L::SPA);                // [NI]
   const int tid = threadIdx.x;
+  constexpr int c0 = H * HX + H;                         // the tile's first interior cell
   for (int e = tid; e < vs; e += BT) load_point(M, S, i0 - H + e % HX, j0 - H + e / HX, sU + e, vs);
   __syncthreads();
   // cell data: x cells (row jj, column a): c = (jj+H)*HX + a, index jj*HX + a;
   // y cells (row b, column ii): c = b*HX + ii + H, index b*TX + ii
-  for (int e = tid; e < NCX + NCY; e += BT) {
-    const bool xd = e < NCX;
-    const int g = xd ? e : e - NCX;
-    const int c = xd ? (g / HX + H) * HX + g % HX : (g / TX) * HX + g % TX + H;
-    double f[4], vn;
-    ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, xd ? 0 : 1, f, vn);
-    double* o = xd ? cx + g : cy + g;
-    const int st = xd ? NCX : NCY;
+  if constexpr (MX) {
+    double fr0[4], fr1[4], vr0, vr1;                     // reference fluxes (x, y) at c0
+    ns2d_flux(sU[c0], sU[vs + c0], sU[2 * vs + c0], sU[3 * vs + c0], P.gamma, 0, fr0, vr0);
+    ns2d_flux(sU[c0], sU[vs + c0], sU[2 * vs + c0], sU[3 * vs + c0], P.gamma, 1, fr1, vr1);
+    for (int e = tid; e < nv * vs; e += BT) sUf[e] = (float)(sU[e] - sU[(e / vs) * vs + c0]);
+    for (int e = tid; e < NCX + NCY; e += BT) {
+      const bool xd = e < NCX;
+      const int g = xd ? e : e - NCX;
+      const int c = xd ? (g / HX + H) * HX + g % HX : (g / TX) * HX + g % TX + H;
+      double f[4], vn;
+      ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, xd ? 0 : 1, f, vn);
+      float* o = xd ? cxf + g : cyf + g;
+      const int st = xd ? NCX : NCY;
+      const double* fr = xd ? fr0 : fr1;
+      const double vr = xd ? vr0 : vr1;
 #pragma unroll
-    for (int m = 0; m < 4; m++) o[m * st] = f[m];
-    o[4 * st] = vn;
+      for (int m = 0; m < 4; m++) o[m * st] = (float)(f[m] - fr[m]);
+      for (int m = 4; m < nv; m++)
+        o[m * st] = (float)(__dmul_rn(vn, sU[m * vs + c]) - __dmul_rn(vr, sU[m * vs + c0]));
+    }
+  } else {
+    for (int e = tid; e < NCX + NCY; e += BT) {
+      const bool xd = e < NCX;
+      const int g = xd ? e : e - NCX;
+      const int c = xd ? (g / HX + H) * HX + g % HX : (g / TX) * HX + g % TX + H;
+      double f[4], vn;
+      ns2d_flux(sU[c], sU[vs + c], sU[2 * vs + c], sU[3 * vs + c], P.gamma, xd ? 0 : 1, f, vn);
+      double* o = xd ? cx + g : cy + g;
+      const int st = xd ? NCX : NCY;
+#pragma unroll
+      for (int m = 0; m < 4; m++) o[m * st] = f[m];
+      o[4 * st] = vn;
+    }
   }
   __syncthreads();
   // geometry of interface f: its cell i (right of the interface) in sU
-  // (base, stride ust along the line), in the cell data (cd, plane cst, stride
-  // cls along the line), the line's reference cell (the tile's first interior
-  // cell of the row or column: cref in sU, cdr in the cell data) and whether it
-  // is inside the member.  Consecutive interfaces of either direction are
-  // consecutive in x, so a warp's shared-memory accesses are unit-stride.
-  auto geo = [&](int f, int& base, int& ust, const double*& cd, int& cst, int& cls, int& dir, int& cref,
-                 const double*& cdr) -> bool {
+  // (base, stride ust along the line), in its direction's cell data (index
+  // cdo, plane cst, stride cls along the line) and whether it is inside the
+  // member.  Consecutive interfaces of either direction are consecutive in x,
+  // so a warp's shared-memory accesses are unit-stride.
+  auto geo = [&](int f, int& base, int& ust, int& cdo, int& cst, int& cls, int& dir) -> bool {
     if (f < NXI) {
       const int ii = f % (TX + 1), jj = f / (TX + 1);
-      base = (jj + H) * HX + ii + H; ust = 1; cd = cx + jj * HX + ii + H; cst = NCX; cls = 1; dir = 0;
-      cref = (jj + H) * HX + H; cdr = cx + jj * HX + H;
+      base = (jj + H) * HX + ii + H; ust = 1; cdo = jj * HX + ii + H; cst = NCX; cls = 1; dir = 0;
       return i0 + ii <= N0 && j0 + jj < N1;
     }
     const int g = f - NXI, ii = g % TX, jj = g / TX;
-    base = (jj + H) * HX + ii + H; ust = HX; cd = cy + (jj + H) * TX + ii; cst = NCY; cls = TX; dir = 1;
-    cref = H * HX + ii + H; cdr = cy + H * TX + ii;
+    base = (jj + H) * HX + ii + H; ust = HX; cdo = (jj + H) * TX + ii; cst = NCY; cls = TX; dir = 1;
     return j0 + jj <= N1 && i0 + ii < N0;
   };
-  for (int e = tid; e < 4 * NI; e += BT) {
-    const int m = e / NI, f = e % NI;
-    int base, ust, cst, cls, dir, cref;
-    const double *cd, *cdr;
-    if (!geo(f, base, ust, cd, cst, cls, dir, cref, cdr)) continue;
-    const double ur = MX ? sU[m * vs + cref] : 0.0, fr = MX ? cdr[m * cst] : 0.0;
-    iface_weno<MX>(P, sU + m * vs + base, ust, cd + m * cst, cls, ur, fr, rec[(0 * 4 + m) * NI + f],
-                   rec[(1 * 4 + m) * NI + f], rec[(2 * 4 + m) * NI + f], rec[(3 * 4 + m) * NI + f]);
+  // a thread takes NW items at a time and finishes them together (their loads
+  // and arithmetic are independent, so their latencies overlap); items past
+  // the end or outside the member are computed on in-tile data and dropped
+  constexpr int NW = 2;
+  auto load_stencil = [&](int m, int base, int ust, int cdo, int cst, int cls, int dir, T* a, T* b) {
+    if constexpr (MX) {
+      const float* u = sUf + m * vs + base;
+      const float* fc = (dir ? cyf : cxf) + m * cst + cdo;
+#pragma unroll
+      for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * ust]; b[r] = fc[(r - 3) * cls]; }
+    } else {
+      const double* u = sU + m * vs + base;
+      if (m < 4) {
+        const double* fc = (dir ? cy : cx) + m * cst + cdo;
+#pragma unroll
+        for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * ust]; b[r] = fc[(r - 3) * cls]; }
+      } else {
+        const double* vn = (dir ? cy : cx) + 4 * cst + cdo;
+#pragma unroll
+        for (int r = 0; r < 6; r++) { a[r] = u[(r - 3) * ust]; b[r] = __dmul_rn(vn[(r - 3) * cls], a[r]); }
+      }
+    }
+  };
+  for (int e0 = tid; e0 < 4 * NI; e0 += NW * BT) {
+    T a[NW][6], b[NW][6], o[NW][4];
+    int at[NW];
+    bool ok[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) {
+      const int e = min(e0 + w * BT, 4 * NI - 1);
+      const int m = e / NI, f = e % NI;
+      int base, ust, cdo, cst, cls, dir;
+      ok[w] = geo(f, base, ust, cdo, cst, cls, dir) && e0 + w * BT < 4 * NI;
+      at[w] = m * NI + f;
+      load_stencil(m, base, ust, cdo, cst, cls, dir, a[w], b[w]);
+    }
+    weno5_iface_n<NW, T>(P, a, b, o);
+#pragma unroll
+    for (int w = 0; w < NW; w++)
+      if (ok[w]) {
+        rec[at[w]] = o[w][0]; rec[at[w] + 4 * NI] = o[w][1]; rec[at[w] + 8 * NI] = o[w][2];
+        rec[at[w] + 12 * NI] = o[w][3];
+      }
   }
   __syncthreads();
   for (int f = tid; f < NI; f += BT) {
-    int base, ust, cst, cls, dir, cref;
-    const double *cd, *cdr;
-    if (!geo(f, base, ust, cd, cst, cls, dir, cref, cdr)) continue;
+    int base, ust, cdo, cst, cls, dir;
+    if (!geo(f, base, ust, cdo, cst, cls, dir)) continue;
     T* so = f < NXI ? fx + f : fy + (f - NXI);
-    iface_upwind_flow<NS2D, UPW, MX>(P, rec + f, 4 * NI, NI, sU + base - ust, sU + base, sU + cref, vs, dir, so,
+    iface_upwind_flow<NS2D, UPW, MX>(P, rec + f, 4 * NI, NI, sU + base - ust, sU + base, sU + c0, vs, dir, so,
                                      f < NXI ? NXI : NYI, spa + f, spm + f);
   }
   __syncthreads();
-  const int np = nv - 4;
-  for (int e = tid; e < np * NI; e += BT) {
-    const int m = 4 + e / NI, f = e % NI;
-    int base, ust, cst, cls, dir, cref;
-    const double *cd, *cdr;
-    if (!geo(f, base, ust, cd, cst, cls, dir, cref, cdr)) continue;
-    const double* u = sU + m * vs + base;
-    const double* vn = cd + 4 * cst;
-    T a[6], b[6], l, r, fl, fr;
-    if (MX) {
-      const double ur = sU[m * vs + cref], frf = __dmul_rn(cdr[4 * cst], ur);
+  const int npi = (nv - 4) * NI;
+  for (int e0 = tid; e0 < npi; e0 += NW * BT) {
+    T a[NW][6], b[NW][6], o[NW][4];
+    int fi[NW], mi[NW];
+    bool ok[NW];
 #pragma unroll
-      for (int q = 0; q < 6; q++) {
-        const double uu = u[(q - 3) * ust];
-        a[q] = (T)(uu - ur);
-        b[q] = (T)(__dmul_rn(vn[(q - 3) * cls], uu) - frf);
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < 6; q++) { a[q] = u[(q - 3) * ust]; b[q] = __dmul_rn(vn[(q - 3) * cls], a[q]); }
+    for (int w = 0; w < NW; w++) {
+      const int e = min(e0 + w * BT, npi - 1);
+      const int m = 4 + e / NI, f = e % NI;
+      int base, ust, cdo, cst, cls, dir;
+      ok[w] = geo(f, base, ust, cdo, cst, cls, dir) && e0 + w * BT < npi;
+      fi[w] = f; mi[w] = m;
+      load_stencil(m, base, ust, cdo, cst, cls, dir, a[w], b[w]);
     }
-    weno5_iface(P, a, b, l, r, fl, fr);
-    const T h = upwind_species(spm[f], spa[f], l, r, fl, fr);
-    if (f < NXI) fx[m * NXI + f] = h;
-    else fy[m * NYI + f - NXI] = h;
+    weno5_iface_n<NW, T>(P, a, b, o);
+#pragma unroll
+    for (int w = 0; w < NW; w++)
+      if (ok[w]) {
+        const int f = fi[w];
+        const T h = upwind_species(spm[f], spa[f], o[w][0], o[w][1], o[w][2], o[w][3]);
+        if (f < NXI) fx[mi[w] * NXI + f] = h;
+        else fy[mi[w] * NYI + f - NXI] = h;
+      }
   }
   __syncthreads();
   // viscous fluxes (k_visc_source on this tile), in the work region; MX:

@@ -98,14 +98,17 @@ __device__ __forceinline__ float rcp_nr(float x) {
 // Nonlinear weights of the fifth-order WENO family for one stencil
 // (m3,m2,m1,p1,p2) and optimal weights (c1,c2,c3).  Jiang-Shu, mapped
 // (Henrick-Aslam-Powers), Borges (WENO-Z) and Yamaleev-Carpenter variants as
-// selected in weno.inp (interpolation.h:255-545).  The Jiang-Shu weights are
-// normalised with a single reciprocal: w_k = c_k prod_{m!=k} q_m / sum, with
-// q_m = (beta_m + eps)^2, which equals c_k/q_k / sum_m c_m/q_m.  Quotients use
-// rcp_nr (Newton-Raphson reciprocal), so weights agree with the reference's
-// divisions to rounding.
-template <typename T>
-__device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T m2, T m1, T p1,
-                                             T p2, T eps, T& w1, T& w2, T& w3) {
+// selected in weno.inp (interpolation.h:255-545); WT_NONE (no_limiting) gives
+// the optimal weights.  The Jiang-Shu weights are normalised with a single
+// reciprocal: w_k = c_k prod_{m!=k} q_m / sum, with q_m = (beta_m + eps)^2,
+// which equals c_k/q_k / sum_m c_m/q_m.  Quotients use rcp_nr (Newton-Raphson
+// reciprocal), so weights agree with the reference's divisions to rounding.
+constexpr int WT_NONE = 4;
+
+template <int WT, typename T>
+__device__ __forceinline__ void weno_weights_t(T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& w1, T& w2,
+                                               T& w3) {
+  if (WT == WT_NONE) { w1 = c1; w2 = c2; w3 = c3; return; }
   const T t1312 = T(13.0 / 12.0), q4 = T(0.25);
   T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
   T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
@@ -113,13 +116,13 @@ __device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T
   T b1 = t1312 * d1 * d1 + q4 * e1 * e1;
   T b2 = t1312 * d2 * d2 + q4 * e2 * e2;
   T b3 = t1312 * d3 * d3 + q4 * e3 * e3;
-  if (type == W_JS || type == W_MAPPED) {
+  if (WT == W_JS || WT == W_MAPPED) {
     T s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
     T q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
     T a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
     T inv = rcp_nr(a1 + a2 + a3);
     w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
-    if (type == W_MAPPED) {
+    if (WT == W_MAPPED) {
       T x1 = w1, x2 = w2, x3 = w3;
       T n1 = x1 * (c1 + c1 * c1 - T(3) * c1 * x1 + x1 * x1), d1m = (c1 * c1 + x1 * (T(1) - T(2) * c1));
       T n2 = x2 * (c2 + c2 * c2 - T(3) * c2 * x2 + x2 * x2), d2m = (c2 * c2 + x2 * (T(1) - T(2) * c2));
@@ -131,12 +134,23 @@ __device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T
     return;
   }
   T tau;
-  if (type == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
+  if (WT == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
   else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = t * t; }
   T r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
   T a1 = c1 * (T(1) + r1 * r1), a2 = c2 * (T(1) + r2 * r2), a3 = c3 * (T(1) + r3 * r3);
   T inv = rcp_nr(a1 + a2 + a3);
   w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+}
+
+template <typename T>
+__device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& w1,
+                                             T& w2, T& w3) {
+  switch (type) {
+    case W_MAPPED: weno_weights_t<W_MAPPED>(c1, c2, c3, m3, m2, m1, p1, p2, eps, w1, w2, w3); break;
+    case W_BORGES: weno_weights_t<W_BORGES>(c1, c2, c3, m3, m2, m1, p1, p2, eps, w1, w2, w3); break;
+    case W_YC: weno_weights_t<W_YC>(c1, c2, c3, m3, m2, m1, p1, p2, eps, w1, w2, w3); break;
+    default: weno_weights_t<W_JS>(c1, c2, c3, m3, m2, m1, p1, p2, eps, w1, w2, w3); break;
+  }
 }
 
 // 3-point candidate values of explicit WENO5 (Interp1PrimFifthOrderWENO.c:144-146)
@@ -150,23 +164,48 @@ __device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p
 }
 
 // The four WENO5 interface values at one interface (Interp1PrimFifthOrderWENO.c
-// for upw = +1 / -1 on u and f): a[0..5] and b[0..5] are u and f at cells
-// i-3 .. i+2 around interface i; left-biased stencils use cells i-3..i+1,
-// right-biased ones cells i+2..i-2.
+// for upw = +1 / -1 on u and f) with the weights of type WT: a[0..5] and
+// b[0..5] are u and f at cells i-3 .. i+2 around interface i; left-biased
+// stencils use cells i-3..i+1, right-biased ones cells i+2..i-2.
+template <int WT, typename T>
+__device__ __forceinline__ void weno5_iface_t(const T* a, const T* b, T eps, T& uL, T& uR, T& fL, T& fR) {
+  const T c1 = T(0.1), c2 = T(0.6), c3 = T(0.3);
+  T w1, w2, w3;
+  weno_weights_t<WT>(c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
+  uL = weno5_value(w1, w2, w3, a[0], a[1], a[2], a[3], a[4]);
+  weno_weights_t<WT>(c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, w1, w2, w3);
+  uR = weno5_value(w1, w2, w3, a[5], a[4], a[3], a[2], a[1]);
+  weno_weights_t<WT>(c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, w1, w2, w3);
+  fL = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
+  weno_weights_t<WT>(c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
+  fR = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
+}
+
+// weno5_iface_t for N independent interfaces with one branch on the weight
+// type (the straight-line code of the N interfaces can be interleaved);
+// o[n][0..3] = uL, uR, fL, fR of interface n.
+template <int N, typename T>
+__device__ __forceinline__ void weno5_iface_n(const DevParams& P, const T (*a)[6], const T (*b)[6], T (*o)[4]) {
+  const T eps = (T)P.eps;
+#define PIAFS_WENO_N(WT) \
+  _Pragma("unroll") for (int n = 0; n < N; n++) weno5_iface_t<WT>(a[n], b[n], eps, o[n][0], o[n][1], o[n][2], o[n][3])
+  switch (P.no_limiting ? WT_NONE : P.weno_type) {
+    case WT_NONE: PIAFS_WENO_N(WT_NONE); break;
+    case W_MAPPED: PIAFS_WENO_N(W_MAPPED); break;
+    case W_BORGES: PIAFS_WENO_N(W_BORGES); break;
+    case W_YC: PIAFS_WENO_N(W_YC); break;
+    default: PIAFS_WENO_N(W_JS); break;
+  }
+#undef PIAFS_WENO_N
+}
+
+// the four WENO5 values at one interface with the deck's weights
 template <typename T>
 __device__ __forceinline__ void weno5_iface(const DevParams& P, const T* a, const T* b, T& uL, T& uR, T& fL,
                                             T& fR) {
-  const T c1 = T(0.1), c2 = T(0.6), c3 = T(0.3), eps = (T)P.eps;
-  T w1, w2, w3;
-  if (P.no_limiting) { w1 = c1; w2 = c2; w3 = c3; }
-  else weno_weights(P.weno_type, c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
-  uL = weno5_value(w1, w2, w3, a[0], a[1], a[2], a[3], a[4]);
-  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, w1, w2, w3);
-  uR = weno5_value(w1, w2, w3, a[5], a[4], a[3], a[2], a[1]);
-  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, w1, w2, w3);
-  fL = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
-  if (!P.no_limiting) weno_weights(P.weno_type, c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
-  fR = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
+  T o[1][4];
+  weno5_iface_n<1, T>(P, (const T(*)[6])a, (const T(*)[6])b, o);
+  uL = o[0][0]; uR = o[0][1]; fL = o[0][2]; fR = o[0][3];
 }
 
 }  // namespace piafs
