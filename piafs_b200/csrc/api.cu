@@ -60,6 +60,7 @@ struct piafs_gpu_sim {
   int* err = nullptr;
   double* aos = nullptr;                   // ghosted AoS staging (host transfers)
   size_t aos_bytes = 0;
+  double* hnu = nullptr;                   // photon density [nz][ps] of the last RK stage (species output)
   // host mirror of the clock
   double t = 0.0;
   int iter = 0;
@@ -89,6 +90,7 @@ static void free_sim(piafs_gpu_sim* s) {
   cudaFree(s->cfl_acc);
   cudaFree(s->err);
   cudaFree(s->aos);
+  cudaFree(s->hnu);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -139,9 +141,12 @@ static void enqueue_hyp(piafs_gpu_sim* s, const double* U, double* out, bool neg
 
 // TimeRHSFunctionExplicit (TimeRHSFunctionExplicit.c:29-77) on SoA arrays:
 // rhs = -hyp + par + source; U must have its ghosts filled.
-static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const double* tdev, double cstage) {
+// hnu: where the source stores the photon density of this evaluation (the
+// reference's Chemistry::nv_hnu), or nullptr
+static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const double* tdev, double cstage,
+                        double* hnu = nullptr) {
   enqueue_hyp(s, U, rhs, true);
-  launch_visc_source(s->P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream);
+  launch_visc_source(s->P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream, hnu);
 }
 
 static void enqueue_bc(piafs_gpu_sim* s, double* u) {
@@ -166,7 +171,7 @@ static void enqueue_step(piafs_gpu_sim* s, bool with_norm) {
       launch_stage(n, Us, s->u, dd, a, st, s->stream);
       enqueue_bc(s, Us);
     }
-    enqueue_rhs(s, s->Ud[st], Us, s->tdev, d.c[st]);
+    enqueue_rhs(s, s->Ud[st], Us, s->tdev, d.c[st], st == ns - 1 ? s->hnu : nullptr);
   }
   const double* dd[MAX_STAGES];
   double b[MAX_STAGES];
@@ -267,6 +272,10 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   if (e == cudaSuccess) e = cudaMemset(s->err, 0, sizeof(int));
   s->aos_bytes = (size_t)P.npg * P.nvars * sizeof(double);
   if (e == cudaSuccess) e = cudaMalloc(&s->aos, s->aos_bytes);
+  // the species files carry the photon density of the last RK stage evaluated
+  // (zero before the first step, as the reference's calloc'd nv_hnu)
+  const bool binary_out = d.op_file_format == "binary" || d.op_file_format == "bin";
+  if (e == cudaSuccess && d.write_species && binary_out) e = alloc(&s->hnu, (size_t)P.nz * P.ps);
   if (e == cudaSuccess) e = cudaMemcpy(s->dxinv, d.dxinv.data(), d.dxinv.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(s->imap, d.imap.data(), d.imap.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -442,9 +451,41 @@ int piafs_gpu_Solve(piafs_gpu_sim* s, const char* output_dir) {
     for (int t = 0; t < d.restart_iter; t++)
       if ((t + 1) % d.file_op_iter == 0) index++;
   std::vector<double> host((size_t)s->P.N0 * s->P.N1 * d.nvars);
+  std::vector<double> hnu_host;
+  // ChemistryWriteSpecies (ChemistryWriteSpecies.c:19-90): per layer iz, the
+  // seven species of the LAST layer (the reference copies layer z_i for every
+  // iz) and the photon density of layer iz, as op_species_z<iz>[_NNNNN].bin,
+  // written before the solution file of the same index (Solve.cpp:56-65)
+  auto species = [&]() -> int {
+    if (!d.write_species || !s->hnu) return PIAFS_OK;
+    const DevParams& P = s->P;
+    const int nz = P.nz, nsp = 8, z_i = nz - 1;
+    hnu_host.resize((size_t)nz * P.ps);
+    CK(cudaMemcpyAsync(hnu_host.data(), s->hnu, hnu_host.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                       s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const long long npts = (long long)P.N0 * P.N1;
+    std::vector<double> sp((size_t)npts * nsp);
+    int width = 1;
+    for (int q = nz; q >= 10; q /= 10) width++;          // (int)log10(nz) + 1
+    for (int iz = d.write_all_zlocs == "no" ? z_i : 0; iz < nz; iz++) {
+      for (long long k = 0; k < npts; k++) {
+        const int i = (int)(k % P.N0), j = (int)(k / P.N0);
+        for (int m = 0; m < nsp - 1; m++) sp[k * nsp + m] = host[k * d.nvars + P.nflow + P.zstride * z_i + m];
+        sp[k * nsp + nsp - 1] = hnu_host[(size_t)iz * P.ps + pidx(P, i, j)];
+      }
+      char name[96];
+      if (overwrite) std::snprintf(name, sizeof(name), "op_species_z%0*d.bin", width, iz);
+      else std::snprintf(name, sizeof(name), "op_species_z%0*d_%05d.bin", width, iz, index);
+      std::string err;
+      if (int r = write_binary(std::string(output_dir) + "/" + name, d, sp.data(), err, nsp)) return fail(r, err);
+    }
+    return PIAFS_OK;
+  };
   auto output = [&]() -> int {
     if (!write) return PIAFS_OK;
     if (int r = piafs_gpu_get_solution(s, host.data())) return r;
+    if (int r = species()) return r;
     char name[64];
     if (overwrite) std::snprintf(name, sizeof(name), "op.bin");
     else std::snprintf(name, sizeof(name), "op_%05d.bin", index);

@@ -158,6 +158,7 @@ int setup_chemistry(const std::string& dir, Deck& d, int nflow, std::string& err
   if (int r = read_keyfile(dir + "/chemistry.inp", kv, found, err)) return r;
   for (auto& it : kv) {
     if (it.first == "nz") get(kv, "nz", nz_layers);
+    else if (it.first == "write_all_zlocs") get(kv, "write_all_zlocs", d.write_all_zlocs);
     else if (v.count(it.first)) get(kv, it.first.c_str(), v[it.first]);
   }
   if (v["f_CO2"] > 1.0 || v["f_CO2"] < 0.0 || v["f_O3"] > 1.0 || v["f_O3"] < 0.0) {
@@ -357,6 +358,9 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
   const int nflow = d.model == "navierstokes2d" ? 4 : 3;
   if (d.include_chem == "yes") {
     if (int r = setup_chemistry(dir, d, nflow, err)) return r;
+    // PhysicsOutput: Euler1DWriteChem always (Euler1DInitialize.c:144-145),
+    // NavierStokes2DWriteChem with write_output yes (NavierStokes2DInitialize.c:189)
+    d.write_species = d.model == "euler1d" || d.write_output == "yes";
   } else if (d.nvars != nflow) {
     err = "nvars has to be " + std::to_string(nflow) + " in solver.inp";
     return PIAFS_ERR_INPUT;
@@ -520,19 +524,20 @@ int make_params(const Deck& d, DevParams& P, std::string& err) {
   return 0;
 }
 
-int write_binary(const std::string& path, const Deck& d, const double* u, std::string& err) {
+int write_binary(const std::string& path, const Deck& d, const double* u, std::string& err, int nvars) {
+  if (nvars < 0) nvars = d.nvars;
   FILE* f = std::fopen(path.c_str(), "wb");
   if (!f) {
     err = "could not open " + path + " for writing";
     return PIAFS_ERR_IO;
   }
-  int hdr[2] = {d.ndims, d.nvars};
+  int hdr[2] = {d.ndims, nvars};
   long long npts = 1;
   for (int s : d.size) npts *= s;
   bool ok = std::fwrite(hdr, sizeof(int), 2, f) == 2;
   ok = ok && std::fwrite(d.size.data(), sizeof(int), d.ndims, f) == (size_t)d.ndims;
   ok = ok && std::fwrite(d.grid.data(), sizeof(double), d.grid.size(), f) == d.grid.size();
-  ok = ok && std::fwrite(u, sizeof(double), npts * d.nvars, f) == (size_t)(npts * d.nvars);
+  ok = ok && std::fwrite(u, sizeof(double), npts * nvars, f) == (size_t)(npts * nvars);
   std::fclose(f);
   if (!ok) {
     err = "short write to " + path;

@@ -36,6 +36,8 @@ struct Deck {
   // chemistry (normalised), valid if chem
   bool chem = false;
   int nz = 1;
+  std::string write_all_zlocs = "yes";   // chemistry.inp: species files for every layer, or the last
+  bool write_species = false;            // the model writes op_species_z*.bin beside the solution
   double chem_gamma = 0, kn[11] = {0}, qn[11] = {0}, I0 = 0, ch_c = 0, ch_h = 0, ch_nu = 0, n_O2 = 0;
   double t_start_norm = 0, t_pulse_norm = 0, sO3 = 0, dz = 0;
   double L_ref = 0, kg = 0, IA = 1, IB = 1, IC = 0;
@@ -62,7 +64,9 @@ struct DeckMemory {
 int read_deck_memory(const DeckMemory& m, Deck& d, std::string& err);
 // Flat device parameters from a parsed deck.
 int make_params(const Deck& d, DevParams& P, std::string& err);
-// Write an op_*.bin file (WriteBinary.c:37-93) from the interior AoS field.
-int write_binary(const std::string& path, const Deck& d, const double* u_interior, std::string& err);
+// Write an op_*.bin file (WriteBinary.c:37-93) from the interior AoS field of
+// nvars variables (the deck's by default).
+int write_binary(const std::string& path, const Deck& d, const double* u_interior, std::string& err,
+                 int nvars = -1);
 
 }  // namespace piafs

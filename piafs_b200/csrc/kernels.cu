@@ -467,7 +467,8 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
                                                      const double* __restrict__ dxinv,
                                                      const double* __restrict__ imap,
                                                      const double* __restrict__ tdev, double cstage,
-                                                     double* __restrict__ rhs, int do_chem) {
+                                                     double* __restrict__ rhs, int do_chem,
+                                                     double* __restrict__ hnu) {
   typedef typename std::conditional<MX, float, double>::type T;
   constexpr int BX = 32, BY = 8, QX = BX + 2, QY = BY + 2, FX = BX + 1, FY = BY + 1;
   __shared__ T su[QY][QX], sv[QY][QX], sT[QY][QX];
@@ -546,21 +547,23 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
   }
   if (do_chem) {
     const double t = *tdev + cstage * P.dt;
-    chem_source_point<T>(P, U, p, pulse_factor(P, t), imap[p], rhs);
+    chem_source_point<T>(P, U, p, pulse_factor(P, t), imap[p], rhs, hnu);
   }
 }
 
 // chemistry source alone (1D, or 2D without viscosity)
 template <bool MX>
 __global__ void k_source(DevParams P, const double* __restrict__ U, const double* __restrict__ imap,
-                         const double* __restrict__ tdev, double cstage, double* __restrict__ rhs) {
+                         const double* __restrict__ tdev, double cstage, double* __restrict__ rhs,
+                         double* __restrict__ hnu) {
   long long n = (long long)P.N0 * P.N1;
   long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (idx >= n) return;
   int i = (int)(idx % P.N0), j = (int)(idx / P.N0);
   long long p = pidx(P, i, j);
   const double t = *tdev + cstage * P.dt;
-  chem_source_point<typename std::conditional<MX, float, double>::type>(P, U, p, pulse_factor(P, t), imap[p], rhs);
+  chem_source_point<typename std::conditional<MX, float, double>::type>(P, U, p, pulse_factor(P, t), imap[p], rhs,
+                                                                        hnu);
 }
 
 __global__ void k_advance_time(double* tdev, double dt) { *tdev += dt; }
@@ -799,17 +802,18 @@ void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, 
 }
 
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
-                        const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s) {
+                        const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s,
+                        double* hnu) {
   do_visc = do_visc && P.ndims == 2 && P.viscous;
   do_chem = do_chem && P.chem;
   if (do_visc) {
     dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
-    if (P.mixed) k_visc_source<true><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem);
-    else k_visc_source<false><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem);
+    if (P.mixed) k_visc_source<true><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
+    else k_visc_source<false><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
   } else if (do_chem) {
     const unsigned nb = nblk((long long)P.N0 * P.N1, 256);
-    if (P.mixed) k_source<true><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs);
-    else k_source<false><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs);
+    if (P.mixed) k_source<true><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs, hnu);
+    else k_source<false><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs, hnu);
   }
 }
 

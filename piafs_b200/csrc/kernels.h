@@ -110,8 +110,10 @@ void launch_upwind_div(const DevParams& P, const double* U, const void* uL, cons
 void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
                          const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
 // rhs += par (if do_visc) then rhs += source (if do_chem)
+// hnu (optional): photon density planes [nz][ps] of this evaluation
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
-                        const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s);
+                        const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s,
+                        double* hnu = nullptr);
 void launch_upwind_iface(const DevParams& P, const double* U, const double* uL, const double* uR, const double* fL,
                          const double* fR, double* fI, int dir, cudaStream_t s);
 void launch_first_deriv(const DevParams& P, double* Df, const double* f, int dir, int bias, int nv, cudaStream_t s);

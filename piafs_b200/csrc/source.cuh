@@ -43,10 +43,13 @@ __device__ __forceinline__ T chem_hnu0(const DevParams& P, double hnu_factor, do
 
 // ChemistrySetPhotonDensity (ChemistrySolve.c:18-65) + _ChemistrySetRHS_ /
 // _ChemistrySetQ_ (chemistry.h:30-137) at point p, arithmetic in T, added to
-// the FP64 rhs; the energy slot takes the heating of the last layer.
+// the FP64 rhs; the energy slot takes the heating of the last layer.  With
+// hnu set, the photon density of layer iz is also stored at hnu[iz * ps + p]
+// (the reference keeps it in Chemistry::nv_hnu for the species output).
 template <typename T>
 __device__ void chem_source_point(const DevParams& P, const double* __restrict__ U, long long p,
-                                  double hnu_factor, double imap_p, double* __restrict__ rhs) {
+                                  double hnu_factor, double imap_p, double* __restrict__ rhs,
+                                  double* __restrict__ hnu = nullptr) {
   const long long ps = P.ps;
   T n_hnu = chem_hnu0<T>(P, hnu_factor, imap_p);
   T Q = T(0);
@@ -55,6 +58,7 @@ __device__ void chem_source_point(const DevParams& P, const double* __restrict__
       const T damp = T(1) - (T)P.dz * (T)(P.sO3 * P.n_O2) * (T)U[(P.nflow + P.zstride * (iz - 1) + 1) * ps + p];
       n_hnu = n_hnu * damp;
     }
+    if (hnu) hnu[iz * ps + p] = (double)n_hnu;
     const int nfv = P.nflow + P.zstride * iz;
     T src[5];
     chem_layer<T>(P, n_hnu, (T)U[(nfv + 0) * ps + p], (T)U[(nfv + 1) * ps + p], (T)U[(nfv + 2) * ps + p],

@@ -3,12 +3,15 @@
 Each fixture directory holds a complete input deck (written by
 piafs_b200.cases with fixed seeds) and ``ref_final.bin``, the final solution
 the reference CPU binary (serial build, oracle/_ref/PIAFS, compiled from the
-llnl/piafs sources by oracle/Makefile) writes for it.  Run from the repository
-root after ``make -C oracle``:
+llnl/piafs sources by oracle/Makefile) writes for it; decks that write the
+photochemical species keep every species file the reference writes, renamed
+``ref_op_species_z<k>_<NNNNN>.bin``.  Run from the repository root after
+``make -C oracle``:
 
     python tests/golden/make_golden.py
 """
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -39,6 +42,10 @@ CASES = {
         N=32, NY=32, n_iter=60, dt=DT2D, upwinding="rf-char", weno={"borges": 1})),
     "ns2d_chem3layer_crweno5_llf_24x20": (cases.ns2d_photochem_beam, dict(
         N=24, NY=20, n_iter=60, dt=DT2D, extra_chem={"z_mm": 3.0, "nz": 20}, layers=3)),
+    # species output (write_output yes): three layers, outputs at steps 0, 20, 40
+    "ns2d_chem3layer_species_16x12": (cases.ns2d_photochem_beam, dict(
+        N=16, NY=12, n_iter=40, dt=DT2D, extra_chem={"z_mm": 3.0, "nz": 20}, layers=3, write_output="yes",
+        file_op_iter=20)),
     "ns2d_shear_crweno5_llf_re200_48x40": (cases.ns2d_shear_layer, dict(N=48, NY=40, n_iter=30, dt=2e-3)),
     "ns2d_shear_weno5_roe_re200_40x32": (cases.ns2d_shear_layer, dict(
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", upwinding="roe")),
@@ -55,10 +62,13 @@ def make(name):
     shutil.rmtree(d, ignore_errors=True)
     meta = gen(d, **kw)
     subprocess.run([REF], cwd=d, check=True, stdout=subprocess.DEVNULL)
-    last = sorted(f for f in os.listdir(d) if f.startswith("op_") and f.endswith(".bin"))[-1]
+    last = sorted(f for f in os.listdir(d) if re.fullmatch(r"op_\d+\.bin", f))[-1]
     os.replace(os.path.join(d, last), os.path.join(d, "ref_final.bin"))
     for f in os.listdir(d):
-        if f not in KEEP and f != "ref_final.bin":
+        if f.startswith("op_species_"):
+            os.replace(os.path.join(d, f), os.path.join(d, "ref_" + f))
+    for f in os.listdir(d):
+        if f not in KEEP and f != "ref_final.bin" and not f.startswith("ref_op_species_"):
             os.remove(os.path.join(d, f))
     return meta
 

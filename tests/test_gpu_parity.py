@@ -75,6 +75,29 @@ def test_solve_writes_reference_format(deck_copy):
     assert np.array_equal(ini.u, u0)
 
 
+def test_species_files_match_the_reference(tmp_path):
+    """ChemistryWriteSpecies output beside each solution file: per output
+    index and layer, the seven species of the last layer and the photon
+    density of that layer from the last RK stage evaluated (zero at the
+    initial output), against the files the reference wrote for the deck."""
+    name = "ns2d_chem3layer_species_16x12"
+    src = os.path.join(GOLDEN, name)
+    with Simulation(src) as sim:
+        sim.solve(str(tmp_path))
+    refs = sorted(f[len("ref_"):] for f in os.listdir(src) if f.startswith("ref_op_species_"))
+    assert len(refs) == 9
+    assert sorted(f for f in os.listdir(tmp_path) if f.startswith("op_species_")) == refs
+    for f in refs:
+        ref = deck.read_op(os.path.join(src, "ref_" + f))
+        got = deck.read_op(str(tmp_path / f))
+        assert got.nvars == ref.nvars == 8 and list(got.size) == list(ref.size)
+        assert all(np.array_equal(a, b) for a, b in zip(got.grid, ref.grid))
+        num = np.sqrt(((got.u - ref.u) ** 2).sum(axis=0))
+        den = np.sqrt((ref.u ** 2).sum(axis=0))
+        rel = np.where(den > 1e-15, num / np.maximum(den, 1e-300), num)
+        assert rel.max() <= TOL, (f, rel)
+
+
 def test_cli_drop_in(deck_copy):
     import subprocess
     name = "euler1d_crweno5_rusanov_mapped_n200"
