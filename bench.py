@@ -43,12 +43,15 @@ TRAFFIC_PER_POINT = {11: (417.0e6 + 774.2e6) / (1536 * 1536)}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 CPU_SAMPLE_N = 512                          # sample grid of the CPU arms
 # Steps timed back to back from the initial condition before the state is
-# reset to it.  At dt = 0.4 dx the 2048^2 CRWENO5/LLF/SSPRK3 case (CFL 0.4 per
+# reset to it.  At dt = 0.4 dx the CRWENO5/LLF/SSPRK3 case (CFL 0.4 per
 # direction, 0.8 summed over the two) lies beyond the scheme's linear
-# stability limit: seeded noise grows into NaN after about 20 steps in the
-# reference's algorithm and in this one alike.  Timing chunks of 12 steps from
-# the initial state keeps every timed step a finite step of the workload.
-CHUNK = 12
+# stability limit at these resolutions: seeded noise grows into NaN after
+# about 24 steps at 2048^2 (in the reference's algorithm and in this one
+# alike) and after 9 at 4096^2, where the growth sets in from step 4.  Timing
+# chunks from the initial state keep every timed step a finite step of the
+# workload (and the mixed-precision error a comparison of smooth states).
+def chunk_steps(n):
+    return 12 if n <= 2048 else 4
 
 
 def parse():
@@ -79,9 +82,10 @@ def make_deck(path, a, n_iter, n=None):
         N = n or a.n or 1024
         return cases.euler1d_density_wave(path, N=N, n_iter=n_iter, dt=1e-4, scheme=a.scheme or "weno5",
                                           op_file_format="none")
+    # CFL 0.4 on this grid (sound speed 1): dt = 0.4 / N
     N = n or a.n or 2048
     return cases.ns2d_photochem_beam(path, N=N, n_iter=n_iter, scheme=a.scheme or "crweno5",
-                                     op_file_format="none", dt=0.4 / 2048)
+                                     op_file_format="none", dt=0.4 / N)
 
 
 def workload_config(a, meta, n_gpus):
@@ -93,7 +97,7 @@ def workload_config(a, meta, n_gpus):
             "time_scheme": "ssprk3", "dt": meta["dt"], "replicas": n_gpus, "parallelism": f"replicas{n_gpus}",
             "precision": a.precision,
             "step": "one SSPRK3 time step (3 RK stages) over the whole grid",
-            "timing": f"chunks of at most {CHUNK} steps from the initial condition, device time summed",
+            "timing": f"chunks of at most {chunk_steps(sz[0])} steps from the initial condition, device time summed",
             "l2": "state arrays (%.0f MB each) exceed the 126 MB L2; no flush" % (
                 8 * meta["nvars"] * (sz[0] + 6) * ((sz[1] + 6) if len(sz) > 1 else 1) / 1e6)}
 
@@ -412,6 +416,7 @@ def main():
         info = sim.info
         npts = info["dim"][0] * info["dim"][1]
         units_per_step = info["nstages"] * npts
+        N = max(info["dim"][0], info["dim"][1])
         stream = torch.cuda.ExternalStream(sim.stream)
 
         u0, t0 = sim.state(), info["t"]
@@ -423,17 +428,17 @@ def main():
         done = 0
         while done < a.warmup:
             reset()
-            n = min(CHUNK, a.warmup - done)
+            n = min(chunk_steps(N), a.warmup - done)
             sim.time_rk(n)
             done += n
-        # timed: K steps in chunks of at most CHUNK from the initial state,
+        # timed: K steps in chunks of at most chunk_steps(N) from the initial state,
         # each chunk bracketed by barrier + synchronize, device time summed
         ms = 0.0
         with ClockSampler(local) as clk:
             time.sleep(0.3)
             done = 0
             while done < a.steps:
-                n = min(CHUNK, a.steps - done)
+                n = min(chunk_steps(N), a.steps - done)
                 reset()
                 barrier()
                 torch.cuda.synchronize()

@@ -107,8 +107,12 @@ __device__ __forceinline__ int stg(int i) { return i + (i >> 4); }
 // arithmetic; it keeps O(1) backgrounds out of the FP32 rounding, and the
 // upwind/divergence kernel that reads these values only differences them
 // along the line or adds the reference back.
+// CTA sizes: up to 512 threads at 8 rows per thread (128 registers), up to 256
+// otherwise
+__host__ __device__ constexpr int crweno_max_threads(int M) { return M == 8 ? 512 : 256; }
+
 template <int M, int DIR, int WT, bool MX>
-__global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
+__global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     k_crweno_pair(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
                   void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
   static_assert(M >= 2, "a chunk needs a separator and at least one interior row");
@@ -302,13 +306,15 @@ __global__ void __launch_bounds__(256, (M <= 8 ? 2 : 1))
   }
 }
 
-// rows per thread: the smallest M that keeps a line within one 256-thread CTA
-// (lines of up to 4097 interfaces)
+// rows per thread: the smallest M that keeps a line within one CTA (256
+// threads, 512 at M = 8: lines of up to 4097 interfaces).  M = 8 with up to
+// 512 threads rather than M = 16 with 256: the 16-row chunks need about twice
+// the registers and would leave half the warps per SM.
 int crweno_rows_per_thread(int N) {
   const int rows = N - 1;
   const int cand[4] = {2, 4, 8, 16};
   for (int c = 0; c < 4; c++)
-    if ((rows + cand[c] - 1) / cand[c] <= 256) return cand[c];
+    if ((rows + cand[c] - 1) / cand[c] <= crweno_max_threads(cand[c])) return cand[c];
   return -1;
 }
 
@@ -322,8 +328,9 @@ void crweno_launch(const DevParams& P, const double* U, const double* F, void* u
   int Pt = (N - 1 + M - 1) / M;
   Pt = ((Pt + 31) / 32) * 32;
   const size_t smem = (size_t)(20 * Pt + 2 * (N + (N >> 4) + 1)) * sizeof(double);
-  // the largest line this M serves: 256 M + 1 interfaces
-  raise_smem_limit<k_crweno_pair<M, DIR, WT, MX>>((20 * 256 + 2 * (256 * M + 2 + ((256 * M + 2) >> 4) + 1)) *
+  // the largest line this M serves: T M + 1 interfaces with T threads
+  constexpr int T = crweno_max_threads(M);
+  raise_smem_limit<k_crweno_pair<M, DIR, WT, MX>>((20 * T + 2 * (T * M + 2 + ((T * M + 2) >> 4) + 1)) *
                                               (int)sizeof(double));
   dim3 grid(nlines, P.nvars, 2);
   k_crweno_pair<M, DIR, WT, MX><<<grid, Pt, smem, s>>>(P, U, F, uL, uR, fL, fR, err);
