@@ -68,6 +68,8 @@ def parse():
                     help="serving: grid points resident at once (0: HBM budget only)")
     ap.add_argument("--members", type=int, default=256, help="ensemble members")
     ap.add_argument("--member-steps", type=int, default=100, help="steps per ensemble member")
+    ap.add_argument("--launch", default=None,
+                    help="ensemble: launch configuration TXxTYxCTAS (tile, CTAs per SM) instead of the autotuner's")
     ap.add_argument("--n", type=int, default=None, help="grid size (default 2048 / 1024)")
     ap.add_argument("--scheme", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -255,12 +257,17 @@ def ensemble_bench(a):
         torch.cuda.synchronize()
         # the launch configuration for this class of ensemble (the autotuner,
         # run once on the full mix; its choice is reused by later ensembles
-        # of the class, so it is timed apart from the solves)
+        # of the class, so it is timed apart from the solves), or the one
+        # given with --launch
         t0 = time.perf_counter()
-        with Batch(precision=a.precision) as B:
-            B.add_many([m["dir"] for m in mem], [steps] * n)
-            B.tune()
-            tuned = B.info
+        if a.launch:
+            tx, ty, mb = (int(x) for x in a.launch.split("x"))
+            tuned = {"tile_x": tx, "tile_y": ty, "min_ctas_per_sm": mb}
+        else:
+            with Batch(precision=a.precision) as B:
+                B.add_many([m["dir"] for m in mem], [steps] * n)
+                B.tune()
+                tuned = B.info
         tune_s = time.perf_counter() - t0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
