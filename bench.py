@@ -231,29 +231,58 @@ def rel_l2_noise_floor(got, ref, floor=1e-6):
     return worst
 
 
+def _dist_setup():
+    """(rank, world, barrier): one process per GPU under torchrun; the
+    process group only brackets the timed regions and gathers results."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+    return rank, world, barrier
+
+
 def ensemble_bench(a):
     """The batched ensemble: every member of cases.ensemble solved (deck read,
     device set-up, steps, solution back to the host) in one batch, against
     the same members solved one at a time through Simulation (FP64).  Both
-    are wall-clock times of complete solves on one GPU; the batched step
-    phase is also reported as grid-point RK-stage updates per second."""
+    are wall-clock times of complete solves; the batched step phase is also
+    reported as grid-point RK-stage updates per second.  Under torchrun the
+    members are split across the ranks by work (piafs_b200.shard.balance),
+    each rank solves its share, and the times are the max over ranks between
+    barriers; only the per-rank results are gathered at the end."""
     import numpy as np
     import torch
-    from piafs_b200 import Batch, Simulation, cases
+    from piafs_b200 import Batch, Simulation, cases, shard
 
+    rank, world, barrier = _dist_setup()
     torch.cuda.init()
     n, steps = a.members, a.member_steps
-    tmp = tempfile.mkdtemp(prefix="piafs_ensemble_")
+    params = cases.ensemble_params(n=n, steps=steps)
+    mine = shard.balance([m["side"] ** 2 * steps for m in params], world)[rank]
+    tmp = tempfile.mkdtemp(prefix=f"piafs_ensemble_r{rank}_")
     try:
-        mem = cases.ensemble(tmp, n=n, steps=steps)
+        mem = cases.ensemble(tmp, n=n, steps=steps, members=mine)
         sides = [m["side"] for m in mem]
         npts = sum(s * s for s in sides)
+        nm = len(mem)
         # warm the CUDA context and the kernels' modules outside the timing
-        with Batch(precision=a.precision) as B:
-            B.add(mem[0]["dir"], 1)
-            B.step(1)
-        with Simulation(mem[0]["dir"]) as s:
-            s.time_rk(1)
+        if nm:
+            with Batch(precision=a.precision) as B:
+                B.add(mem[0]["dir"], 1)
+                B.step(1)
+            with Simulation(mem[0]["dir"]) as s:
+                s.time_rk(1)
         torch.cuda.synchronize()
         # the launch configuration for this class of ensemble (the autotuner,
         # run once on the full mix; its choice is reused by later ensembles
@@ -265,51 +294,71 @@ def ensemble_bench(a):
             tuned = {"tile_x": tx, "tile_y": ty, "min_ctas_per_sm": mb}
         else:
             with Batch(precision=a.precision) as B:
-                B.add_many([m["dir"] for m in mem], [steps] * n)
+                if nm:
+                    B.add_many([m["dir"] for m in mem], [steps] * nm)
                 B.tune()
                 tuned = B.info
         tune_s = time.perf_counter() - t0
         torch.cuda.synchronize()
+        barrier()
         t0 = time.perf_counter()
         with Batch(precision=a.precision) as B:
             B.set_launch(tuned["tile_x"], tuned["tile_y"], tuned["min_ctas_per_sm"])
-            ids = B.add_many([m["dir"] for m in mem], [steps] * n)
+            ids = B.add_many([m["dir"] for m in mem], [steps] * nm) if nm else []
             t1 = time.perf_counter()
-            admit = t1 - t0
             B.step(steps)
             t2 = time.perf_counter()
             sols = [B.solution(i) for i in ids]
             t3 = time.perf_counter()
             binfo = B.info
-        batched = t3 - t0
-        worst = 0.0
-        t0 = time.perf_counter()
+        barrier()
+        batched = time.perf_counter() - t0
+        t0s = time.perf_counter()
         one = []
         for m in mem:
             with Simulation(m["dir"]) as s:
                 s.time_rk(steps)
                 one.append(s.solution())
-        single = time.perf_counter() - t0
+        barrier()
+        single = time.perf_counter() - t0s
+        worst = 0.0
         for sb, so in zip(sols, one):
             worst = max(worst, rel_l2_noise_floor(sb, so))
         finite = all(bool(np.isfinite(x).all()) for x in sols)
-        units = 3 * steps * npts
-        line = {"metric": "ensemble solves/s", "value": n / batched, "unit": "solves/s", "n_gpus": 1,
-                "higher_is_better": True, "vs_baseline": None,
+        mine_res = {"members": [m["index"] for m in mem], "points": npts, "batched": batched,
+                    "single": single, "admit": t1 - t0, "step": t2 - t1, "results": t3 - t2, "worst": worst,
+                    "finite": finite, "tune_s": tune_s}
+        allr = shard.gather(mine_res)
+        if rank != 0:
+            return 0
+        done = sorted(k for r in allr for k in r["members"])
+        assert done == list(range(n)), "every member solved exactly once"
+        batched = max(r["batched"] for r in allr)
+        single = max(r["single"] for r in allr)
+        step_s = max(r["step"] for r in allr)
+        total_pts = sum(r["points"] for r in allr)
+        all_sides = [m["side"] for m in params]
+        units = 3 * steps * total_pts
+        line = {"metric": "ensemble solves/s", "value": n / batched, "unit": "solves/s", "n_gpus": world,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                 "dtype": "f64" if a.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded ensemble decks)",
                 "config": {"workload": f"ensemble_{n}_ns2d_photochem_weno5_llf_ssprk3_{steps}steps",
-                           "members": n, "steps": steps, "sides": [min(sides), max(sides)],
-                           "total_points": npts, "precision": a.precision,
+                           "members": n, "steps": steps, "sides": [min(all_sides), max(all_sides)],
+                           "total_points": total_pts, "precision": a.precision,
                            "tile": [binfo["tile_x"], binfo["tile_y"]],
-                           "min_ctas_per_sm": binfo["min_ctas_per_sm"], "tune_s": tune_s,
-                           "launches_per_step": binfo["launches_per_step"]},
-                "batched": {"wall_s": batched, "admit_s": admit,
-                            "step_s": t2 - t1, "pt_stage_updates_per_s": units / (t2 - t1),
-                            "results_s": t3 - t2},
+                           "min_ctas_per_sm": binfo["min_ctas_per_sm"],
+                           "tune_s": max(r["tune_s"] for r in allr),
+                           "launches_per_step": binfo["launches_per_step"],
+                           "parallelism": f"members split by work over {world} GPU(s)",
+                           "members_per_rank": [len(r["members"]) for r in allr]},
+                "batched": {"wall_s": batched, "admit_s": max(r["admit"] for r in allr),
+                            "step_s": step_s, "pt_stage_updates_per_s": units / step_s,
+                            "results_s": max(r["results"] for r in allr)},
                 "one_at_a_time": {"wall_s": single, "solves_per_s": n / single, "precision": "fp64"},
                 "speedup_vs_one_at_a_time": single / batched,
-                "accuracy": {"max_rel_l2_vs_one_at_a_time": worst}, "finite": finite}
+                "accuracy": {"max_rel_l2_vs_one_at_a_time": max(r["worst"] for r in allr)},
+                "finite": all(r["finite"] for r in allr)}
         print(json.dumps(line))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
@@ -321,33 +370,48 @@ def serving_bench(a):
     """The request stream of cases.serving_trace (Poisson arrivals at 2000
     requests/s, 70% 1D Euler / 30% 2D photochemical, 50-500 steps), its first
     --requests requests replayed in real time through the continuous-batching
-    serving loop under the HBM budget.  Latency = result ready - arrival."""
+    serving loop under the HBM budget.  Latency = result ready - arrival.
+    Under torchrun request k goes to rank k mod N (each rank serves a Poisson
+    stream of rate / N against its own budget); latencies are gathered."""
     import numpy as np
     import torch
-    from piafs_b200 import Request, serve_trace, cases
+    from piafs_b200 import Request, serve_trace, cases, shard
 
+    rank, world, barrier = _dist_setup()
     torch.cuda.init()
     reqs, arr = cases.serving_trace(n=a.requests)
-    rq = [Request(**r) for r in reqs]
+    mine = shard.round_robin(len(reqs), rank, world)
+    rq = [Request(**reqs[k]) for k in mine]
+    my_arr = [float(arr[k]) for k in mine]
     # warm the context and the kernels
-    serve_trace(rq[:2], [0.0, 0.0], precision=a.precision)
+    if rq:
+        serve_trace(rq[:2], [0.0] * len(rq[:2]), precision=a.precision)
     budget = int(a.hbm_budget_gb * 1e9)
-    t0 = time.perf_counter()
     maxpts = int(a.max_resident_points)
-    res = serve_trace(rq, list(arr), precision=a.precision, hbm_budget_bytes=budget, steps_per_round=4,
-                      max_resident_points=maxpts)
+    barrier()
+    t0 = time.perf_counter()
+    res = serve_trace(rq, my_arr, precision=a.precision, hbm_budget_bytes=budget, steps_per_round=4,
+                      max_resident_points=maxpts) if rq else []
     wall = time.perf_counter() - t0
+    barrier()
+    allr = shard.gather({"res": res, "wall": wall, "idx": mine})
+    if rank != 0:
+        return 0
+    res = [r for g in allr for r in g["res"]]
+    assert sorted(k for g in allr for k in g["idx"]) == list(range(len(reqs))), "every request served once"
+    wall = max(g["wall"] for g in allr)
     lat = np.array([r["finished_s"] - r["arrival_s"] for r in res])
     wait = np.array([r["admitted_s"] - r["arrival_s"] for r in res])
     units = sum(3 * q["nsteps"] * (q["n"] if q["kind"] == 1 else q["n"] ** 2) for q in reqs)
     span = max(r["finished_s"] for r in res) - min(r["arrival_s"] for r in res)
-    line = {"metric": "served solves/s", "value": len(res) / span, "unit": "solves/s", "n_gpus": 1,
-            "higher_is_better": True, "vs_baseline": None,
+    line = {"metric": "served solves/s", "value": len(res) / span, "unit": "solves/s", "n_gpus": world,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32+f64", "data": "synthetic (seeded request stream)",
             "config": {"workload": f"serving_{len(res)}req_poisson2000_70pct1d_30pct2d_50to500steps",
                        "requests": len(res), "rate_per_s": 2000.0, "precision": a.precision,
                        "hbm_budget_gb": a.hbm_budget_gb, "steps_per_round": 4,
                        "max_resident_points": maxpts, "admission": "FIFO",
+                       "parallelism": f"request k on GPU k mod {world}",
                        "pt_stage_updates": units},
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
@@ -368,9 +432,9 @@ def main():
     metric = "pt-stage updates/s"
 
     if a.workload == "ensemble" and a.impl == "gpu":
-        return ensemble_bench(a) if rank == 0 else 0
+        return ensemble_bench(a)
     if a.workload == "serving" and a.impl == "gpu":
-        return serving_bench(a) if rank == 0 else 0
+        return serving_bench(a)
 
     if a.impl == "reference":
         if rank != 0:

@@ -230,8 +230,29 @@ def ns2d_density_wave(path: str, N: int = 64, NY: Optional[int] = None, axis: in
     return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}
 
 
+def ensemble_params(n: int = 256, steps: int = 100, seed: int = 1, side_range=(64, 512),
+                    dt: float = 0.4 / 2048):
+    """The member parameters of ``ensemble`` (no files written): per member
+    its index, grid side, beam amplitude and radius, Re, beam half-angle and
+    time step, drawn in member order from ``seed``."""
+    rng = np.random.default_rng(seed)
+    lo, hi = side_range
+    out = []
+    for k in range(n):
+        side = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) / 32.0)) * 32
+        side = min(max(side, 32 * math.ceil(lo / 32)), hi)
+        amp = float(rng.uniform(0.5, 1.5))
+        radius = float(rng.uniform(0.02, 0.1))
+        Re = float(math.exp(rng.uniform(math.log(1e3), math.log(1e5))))
+        theta = math.asin(min(1.0, math.sin(THETA_RE_1E4) * 1e4 / Re))
+        mdt = min(0.4 / side, dt * 1e4 / Re, 0.1 * Re / (side * side))
+        out.append({"index": k, "side": side, "beam_amp": amp, "beam_radius": radius, "Re": Re, "theta": theta,
+                    "steps": steps, "dt": mdt})
+    return out
+
+
 def ensemble(root: str, n: int = 256, steps: int = 100, seed: int = 1, side_range=(64, 512),
-             dt: float = 0.4 / 2048, op_file_format: str = "none"):
+             dt: float = 0.4 / 2048, op_file_format: str = "none", members=None):
     """The batched-ensemble workload: ``n`` independent 2D photochemical
     Navier-Stokes members (``ns2d_photochem_beam`` decks) with grid sides
     drawn log-uniformly in ``side_range`` and rounded to multiples of 32, beam
@@ -244,23 +265,21 @@ def ensemble(root: str, n: int = 256, steps: int = 100, seed: int = 1, side_rang
     0.4, capped at the pulse resolution of the 2048^2 workload at Re = 1e4
     (dt_2048 = 0.4/2048, about 35 steps per pulse width) and at a diffusion
     number nu dt / dx^2 of about 0.2 for the thermal diffusivity
-    gamma / (Pr Re).  Member k's field noise uses seed 1000 * seed + k."""
-    rng = np.random.default_rng(seed)
-    lo, hi = side_range
+    gamma / (Pr Re).  Member k's field noise uses seed 1000 * seed + k.
+    ``members`` (indices) restricts the decks written and returned to a
+    subset; member k is the same whichever subset it is written in.  Returns
+    the ``ensemble_params`` dicts of the written members with their "dir"."""
+    keep = None if members is None else set(int(k) for k in members)
     out = []
-    for k in range(n):
-        side = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))) / 32.0)) * 32
-        side = min(max(side, 32 * math.ceil(lo / 32)), hi)
-        amp = float(rng.uniform(0.5, 1.5))
-        radius = float(rng.uniform(0.02, 0.1))
-        Re = float(math.exp(rng.uniform(math.log(1e3), math.log(1e5))))
-        theta = math.asin(min(1.0, math.sin(THETA_RE_1E4) * 1e4 / Re))
+    for m in ensemble_params(n, steps, seed, side_range, dt):
+        k = m["index"]
+        if keep is not None and k not in keep:
+            continue
         d = os.path.join(root, f"member{k:04d}")
-        mdt = min(0.4 / side, dt * 1e4 / Re, 0.1 * Re / (side * side))
-        ns2d_photochem_beam(d, N=side, n_iter=steps, scheme="weno5", seed=1000 * seed + k, beam_amp=amp,
-                            beam_radius=radius, theta=theta, Re=Re, dt=mdt, op_file_format=op_file_format)
-        out.append({"dir": d, "side": side, "beam_amp": amp, "beam_radius": radius, "Re": Re, "steps": steps,
-                    "dt": mdt})
+        ns2d_photochem_beam(d, N=m["side"], n_iter=steps, scheme="weno5", seed=1000 * seed + k,
+                            beam_amp=m["beam_amp"], beam_radius=m["beam_radius"], theta=m["theta"], Re=m["Re"],
+                            dt=m["dt"], op_file_format=op_file_format)
+        out.append(dict(m, dir=d))
     return out
 
 
