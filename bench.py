@@ -527,10 +527,13 @@ def main():
         last_chunk = n
         value = units_per_step * a.steps * n_gpus / (ms_max / 1e3)
 
-        # mixed precision: error of the last chunk's end state against the FP64
-        # path over the same steps from the same initial state
+        # mixed precision: error against the FP64 path after one full chunk of
+        # steps from the same initial state
         err = None
         if a.precision == "mixed":
+            last_chunk = chunk_steps(N)
+            reset()
+            sim.time_rk(last_chunk)
             got = sim.solution()
             with Simulation(tmp, precision="fp64") as ref_sim:
                 ref_sim.time_rk(last_chunk)

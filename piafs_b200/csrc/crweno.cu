@@ -39,7 +39,13 @@ constexpr int WT_NOLIM = 4;   // no_limiting: optimal weights everywhere
 
 // Nonlinear CRWENO5 weights (optimal weights 0.2, 0.5, 0.3) from the three
 // smoothness indicators of one stencil; tau is the WENO-Z / Yamaleev-Carpenter
-// reference indicator (interpolation.h:255-545).
+// reference indicator (interpolation.h:255-545).  The weights come back up
+// to a common positive factor (the normalisation by their sum, a reciprocal
+// and three products, is left out) except for the mapped weights, whose
+// mapping needs them normalised: every coefficient of a compact row is linear
+// in the weights, and the line solve scales each row to a unit diagonal, so
+// the factor cancels.  The unnormalised weights are the products the
+// normalisation would divide, so they overflow no sooner.
 template <int WT, typename R>
 __device__ __forceinline__ void crw_weights(R b1, R b2, R b3, R tau, R eps, R& w1, R& w2, R& w3) {
   constexpr R c1 = R(0.2), c2 = R(0.5), c3 = R(0.3);
@@ -50,6 +56,7 @@ __device__ __forceinline__ void crw_weights(R b1, R b2, R b3, R tau, R eps, R& w
     const R s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
     const R q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
     const R a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
+    if (WT == W_JS) { w1 = a1; w2 = a2; w3 = a3; return; }
     const R inv = rcp_nr(a1 + a2 + a3);
     w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
     if (WT == W_MAPPED) {   // Henrick-Aslam-Powers mapping
@@ -62,9 +69,7 @@ __device__ __forceinline__ void crw_weights(R b1, R b2, R b3, R tau, R eps, R& w
     }
   } else {
     const R r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
-    const R a1 = c1 * (R(1) + r1 * r1), a2 = c2 * (R(1) + r2 * r2), a3 = c3 * (R(1) + r3 * r3);
-    const R inv = rcp_nr(a1 + a2 + a3);
-    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+    w1 = c1 * (R(1) + r1 * r1); w2 = c2 * (R(1) + r2 * r2); w3 = c3 * (R(1) + r3 * r3);
   }
 }
 
