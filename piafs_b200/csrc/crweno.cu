@@ -44,8 +44,9 @@ constexpr int WT_NOLIM = 4;   // no_limiting: optimal weights everywhere
 // and three products, is left out) except for the mapped weights, whose
 // mapping needs them normalised: every coefficient of a compact row is linear
 // in the weights, and the line solve scales each row to a unit diagonal, so
-// the factor cancels.  The unnormalised weights are the products the
-// normalisation would divide, so they overflow no sooner.
+// the factor cancels.  In FP32 (mixed precision, cells relative to the line's
+// first value) the products stay finite for cell values within about 1e4 of
+// that reference.
 template <int WT, typename R>
 __device__ __forceinline__ void crw_weights(R b1, R b2, R b3, R tau, R eps, R& w1, R& w2, R& w3) {
   constexpr R c1 = R(0.2), c2 = R(0.5), c3 = R(0.3);
@@ -141,7 +142,7 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
   O* oR = (O*)(isF ? fR : uR) + (long long)v * P.pis + ibase;
   const int s = 1 + k * M;          // separator row (interface) of this thread
   const int kN = (N - 2) / M;       // thread owning row N-1
-  const R eps = (R)P.eps;
+  const R eps = R(4) * (R)P.eps;   // with the smoothness indicators at 4x (below)
   const double ref = MX ? src[0] : 0.0;
 
   // cells s-3 .. s+M+1
@@ -160,8 +161,10 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     if (k == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
   }
 
-  // smoothness indicators of the windows centred at cells s-2+t (t = 0..M+2):
-  // b1: 13/12 d^2 + 1/4 (a-4b+3c)^2, b2: .. (a-c)^2, b3: .. (3a-4b+c)^2
+  // smoothness indicators of the windows centred at cells s-2+t (t = 0..M+2),
+  // kept at 4x their value with eps at 4x, which scales every weight of a
+  // stencil by the same factor: b1: 13/3 d^2 + (a-4b+3c)^2, b2: .. (a-c)^2,
+  // b3: .. (3a-4b+c)^2
   R b1[M + 3], b2[M + 3], b3[M + 3];
   if (WT != WT_NOLIM) {
 #pragma unroll
@@ -169,15 +172,16 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
       const R a = c[t], b = c[t + 1], cc = c[t + 2];
       const R d = a - R(2) * b + cc;
       const R e1 = a - R(4) * b + R(3) * cc, e2 = a - cc, e3 = R(3) * a - R(4) * b + cc;
-      const R dd = R(13.0 / 12.0) * d * d;
-      b1[t] = dd + R(0.25) * e1 * e1;
-      b2[t] = dd + R(0.25) * e2 * e2;
-      b3[t] = dd + R(0.25) * e3 * e3;
+      const R dd = R(13.0 / 3.0) * d * d;
+      b1[t] = dd + e1 * e1;
+      b2[t] = dd + e2 * e2;
+      b3[t] = dd + e3 * e3;
     }
   }
-  // two-cell averages of the compact right-hand side, cells (s-3+j, s-2+j):
-  // pp = 5/6 left + 1/6 right, qq = 1/6 left + 5/6 right
-  constexpr R s6 = R(1.0 / 6.0), s56 = R(5.0 * (1.0 / 6.0));
+  // two-cell averages of the compact right-hand side at 3x (the rows are built
+  // at 3x, below), cells (s-3+j, s-2+j): pp = 5/2 left + 1/2 right,
+  // qq = 1/2 left + 5/2 right
+  constexpr R s6 = R(0.5), s56 = R(2.5);
   R pp[M + 3], qq[M + 3];
 #pragma unroll
   for (int j = 1; j < M + 3; j++) {
@@ -199,18 +203,19 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
         R w1, w2, w3, f1, f2, f3, tau = R(0);
         if (q == 0) {
           if (WT == W_BORGES) tau = fabs(b3[r + 2] - b1[r]);
-          if (WT == W_YC) { const R t4 = c[r] - R(4) * c[r + 1] + R(6) * c[r + 2] - R(4) * c[r + 3] + c[r + 4]; tau = t4 * t4; }
+          if (WT == W_YC) { const R t4 = c[r] - R(4) * c[r + 1] + R(6) * c[r + 2] - R(4) * c[r + 3] + c[r + 4]; tau = R(4) * t4 * t4; }
           crw_weights<WT, R>(b1[r], b2[r + 1], b3[r + 2], tau, eps, w1, w2, w3);
           f1 = qq[r + 1]; f2 = pp[r + 2]; f3 = qq[r + 2];
         } else {
           if (WT == W_BORGES) tau = fabs(b1[r + 1] - b3[r + 3]);
-          if (WT == W_YC) { const R t4 = c[r + 5] - R(4) * c[r + 4] + R(6) * c[r + 3] - R(4) * c[r + 2] + c[r + 1]; tau = t4 * t4; }
+          if (WT == W_YC) { const R t4 = c[r + 5] - R(4) * c[r + 4] + R(6) * c[r + 3] - R(4) * c[r + 2] + c[r + 1]; tau = R(4) * t4 * t4; }
           crw_weights<WT, R>(b3[r + 3], b2[r + 2], b1[r + 1], tau, eps, w1, w2, w3);
           f1 = pp[r + 3]; f2 = qq[r + 2]; f3 = pp[r + 2];
         }
-        constexpr R t3 = R(1.0 / 3.0), t23 = R(2.0 * (1.0 / 3.0));
-        const R lo = t23 * w1 + t3 * w2, hi = t3 * w3;
-        Br = t3 * w1 + t23 * w2 + t23 * w3;
+        // the compact row at 3x: (2 w1 + w2, w1 + 2 w2 + 2 w3, w3) and 3x the
+        // right-hand side (pp, qq above)
+        const R lo = R(2) * w1 + w2, hi = w3;
+        Br = w1 + R(2) * (w2 + w3);
         Ar = q == 0 ? lo : hi;
         Cr = q == 0 ? hi : lo;
         Rr = w1 * f1 + w2 * f2 + w3 * f3;
