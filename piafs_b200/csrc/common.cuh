@@ -99,46 +99,56 @@ __device__ __forceinline__ float rcp_nr(float x) {
 // (m3,m2,m1,p1,p2) and optimal weights (c1,c2,c3).  Jiang-Shu, mapped
 // (Henrick-Aslam-Powers), Borges (WENO-Z) and Yamaleev-Carpenter variants as
 // selected in weno.inp (interpolation.h:255-545); WT_NONE (no_limiting) gives
-// the optimal weights.  The Jiang-Shu weights are normalised with a single
-// reciprocal: w_k = c_k prod_{m!=k} q_m / sum, with q_m = (beta_m + eps)^2,
-// which equals c_k/q_k / sum_m c_m/q_m.  Quotients use rcp_nr (Newton-Raphson
+// the optimal weights.  weno_alpha_t returns them unnormalised, a_k, with
+// their normalising factor inv = 1 / sum a_k: a weight is w_k = a_k inv, and a
+// reconstruction sum_k w_k f_k is formed as (sum_k a_k f_k) inv.  The
+// Jiang-Shu a_k = c_k prod_{m!=k} q_m with q_m = (beta_m + eps)^2 (equal to
+// c_k/q_k up to a common factor).  The smoothness indicators are kept at 4x
+// their value with eps at 4x (and the Yamaleev-Carpenter tau at 4x), which
+// scales all a_k of a stencil alike.  Quotients use rcp_nr (Newton-Raphson
 // reciprocal), so weights agree with the reference's divisions to rounding.
 constexpr int WT_NONE = 4;
 
 template <int WT, typename T>
-__device__ __forceinline__ void weno_weights_t(T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& w1, T& w2,
-                                               T& w3) {
-  if (WT == WT_NONE) { w1 = c1; w2 = c2; w3 = c3; return; }
-  const T t1312 = T(13.0 / 12.0), q4 = T(0.25);
+__device__ __forceinline__ void weno_alpha_t(T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& a1, T& a2,
+                                             T& a3, T& inv) {
+  if (WT == WT_NONE) { a1 = c1; a2 = c2; a3 = c3; inv = T(1); return; }
+  const T t1343 = T(13.0 / 3.0), e4 = T(4) * eps;
   T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
   T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
   T d3 = m1 - T(2) * p1 + p2, e3 = T(3) * m1 - T(4) * p1 + p2;
-  T b1 = t1312 * d1 * d1 + q4 * e1 * e1;
-  T b2 = t1312 * d2 * d2 + q4 * e2 * e2;
-  T b3 = t1312 * d3 * d3 + q4 * e3 * e3;
+  T b1 = t1343 * d1 * d1 + e1 * e1;
+  T b2 = t1343 * d2 * d2 + e2 * e2;
+  T b3 = t1343 * d3 * d3 + e3 * e3;
   if (WT == W_JS || WT == W_MAPPED) {
-    T s1 = b1 + eps, s2 = b2 + eps, s3 = b3 + eps;
+    T s1 = b1 + e4, s2 = b2 + e4, s3 = b3 + e4;
     T q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
-    T a1 = c1 * q2 * q3, a2 = c2 * q1 * q3, a3 = c3 * q1 * q2;
-    T inv = rcp_nr(a1 + a2 + a3);
-    w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
+    a1 = c1 * q2 * q3; a2 = c2 * q1 * q3; a3 = c3 * q1 * q2;
+    inv = rcp_nr(a1 + a2 + a3);
     if (WT == W_MAPPED) {
-      T x1 = w1, x2 = w2, x3 = w3;
+      T x1 = a1 * inv, x2 = a2 * inv, x3 = a3 * inv;
       T n1 = x1 * (c1 + c1 * c1 - T(3) * c1 * x1 + x1 * x1), d1m = (c1 * c1 + x1 * (T(1) - T(2) * c1));
       T n2 = x2 * (c2 + c2 * c2 - T(3) * c2 * x2 + x2 * x2), d2m = (c2 * c2 + x2 * (T(1) - T(2) * c2));
       T n3 = x3 * (c3 + c3 * c3 - T(3) * c3 * x3 + x3 * x3), d3m = (c3 * c3 + x3 * (T(1) - T(2) * c3));
-      T A1 = n1 * rcp_nr(d1m), A2 = n2 * rcp_nr(d2m), A3 = n3 * rcp_nr(d3m);
-      T inv2 = rcp_nr(A1 + A2 + A3);
-      w1 = A1 * inv2; w2 = A2 * inv2; w3 = A3 * inv2;
+      a1 = n1 * rcp_nr(d1m); a2 = n2 * rcp_nr(d2m); a3 = n3 * rcp_nr(d3m);
+      inv = rcp_nr(a1 + a2 + a3);
     }
     return;
   }
   T tau;
   if (WT == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
-  else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = t * t; }
-  T r1 = tau * rcp_nr(b1 + eps), r2 = tau * rcp_nr(b2 + eps), r3 = tau * rcp_nr(b3 + eps);
-  T a1 = c1 * (T(1) + r1 * r1), a2 = c2 * (T(1) + r2 * r2), a3 = c3 * (T(1) + r3 * r3);
-  T inv = rcp_nr(a1 + a2 + a3);
+  else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = T(4) * t * t; }
+  T r1 = tau * rcp_nr(b1 + e4), r2 = tau * rcp_nr(b2 + e4), r3 = tau * rcp_nr(b3 + e4);
+  a1 = c1 * (T(1) + r1 * r1); a2 = c2 * (T(1) + r2 * r2); a3 = c3 * (T(1) + r3 * r3);
+  inv = rcp_nr(a1 + a2 + a3);
+}
+
+// the normalised weights
+template <int WT, typename T>
+__device__ __forceinline__ void weno_weights_t(T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& w1, T& w2,
+                                               T& w3) {
+  T a1, a2, a3, inv;
+  weno_alpha_t<WT>(c1, c2, c3, m3, m2, m1, p1, p2, eps, a1, a2, a3, inv);
   w1 = a1 * inv; w2 = a2 * inv; w3 = a3 * inv;
 }
 
@@ -164,21 +174,22 @@ __device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p
 }
 
 // The four WENO5 interface values at one interface (Interp1PrimFifthOrderWENO.c
-// for upw = +1 / -1 on u and f) with the weights of type WT: a[0..5] and
+// for upw = +1 / -1 on u and f) with the weights of type WT (each value formed
+// from the unnormalised weights, then scaled by their normalisation): a[0..5] and
 // b[0..5] are u and f at cells i-3 .. i+2 around interface i; left-biased
 // stencils use cells i-3..i+1, right-biased ones cells i+2..i-2.
 template <int WT, typename T>
 __device__ __forceinline__ void weno5_iface_t(const T* a, const T* b, T eps, T& uL, T& uR, T& fL, T& fR) {
   const T c1 = T(0.1), c2 = T(0.6), c3 = T(0.3);
-  T w1, w2, w3;
-  weno_weights_t<WT>(c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, w1, w2, w3);
-  uL = weno5_value(w1, w2, w3, a[0], a[1], a[2], a[3], a[4]);
-  weno_weights_t<WT>(c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, w1, w2, w3);
-  uR = weno5_value(w1, w2, w3, a[5], a[4], a[3], a[2], a[1]);
-  weno_weights_t<WT>(c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, w1, w2, w3);
-  fL = weno5_value(w1, w2, w3, b[0], b[1], b[2], b[3], b[4]);
-  weno_weights_t<WT>(c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, w1, w2, w3);
-  fR = weno5_value(w1, w2, w3, b[5], b[4], b[3], b[2], b[1]);
+  T a1, a2, a3, inv;
+  weno_alpha_t<WT>(c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, a1, a2, a3, inv);
+  uL = weno5_value(a1, a2, a3, a[0], a[1], a[2], a[3], a[4]) * inv;
+  weno_alpha_t<WT>(c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, a1, a2, a3, inv);
+  uR = weno5_value(a1, a2, a3, a[5], a[4], a[3], a[2], a[1]) * inv;
+  weno_alpha_t<WT>(c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, a1, a2, a3, inv);
+  fL = weno5_value(a1, a2, a3, b[0], b[1], b[2], b[3], b[4]) * inv;
+  weno_alpha_t<WT>(c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, a1, a2, a3, inv);
+  fR = weno5_value(a1, a2, a3, b[5], b[4], b[3], b[2], b[1]) * inv;
 }
 
 // weno5_iface_t for N independent interfaces with one branch on the weight
