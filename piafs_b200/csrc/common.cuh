@@ -109,17 +109,13 @@ __device__ __forceinline__ float rcp_nr(float x) {
 // reciprocal), so weights agree with the reference's divisions to rounding.
 constexpr int WT_NONE = 4;
 
+// the unnormalised weights from the stencil's three (4x) smoothness
+// indicators and, for Z / YC, the reference indicator tau (4x)
 template <int WT, typename T>
-__device__ __forceinline__ void weno_alpha_t(T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& a1, T& a2,
+__device__ __forceinline__ void weno_alpha_b(T c1, T c2, T c3, T b1, T b2, T b3, T tau, T eps, T& a1, T& a2,
                                              T& a3, T& inv) {
   if (WT == WT_NONE) { a1 = c1; a2 = c2; a3 = c3; inv = T(1); return; }
-  const T t1343 = T(13.0 / 3.0), e4 = T(4) * eps;
-  T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
-  T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
-  T d3 = m1 - T(2) * p1 + p2, e3 = T(3) * m1 - T(4) * p1 + p2;
-  T b1 = t1343 * d1 * d1 + e1 * e1;
-  T b2 = t1343 * d2 * d2 + e2 * e2;
-  T b3 = t1343 * d3 * d3 + e3 * e3;
+  const T e4 = T(4) * eps;
   if (WT == W_JS || WT == W_MAPPED) {
     T s1 = b1 + e4, s2 = b2 + e4, s3 = b3 + e4;
     T q1 = s1 * s1, q2 = s2 * s2, q3 = s3 * s3;
@@ -135,12 +131,26 @@ __device__ __forceinline__ void weno_alpha_t(T c1, T c2, T c3, T m3, T m2, T m1,
     }
     return;
   }
-  T tau;
   if (WT == W_BORGES) tau = (b3 - b1) < T(0) ? (b1 - b3) : (b3 - b1);
-  else { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = T(4) * t * t; }
   T r1 = tau * rcp_nr(b1 + e4), r2 = tau * rcp_nr(b2 + e4), r3 = tau * rcp_nr(b3 + e4);
   a1 = c1 * (T(1) + r1 * r1); a2 = c2 * (T(1) + r2 * r2); a3 = c3 * (T(1) + r3 * r3);
   inv = rcp_nr(a1 + a2 + a3);
+}
+
+template <int WT, typename T>
+__device__ __forceinline__ void weno_alpha_t(T c1, T c2, T c3, T m3, T m2, T m1, T p1, T p2, T eps, T& a1, T& a2,
+                                             T& a3, T& inv) {
+  if (WT == WT_NONE) { a1 = c1; a2 = c2; a3 = c3; inv = T(1); return; }
+  const T t1343 = T(13.0 / 3.0);
+  T d1 = m3 - T(2) * m2 + m1, e1 = m3 - T(4) * m2 + T(3) * m1;
+  T d2 = m2 - T(2) * m1 + p1, e2 = m2 - p1;
+  T d3 = m1 - T(2) * p1 + p2, e3 = T(3) * m1 - T(4) * p1 + p2;
+  T b1 = t1343 * d1 * d1 + e1 * e1;
+  T b2 = t1343 * d2 * d2 + e2 * e2;
+  T b3 = t1343 * d3 * d3 + e3 * e3;
+  T tau = T(0);
+  if (WT == W_YC) { T t = m3 - T(4) * m2 + T(6) * m1 - T(4) * p1 + p2; tau = T(4) * t * t; }
+  weno_alpha_b<WT>(c1, c2, c3, b1, b2, b3, tau, eps, a1, a2, a3, inv);
 }
 
 // the normalised weights
@@ -178,18 +188,49 @@ __device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p
 // from the unnormalised weights, then scaled by their normalisation): a[0..5] and
 // b[0..5] are u and f at cells i-3 .. i+2 around interface i; left-biased
 // stencils use cells i-3..i+1, right-biased ones cells i+2..i-2.
+// Both biases of one field at interface i from the cells c[0..5] = i-3 .. i+2:
+// the left-biased stencil uses the windows (c0 c1 c2), (c1 c2 c3), (c2 c3 c4),
+// the right-biased one (c3 c4 c5), (c2 c3 c4), (c1 c2 c3) read backwards, so
+// the four windows' curvature terms (13/3 d^2) are computed once for both.
 template <int WT, typename T>
-__device__ __forceinline__ void weno5_iface_t(const T* a, const T* b, T eps, T& uL, T& uR, T& fL, T& fR) {
+__device__ __forceinline__ void weno5_pair_t(const T* c, T eps, T& vL, T& vR) {
   const T c1 = T(0.1), c2 = T(0.6), c3 = T(0.3);
   T a1, a2, a3, inv;
-  weno_alpha_t<WT>(c1, c2, c3, a[0], a[1], a[2], a[3], a[4], eps, a1, a2, a3, inv);
-  uL = weno5_value(a1, a2, a3, a[0], a[1], a[2], a[3], a[4]) * inv;
-  weno_alpha_t<WT>(c1, c2, c3, a[5], a[4], a[3], a[2], a[1], eps, a1, a2, a3, inv);
-  uR = weno5_value(a1, a2, a3, a[5], a[4], a[3], a[2], a[1]) * inv;
-  weno_alpha_t<WT>(c1, c2, c3, b[0], b[1], b[2], b[3], b[4], eps, a1, a2, a3, inv);
-  fL = weno5_value(a1, a2, a3, b[0], b[1], b[2], b[3], b[4]) * inv;
-  weno_alpha_t<WT>(c1, c2, c3, b[5], b[4], b[3], b[2], b[1], eps, a1, a2, a3, inv);
-  fR = weno5_value(a1, a2, a3, b[5], b[4], b[3], b[2], b[1]) * inv;
+  if (WT == WT_NONE) {
+    vL = weno5_value(c1, c2, c3, c[0], c[1], c[2], c[3], c[4]);
+    vR = weno5_value(c1, c2, c3, c[5], c[4], c[3], c[2], c[1]);
+    return;
+  }
+  const T t1343 = T(13.0 / 3.0);
+  T dd[4];
+#pragma unroll
+  for (int w = 0; w < 4; w++) {
+    const T d = c[w] - T(2) * c[w + 1] + c[w + 2];
+    dd[w] = t1343 * d * d;
+  }
+  // e-forms: x0 - 4 x1 + 3 x2, x0 - x2, 3 x0 - 4 x1 + x2 of window (x0 x1 x2)
+  const T eA0 = c[0] - T(4) * c[1] + T(3) * c[2];
+  const T eB1 = c[1] - c[3], eA1 = c[1] - T(4) * c[2] + T(3) * c[3];
+  const T eC2 = T(3) * c[2] - T(4) * c[3] + c[4], eB2 = c[2] - c[4];
+  const T eC3 = T(3) * c[3] - T(4) * c[4] + c[5];
+  T tauL = T(0), tauR = T(0);
+  if (WT == W_YC) {
+    const T tl = c[0] - T(4) * c[1] + T(6) * c[2] - T(4) * c[3] + c[4];
+    const T tr = c[5] - T(4) * c[4] + T(6) * c[3] - T(4) * c[2] + c[1];
+    tauL = T(4) * tl * tl; tauR = T(4) * tr * tr;
+  }
+  weno_alpha_b<WT>(c1, c2, c3, dd[0] + eA0 * eA0, dd[1] + eB1 * eB1, dd[2] + eC2 * eC2, tauL, eps, a1, a2, a3,
+                   inv);
+  vL = weno5_value(a1, a2, a3, c[0], c[1], c[2], c[3], c[4]) * inv;
+  weno_alpha_b<WT>(c1, c2, c3, dd[3] + eC3 * eC3, dd[2] + eB2 * eB2, dd[1] + eA1 * eA1, tauR, eps, a1, a2, a3,
+                   inv);
+  vR = weno5_value(a1, a2, a3, c[5], c[4], c[3], c[2], c[1]) * inv;
+}
+
+template <int WT, typename T>
+__device__ __forceinline__ void weno5_iface_t(const T* a, const T* b, T eps, T& uL, T& uR, T& fL, T& fR) {
+  weno5_pair_t<WT>(a, eps, uL, uR);
+  weno5_pair_t<WT>(b, eps, fL, fR);
 }
 
 // weno5_iface_t for N independent interfaces with one branch on the weight
