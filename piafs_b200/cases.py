@@ -50,7 +50,7 @@ def chem_gamma(f_CO2: float = 0.0) -> float:
 def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float = 1e-4,
                          amp: float = 0.2, scheme: str = "weno5", upwinding: str = "roe",
                          time_scheme_type: str = "ssprk3", file_op_iter: Optional[int] = None,
-                         op_file_format: str = "binary", weno: Optional[Dict] = None,
+                         op_file_format: str = "binary", weno: Optional[Dict] = None, interp: str = "components",
                          screen_op_iter: int = 0) -> Dict:
     os.makedirs(path, exist_ok=True)
     gamma = 1.4
@@ -62,7 +62,7 @@ def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float
     deck.write_keyfile(os.path.join(path, "solver.inp"), {
         "ndims": 1, "nvars": 3, "size": N, "ghost": 3, "n_iter": n_iter,
         "time_scheme": "rk", "time_scheme_type": time_scheme_type,
-        "hyp_space_scheme": scheme, "hyp_interp_type": "components", "dt": dt,
+        "hyp_space_scheme": scheme, "hyp_interp_type": interp, "dt": dt,
         "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
         "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
         "model": "euler1d",
@@ -85,6 +85,7 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
                         cfl: float = 0.4, dt: Optional[float] = None, file_op_iter: Optional[int] = None,
                         op_file_format: str = "binary", chemistry: bool = True,
                         noise: float = 1e-6, weno: Optional[Dict] = None, extra_chem: Optional[Dict] = None,
+                        interp: str = "components",
                         screen_op_iter: int = 0, write_output: str = "no", layers: int = 1) -> Dict:
     """``layers`` is the number of simulated z-layers, z_i + 1 with
     z_i = ceil(z_mm 1e-3 nz / Lz) from chemistry.inp (ChemistryInitialize.c:353);
@@ -115,7 +116,7 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
     deck.write_keyfile(os.path.join(path, "solver.inp"), {
         "ndims": 2, "nvars": nvars, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
         "time_scheme": "rk", "time_scheme_type": time_scheme_type,
-        "hyp_space_scheme": scheme, "hyp_interp_type": "components",
+        "hyp_space_scheme": scheme, "hyp_interp_type": interp,
         "par_space_scheme": "2", "dt": dt,
         "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
         "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
@@ -148,7 +149,7 @@ def ns2d_shear_layer(path: str, N: int = 64, NY: Optional[int] = None, n_iter: i
                      scheme: str = "crweno5", upwinding: str = "llf-char", Re: float = 200.0,
                      time_scheme_type: str = "ssprk3", weno: Optional[Dict] = None, delta: float = 0.05,
                      amp: float = 0.05, file_op_iter: Optional[int] = None, op_file_format: str = "binary",
-                     screen_op_iter: int = 0) -> Dict:
+                     screen_op_iter: int = 0, interp: str = "components") -> Dict:
     """2D Navier-Stokes (no chemistry) double shear layer, periodic in x, slip
     walls in y: u = tanh((y-1/4)/delta) - tanh((y-3/4)/delta) - 1,
     v = amp sin(2 pi x), rho = 1, p = 1/gamma; Re from physics.inp."""
@@ -170,7 +171,7 @@ def ns2d_shear_layer(path: str, N: int = 64, NY: Optional[int] = None, n_iter: i
     deck.write_keyfile(os.path.join(path, "solver.inp"), {
         "ndims": 2, "nvars": 4, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
         "time_scheme": "rk", "time_scheme_type": time_scheme_type,
-        "hyp_space_scheme": scheme, "hyp_interp_type": "components", "par_space_scheme": "2",
+        "hyp_space_scheme": scheme, "hyp_interp_type": interp, "par_space_scheme": "2",
         "dt": dt, "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
         "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
         "model": "navierstokes2d",

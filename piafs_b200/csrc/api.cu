@@ -114,7 +114,8 @@ static void enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* cons
   }
   launch_flux(P, U, s->fC, d, s->stream);
   mark();
-  if (P.scheme == WENO5) launch_weno5(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
+  if (P.scheme == WENO5 && P.char_interp) launch_weno5_char(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
+  else if (P.scheme == WENO5) launch_weno5(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
   else launch_crweno(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->err, s->stream);
   mark();
 }
@@ -235,6 +236,10 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   if (r) { delete s; return fail(r, err); }
   s->precision = precision;
   s->P.mixed = precision == PIAFS_PRECISION_MIXED ? 1 : 0;
+  if (s->P.mixed && s->P.char_interp) {
+    delete s;
+    return fail(PIAFS_ERR_UNSUPPORTED, "mixed precision runs hyp_interp_type components");
+  }
   const char* ng = std::getenv("PIAFS_GPU_NO_GRAPH");
   s->use_graph = !(ng && ng[0] == '1');
   const DevParams& P = s->P;
@@ -593,7 +598,9 @@ int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* s, double* fI, const doubl
   P.mixed = 0;   // operator-level entry points are FP64
   to_soa(s, u, s->scratch);
   to_soa(s, fC, s->fC);
-  if (P.scheme == WENO5)
+  if (P.scheme == WENO5 && P.char_interp)
+    launch_weno5_char(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);
+  else if (P.scheme == WENO5)
     launch_weno5(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);
   else
     launch_crweno(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->err, s->stream);

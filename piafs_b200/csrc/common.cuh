@@ -42,6 +42,7 @@ struct DevParams {
   double chem_gamma, I0, ch_c, ch_h, ch_nu, n_O2, t_start_norm, t_pulse_norm, sO3, dz;
   double dt;
   int mixed;             // 1: FP32 inner arithmetic on FP64 state (mixed precision)
+  int char_interp;       // 1: WENO5 on characteristic variables (hyp_interp_type characteristic)
 };
 
 __host__ __device__ inline long long pidx(const DevParams& P, int i, int j) {
@@ -249,6 +250,19 @@ __device__ __forceinline__ void weno5_iface_n(const DevParams& P, const T (*a)[6
     default: PIAFS_WENO_N(W_JS); break;
   }
 #undef PIAFS_WENO_N
+}
+
+// weno5_pair_t with the deck's weights
+template <typename T>
+__device__ __forceinline__ void weno5_pair(const DevParams& P, const T* c, T& vL, T& vR) {
+  const T eps = (T)P.eps;
+  switch (P.no_limiting ? WT_NONE : P.weno_type) {
+    case WT_NONE: weno5_pair_t<WT_NONE>(c, eps, vL, vR); break;
+    case W_MAPPED: weno5_pair_t<W_MAPPED>(c, eps, vL, vR); break;
+    case W_BORGES: weno5_pair_t<W_BORGES>(c, eps, vL, vR); break;
+    case W_YC: weno5_pair_t<W_YC>(c, eps, vL, vR); break;
+    default: weno5_pair_t<W_JS>(c, eps, vL, vR); break;
+  }
 }
 
 // the four WENO5 values at one interface with the deck's weights

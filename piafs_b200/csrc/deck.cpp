@@ -304,8 +304,12 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
     err = "hyp_space_scheme " + d.hyp_space_scheme + " is not on the GPU path (weno5, crweno5)";
     return PIAFS_ERR_UNSUPPORTED;
   }
-  if (d.hyp_interp_type != "components" && d.nvars > 1) {
-    err = "hyp_interp_type " + d.hyp_interp_type + " is not on the GPU path (components)";
+  // characteristic interpolation: WENO5 only (CRWENO5 on characteristic
+  // variables needs the block-tridiagonal solver, blocktridiagLU.c)
+  if (d.hyp_interp_type != "components" && d.nvars > 1 &&
+      !(d.hyp_interp_type == "characteristic" && d.hyp_space_scheme == "weno5")) {
+    err = "hyp_interp_type " + d.hyp_interp_type + " with " + d.hyp_space_scheme +
+          " is not on the GPU path (components; characteristic with weno5)";
     return PIAFS_ERR_UNSUPPORTED;
   }
   if (d.ghosts < 3) { err = "WENO5/CRWENO5 need ghost >= 3"; return PIAFS_ERR_INPUT; }
@@ -496,6 +500,7 @@ int make_params(const Deck& d, DevParams& P, std::string& err) {
   P.pis = (nmax + 31) / 32 * 32;
   P.model = d.model == "navierstokes2d" ? NS2D : EULER1D;
   P.scheme = d.hyp_space_scheme == "crweno5" ? CRWENO5 : WENO5;
+  P.char_interp = (d.hyp_interp_type == "characteristic" && d.nvars > 1) ? 1 : 0;
   P.upwind = d.upwinding == "roe" ? UPW_ROE : d.upwinding == "rf-char" ? UPW_RF
            : d.upwinding == "llf-char" ? UPW_LLF : UPW_RUSANOV;
   P.weno_type = d.yc ? W_YC : d.borges ? W_BORGES : d.mapped ? W_MAPPED : W_JS;

@@ -248,6 +248,77 @@ __global__ void k_weno5(DevParams P, const double* __restrict__ U, const double*
   weno5_iface(P, a, b, uL[o], uR[o], fL[o], fR[o]);
 }
 
+// ======================================================== WENO5 (characteristic)
+// Interp1PrimFifthOrderWENOChar (Interp1PrimFifthOrderWENOChar.c:92-200) with
+// the weights of WENOFifthOrderCalculateWeightsChar
+// (WENOFifthOrderCalculateWeights.c:761-1409): at each interface the flow
+// variables of the six stencil cells, of u and of the flux f alike, are
+// projected on the left eigenvectors of the Roe average of the two cells
+// beside the interface, each characteristic field is WENO5-reconstructed
+// (weights from its own projected values) for both biases, and the results
+// go back through the right eigenvectors.  The passive variables have unit
+// eigenvectors (navierstokes2d.h:243-247), so their reconstruction is the
+// component one.  One thread per interface.  (The reference takes the
+// average of the cells in the order of each bias; it is the same state to
+// rounding, and one average serves both biases here.)
+template <int MODEL, int DIR>
+__global__ void k_weno5_char(DevParams P, const double* __restrict__ U, const double* __restrict__ F,
+                             double* __restrict__ uL, double* __restrict__ uR, double* __restrict__ fL,
+                             double* __restrict__ fR) {
+  constexpr int NF = Flow<MODEL>::NF;
+  const long long ni = P.nint[DIR];
+  const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (q >= ni) return;
+  int i, l;
+  iface_decode<DIR>(P, q, i, l);
+  const long long st = DIR == 0 ? 1 : P.W0;
+  const long long c0 = cell_of<DIR>(P, i, l);    // cell i (right of the interface)
+  const long long ps = P.ps;
+  double cl[4], cr[4], ua[4], L[4][4], R[4][4];
+#pragma unroll
+  for (int m = 0; m < NF; m++) { cl[m] = U[m * ps + c0 - st]; cr[m] = U[m * ps + c0]; }
+  Flow<MODEL>::roe_avg(cl, cr, P.gamma, ua);
+  Flow<MODEL>::eigvec(ua, P.gamma, DIR, L, R);
+#pragma unroll
+  for (int fld = 0; fld < 2; fld++) {
+    const double* src = fld ? F : U;
+    double w[NF][6];                              // characteristic values, cells i-3 .. i+2
+#pragma unroll
+    for (int r = 0; r < 6; r++) {
+      double cv[4];
+#pragma unroll
+      for (int m = 0; m < NF; m++) cv[m] = src[m * ps + c0 + (r - 3) * st];
+#pragma unroll
+      for (int v = 0; v < NF; v++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < NF; k++) acc += L[v][k] * cv[k];
+        w[v][r] = acc;
+      }
+    }
+    double vl[4], vr[4];
+#pragma unroll
+    for (int v = 0; v < NF; v++) weno5_pair(P, w[v], vl[v], vr[v]);
+    double* oL = fld ? fL : uL;
+    double* oR = fld ? fR : uR;
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+      double sl = 0.0, sr = 0.0;
+#pragma unroll
+      for (int v = 0; v < NF; v++) { sl += R[k][v] * vl[v]; sr += R[k][v] * vr[v]; }
+      oL[k * P.pis + q] = sl;
+      oR[k * P.pis + q] = sr;
+    }
+  }
+  for (int m = NF; m < P.nvars; m++) {
+    double a[6], b[6];
+#pragma unroll
+    for (int r = 0; r < 6; r++) { a[r] = U[m * ps + c0 + (r - 3) * st]; b[r] = F[m * ps + c0 + (r - 3) * st]; }
+    const long long o = (long long)m * P.pis + q;
+    weno5_iface(P, a, b, uL[o], uR[o], fL[o], fR[o]);
+  }
+}
+
 // ============================================================ upwind + div
 // Upwind (NavierStokes2DUpwind*/Euler1DUpwind*) at the interfaces of a tile,
 // then hyp += dxinv (fI[j+1] - fI[j]) (HyperbolicFunction.c:97-112) and the
@@ -724,6 +795,17 @@ void launch_weno5(const DevParams& P, const double* U, const double* F, void* uL
   } else {
     if (dir == 0) k_weno5<0, false><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
     else k_weno5<1, false><<<nblk(n, 256), 256, 0, s>>>(P, U, F, uL, uR, fL, fR);
+  }
+}
+
+void launch_weno5_char(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                       double* fR, int dir, cudaStream_t s) {
+  const unsigned nb = nblk(P.nint[dir], 128);
+  if (P.model == NS2D) {
+    if (dir == 0) k_weno5_char<NS2D, 0><<<nb, 128, 0, s>>>(P, U, F, uL, uR, fL, fR);
+    else k_weno5_char<NS2D, 1><<<nb, 128, 0, s>>>(P, U, F, uL, uR, fL, fR);
+  } else {
+    k_weno5_char<EULER1D, 0><<<nb, 128, 0, s>>>(P, U, F, uL, uR, fL, fR);
   }
 }
 

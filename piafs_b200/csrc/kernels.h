@@ -91,6 +91,9 @@ void launch_cfl(const DevParams& P, const double* u, const double* dxinv, unsign
 void launch_flux(const DevParams& P, const double* U, double* F, int dir, cudaStream_t s);
 // WENO5 interface values; doubles, or floats relative to each line's first
 // value when P.mixed
+// WENO5 on characteristic variables (FP64; all four interface arrays)
+void launch_weno5_char(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                       double* fR, int dir, cudaStream_t s);
 void launch_weno5(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
                   int dir, cudaStream_t s);
 // CRWENO5 interface values (crweno.cu); -1 if a line is too long.  The

@@ -10,8 +10,23 @@ if ROOT not in sys.path:
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
-def golden_cases():
-    return sorted(d for d in os.listdir(GOLDEN) if os.path.isfile(os.path.join(GOLDEN, d, "ref_final.bin")))
+def interp_type(d):
+    """hyp_interp_type of a deck directory (the reference's default when absent)."""
+    for line in open(os.path.join(d, "solver.inp")):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == "hyp_interp_type":
+            return parts[1]
+    return "characteristic"
+
+
+def golden_cases(components_only=False):
+    """Golden fixture names; components_only leaves out the decks that
+    interpolate characteristic variables (the CPU oracle and the mixed
+    precision path restate component-wise interpolation only)."""
+    names = sorted(d for d in os.listdir(GOLDEN) if os.path.isfile(os.path.join(GOLDEN, d, "ref_final.bin")))
+    if components_only:
+        names = [n for n in names if interp_type(os.path.join(GOLDEN, n)) == "components"]
+    return names
 
 
 def pytest_configure(config):

@@ -46,6 +46,15 @@ CASES = {
     "ns2d_chem3layer_species_16x12": (cases.ns2d_photochem_beam, dict(
         N=16, NY=12, n_iter=40, dt=DT2D, extra_chem={"z_mm": 3.0, "nz": 20}, layers=3, write_output="yes",
         file_op_iter=20)),
+    # WENO5 on characteristic variables (the reference's default interpolation)
+    "euler1d_weno5char_roe_n256": (cases.euler1d_density_wave, dict(
+        N=256, n_iter=200, dt=4e-4, interp="characteristic")),
+    "euler1d_weno5char_llf_yc_n128": (cases.euler1d_density_wave, dict(
+        N=128, n_iter=100, dt=2e-3, upwinding="llf-char", weno={"yc": 1}, interp="characteristic")),
+    "ns2d_shear_weno5char_llf_re200_40x32": (cases.ns2d_shear_layer, dict(
+        N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", interp="characteristic")),
+    "ns2d_chem_weno5char_rf_32x24": (cases.ns2d_photochem_beam, dict(
+        N=32, NY=24, n_iter=60, dt=DT2D, scheme="weno5", upwinding="rf-char", interp="characteristic")),
     "ns2d_shear_crweno5_llf_re200_48x40": (cases.ns2d_shear_layer, dict(N=48, NY=40, n_iter=30, dt=2e-3)),
     "ns2d_shear_weno5_roe_re200_40x32": (cases.ns2d_shear_layer, dict(
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", upwinding="roe")),

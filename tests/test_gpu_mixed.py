@@ -46,7 +46,7 @@ def run(d, precision, steps=None):
         return sim.solution(), sim.info["nvars"]
 
 
-@pytest.mark.parametrize("name", golden_cases())
+@pytest.mark.parametrize("name", golden_cases(components_only=True))
 def test_mixed_tracks_fp64(name):
     d = os.path.join(GOLDEN, name)
     ref, nv = run(d, "fp64")

@@ -98,6 +98,25 @@ def test_species_files_match_the_reference(tmp_path):
         assert rel.max() <= TOL, (f, rel)
 
 
+def test_characteristic_interpolation_refusals(tmp_path):
+    """WENO5 on characteristic variables runs in FP64 single simulations; the
+    mixed-precision path and batched members refuse it, as the solver refuses
+    CRWENO5 on characteristic variables (the block-tridiagonal solve)."""
+    from piafs_b200 import Batch, PiafsError
+    d = os.path.join(GOLDEN, "ns2d_chem_weno5char_rf_32x24")
+    with pytest.raises(PiafsError) as ex:
+        Simulation(d, precision="mixed")
+    assert ex.value.code == 3
+    with Batch() as b, pytest.raises(PiafsError) as ex:
+        b.add(d)
+    assert ex.value.code == 3
+    c = str(tmp_path / "crwchar")
+    cases.ns2d_shear_layer(c, N=24, NY=20, n_iter=2, interp="characteristic")
+    with pytest.raises(PiafsError) as ex:
+        Simulation(c)
+    assert ex.value.code == 3
+
+
 def test_cli_drop_in(deck_copy):
     import subprocess
     name = "euler1d_crweno5_rusanov_mapped_n200"
