@@ -39,6 +39,16 @@ _CP_O2, _CV_O2 = 918.45, 650.0
 THETA_RE_1E4 = 4.2117e-5
 
 
+def _sponge_zones(sponge: Optional[Dict]):
+    """The sponge zone of a deck, if any: dict(dim, face, extent, values)
+    with extent = xmin, xmax per dimension and the reference state values
+    (BCSponge.c: the solution is relaxed towards them inside the box)."""
+    if not sponge:
+        return []
+    return [deck.BoundaryZone("sponge", sponge["dim"], sponge["face"], list(sponge["extent"]),
+                              values=list(sponge["values"]))]
+
+
 def chem_gamma(f_CO2: float = 0.0) -> float:
     """Specific-heat ratio of the O2/CO2 mixture (ChemistryInitialize.c:263-266)."""
     f_O2 = 1.0 - f_CO2
@@ -51,6 +61,7 @@ def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float
                          amp: float = 0.2, scheme: str = "weno5", upwinding: str = "roe",
                          time_scheme_type: str = "ssprk3", file_op_iter: Optional[int] = None,
                          op_file_format: str = "binary", weno: Optional[Dict] = None, interp: str = "components",
+                         sponge: Optional[Dict] = None,
                          screen_op_iter: int = 0) -> Dict:
     os.makedirs(path, exist_ok=True)
     gamma = 1.4
@@ -70,6 +81,7 @@ def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float
     deck.write_boundary(os.path.join(path, "boundary.inp"), [
         deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0]),
         deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0]),
+    ] + _sponge_zones(sponge) + [
     ])
     deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding})
     if weno:
@@ -149,7 +161,7 @@ def ns2d_shear_layer(path: str, N: int = 64, NY: Optional[int] = None, n_iter: i
                      scheme: str = "crweno5", upwinding: str = "llf-char", Re: float = 200.0,
                      time_scheme_type: str = "ssprk3", weno: Optional[Dict] = None, delta: float = 0.05,
                      amp: float = 0.05, file_op_iter: Optional[int] = None, op_file_format: str = "binary",
-                     screen_op_iter: int = 0, interp: str = "components") -> Dict:
+                     screen_op_iter: int = 0, interp: str = "components", sponge: Optional[Dict] = None) -> Dict:
     """2D Navier-Stokes (no chemistry) double shear layer, periodic in x, slip
     walls in y: u = tanh((y-1/4)/delta) - tanh((y-3/4)/delta) - 1,
     v = amp sin(2 pi x), rho = 1, p = 1/gamma; Re from physics.inp."""
@@ -182,6 +194,7 @@ def ns2d_shear_layer(path: str, N: int = 64, NY: Optional[int] = None, n_iter: i
         deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0, -big, big]),
         deck.BoundaryZone("slip-wall", 1, 1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
         deck.BoundaryZone("slip-wall", 1, -1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
+    ] + _sponge_zones(sponge) + [
     ])
     deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding, "Re": Re,
                                                            "Pr": 0.72})

@@ -61,6 +61,10 @@ struct piafs_gpu_sim {
   double* aos = nullptr;                   // ghosted AoS staging (host transfers)
   size_t aos_bytes = 0;
   double* hnu = nullptr;                   // photon density [nz][ps] of the last RK stage (species output)
+  // sponge zones: extents on the host, ramp and reference state in sponge_buf
+  struct SpongeDev { int dim; int is[2], ie[2]; size_t sig_off, ref_off; };
+  std::vector<SpongeDev> sponges;
+  double* sponge_buf = nullptr;
   // host mirror of the clock
   double t = 0.0;
   int iter = 0;
@@ -91,6 +95,7 @@ static void free_sim(piafs_gpu_sim* s) {
   cudaFree(s->err);
   cudaFree(s->aos);
   cudaFree(s->hnu);
+  cudaFree(s->sponge_buf);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -144,10 +149,17 @@ static void enqueue_hyp(piafs_gpu_sim* s, const double* U, double* out, bool neg
 // rhs = -hyp + par + source; U must have its ghosts filled.
 // hnu: where the source stores the photon density of this evaluation (the
 // reference's Chemistry::nv_hnu), or nullptr
+// the sponge zones' source (SourceFunction.c:42-57) added to rhs
+static void enqueue_sponge(piafs_gpu_sim* s, const double* U, double* rhs) {
+  for (const auto& z : s->sponges)
+    launch_sponge(s->P, U, rhs, z.dim, z.is, z.ie, s->sponge_buf + z.sig_off, s->sponge_buf + z.ref_off, s->stream);
+}
+
 static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const double* tdev, double cstage,
                         double* hnu = nullptr) {
   enqueue_hyp(s, U, rhs, true);
   launch_visc_source(s->P, U, s->dxinv, s->imap, tdev, cstage, rhs, 1, 1, s->stream, hnu);
+  enqueue_sponge(s, U, rhs);
 }
 
 static void enqueue_bc(piafs_gpu_sim* s, double* u) {
@@ -281,6 +293,21 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   // (zero before the first step, as the reference's calloc'd nv_hnu)
   const bool binary_out = d.op_file_format == "binary" || d.op_file_format == "bin";
   if (e == cudaSuccess && d.write_species && binary_out) e = alloc(&s->hnu, (size_t)P.nz * P.ps);
+  if (e == cudaSuccess && !d.sponges.empty()) {
+    std::vector<double> hb;
+    for (const auto& z : d.sponges) {
+      piafs_gpu_sim::SpongeDev sd{};
+      sd.dim = z.dim;
+      for (int k = 0; k < 2; k++) { sd.is[k] = z.is[k]; sd.ie[k] = z.ie[k]; }
+      sd.ref_off = hb.size();
+      hb.insert(hb.end(), z.uref.begin(), z.uref.end());
+      sd.sig_off = hb.size();
+      hb.insert(hb.end(), z.sigma.begin(), z.sigma.end());
+      s->sponges.push_back(sd);
+    }
+    e = alloc(&s->sponge_buf, hb.size());
+    if (e == cudaSuccess) e = cudaMemcpy(s->sponge_buf, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice);
+  }
   if (e == cudaSuccess) e = cudaMemcpy(s->dxinv, d.dxinv.data(), d.dxinv.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(s->imap, d.imap.data(), d.imap.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -411,6 +438,7 @@ int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) 
     CK(cudaEventRecord(ev[0], s->stream));
     enqueue_hyp(s, U, R, true, ev.data(), &k);
     launch_visc_source(P, U, s->dxinv, s->imap, s->tdev, 0.0, R, 1, 1, s->stream);
+    enqueue_sponge(s, U, R);
     CK(cudaEventRecord(ev[++k], s->stream));
     CK(cudaStreamSynchronize(s->stream));
     for (int i = 0; i < np; i++) {
@@ -565,6 +593,7 @@ static int visc_or_source(piafs_gpu_sim* s, double* out, const double* u, double
   CK(cudaMemsetAsync(R, 0, (size_t)P.nvars * P.ps * sizeof(double), s->stream));
   if (int r = set_top_t(s, t)) return r;
   launch_visc_source(P, U, s->dxinv, s->imap, s->top_t, 0.0, R, visc, chem, s->stream);
+  if (chem) enqueue_sponge(s, U, R);   // the sponge is part of SourceFunction
   launch_soa_to_aos(R, out, P.npg, P.nvars, P.ps, s->stream);
   return finish(s);
 }

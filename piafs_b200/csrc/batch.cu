@@ -313,6 +313,7 @@ int parse_member(const char* deck_dir, HostMember& hm, DevParams& P, std::string
   if (r) return r;
   if (P.scheme != WENO5) { err = "batched members use hyp_space_scheme weno5"; return PIAFS_ERR_UNSUPPORTED; }
   if (P.char_interp) { err = "batched members use hyp_interp_type components"; return PIAFS_ERR_UNSUPPORTED; }
+  if (!hm.deck.sponges.empty()) { err = "batched members have no sponge zones"; return PIAFS_ERR_UNSUPPORTED; }
   if (!((P.ndims == 2 && P.model == NS2D) || (P.ndims == 1 && P.model == EULER1D && !P.chem))) {
     err = "batched members are 2D navierstokes2d or 1D euler1d without chemistry";
     return PIAFS_ERR_UNSUPPORTED;

@@ -433,6 +433,7 @@ boundaries:
   int nb = std::atoi(t[i++].c_str());
   if (nb < 0 || nb > MAX_ZONES) { err = "too many boundary zones"; return PIAFS_ERR_UNSUPPORTED; }
   d.zones.clear();
+  d.sponges.clear();
   for (int n = 0; n < nb; n++) {
     if (i + 3 + 2 * d.ndims > t.size()) { err = "boundary.inp: truncated"; return PIAFS_ERR_INPUT; }
     Zone z{};
@@ -441,13 +442,41 @@ boundaries:
     z.face = std::atoi(t[i++].c_str());
     double ext[4] = {0, 0, 0, 0};
     for (int k = 0; k < 2 * d.ndims; k++) ext[k] = std::atof(t[i++].c_str());
+    if (type == "sponge") {
+      // InitializeBoundaries.c:113-118 (reference state), :313-326 (extent
+      // from FindInterval in every dimension); the ghost fill is a no-op
+      // (BCSpongeUDummy) and the zone acts through the source (BCSpongeSource)
+      if (z.dim < 0 || z.dim >= d.ndims || (z.face != 1 && z.face != -1) || i + d.nvars > t.size()) {
+        err = "boundary.inp: bad sponge zone";
+        return PIAFS_ERR_INPUT;
+      }
+      SpongeZone sz{};
+      sz.dim = z.dim;
+      sz.face = z.face;
+      for (int v = 0; v < d.nvars; v++) sz.uref.push_back(std::atof(t[i++].c_str()));
+      size_t off = 0;
+      for (int k = 0; k < 2; k++) {
+        if (k >= d.ndims) { sz.is[k] = 0; sz.ie[k] = 1; continue; }
+        find_interval(ext[2 * k], ext[2 * k + 1], d.grid.data() + off, d.size[k], sz.is[k], sz.ie[k]);
+        if (k == sz.dim) {
+          const double xstart = ext[2 * k], xend = ext[2 * k + 1];
+          for (int q = sz.is[k]; q < sz.ie[k]; q++) {
+            const double x = d.grid[off + q];   // _GetCoordinate_ (basic.h:34-39)
+            sz.sigma.push_back(sz.face > 0 ? (x - xstart) / (xend - xstart) : (x - xend) / (xstart - xend));
+          }
+        }
+        off += d.size[k];
+      }
+      if (sz.ie[0] > sz.is[0] && sz.ie[1] > sz.is[1]) d.sponges.push_back(sz);
+      continue;
+    }
     if (type == "periodic") z.type = BC_PERIODIC;
     else if (type == "extrapolate") z.type = BC_EXTRAPOLATE;
     else if (type == "slip-wall") {
       z.type = BC_SLIPWALL;
       for (int k = 0; k < d.ndims; k++) z.vel[k] = std::atof(t[i++].c_str());
     } else {
-      err = "boundary type " + type + " is not on the GPU path (periodic, extrapolate, slip-wall)";
+      err = "boundary type " + type + " is not on the GPU path (periodic, extrapolate, slip-wall, sponge)";
       return PIAFS_ERR_UNSUPPORTED;
     }
     if (z.dim < 0 || z.dim >= d.ndims || (z.face != 1 && z.face != -1)) {

@@ -14,6 +14,15 @@
 
 namespace piafs {
 
+// A sponge zone (BCSponge.c): inside the box [is, ie) of interior points the
+// source gets -sigma_i (u - uref), sigma ramping linearly along `dim`.
+struct SpongeZone {
+  int dim, face;
+  int is[2], ie[2];
+  std::vector<double> sigma;   // per index along dim, is[dim] .. ie[dim]-1
+  std::vector<double> uref;    // nvars
+};
+
 struct Deck {
   // solver.inp (ReadInputs.c:202-229 defaults)
   int ndims = 1, nvars = 1, ghosts = 1;
@@ -48,6 +57,7 @@ struct Deck {
   std::vector<double> u0;       // AoS with ghosts
   std::vector<double> imap;     // ghosted (chemistry only)
   std::vector<Zone> zones;
+  std::vector<SpongeZone> sponges;
 };
 
 // Parse the deck in `dir`.  Returns 0 on success, otherwise a PIAFS_ERR_*

@@ -622,6 +622,21 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
   }
 }
 
+// BCSpongeSource (BCSponge.c:42-73) added to the RHS: at the interior points
+// of the box [is0, ie0) x [is1, ie1), rhs_v -= sigma (u_v - uref_v), sigma the
+// ramp value at the point's index along the sponge dimension.
+__global__ void k_sponge(DevParams P, const double* __restrict__ U, double* __restrict__ rhs, int dim, int is0,
+                         int ie0, int is1, int ie1, const double* __restrict__ sigma,
+                         const double* __restrict__ uref) {
+  const int n0 = ie0 - is0, n1 = ie1 - is1;
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= (long long)n0 * n1) return;
+  const int i = is0 + (int)(k % n0), j = is1 + (int)(k / n0);
+  const long long p = pidx(P, i, j);
+  const double sg = sigma[dim == 0 ? i - is0 : j - is1];
+  for (int v = 0; v < P.nvars; v++) rhs[v * P.ps + p] -= sg * (U[v * P.ps + p] - uref[v]);
+}
+
 // chemistry source alone (1D, or 2D without viscosity)
 template <bool MX>
 __global__ void k_source(DevParams P, const double* __restrict__ U, const double* __restrict__ imap,
@@ -897,6 +912,13 @@ void launch_visc_source(const DevParams& P, const double* U, const double* dxinv
     if (P.mixed) k_source<true><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs, hnu);
     else k_source<false><<<nb, 256, 0, s>>>(P, U, imap, tdev, cstage, rhs, hnu);
   }
+}
+
+void launch_sponge(const DevParams& P, const double* U, double* rhs, int dim, const int* is, const int* ie,
+                   const double* sigma, const double* uref, cudaStream_t s) {
+  const long long n = (long long)(ie[0] - is[0]) * (ie[1] - is[1]);
+  if (n <= 0) return;
+  k_sponge<<<nblk(n, 256), 256, 0, s>>>(P, U, rhs, dim, is[0], ie[0], is[1], ie[1], sigma, uref);
 }
 
 void launch_advance_time(double* tdev, double dt, cudaStream_t s) { k_advance_time<<<1, 1, 0, s>>>(tdev, dt); }

@@ -113,6 +113,10 @@ void launch_upwind_div(const DevParams& P, const double* U, const void* uL, cons
 void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
                          const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
 // rhs += par (if do_visc) then rhs += source (if do_chem)
+// sponge zone source on the RHS (box [is, ie) per dimension, sigma per index
+// along dim, uref per variable; sigma and uref in device memory)
+void launch_sponge(const DevParams& P, const double* U, double* rhs, int dim, const int* is, const int* ie,
+                   const double* sigma, const double* uref, cudaStream_t s);
 // hnu (optional): photon density planes [nz][ps] of this evaluation
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,
                         const double* tdev, double cstage, double* rhs, int do_visc, int do_chem, cudaStream_t s,

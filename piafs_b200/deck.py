@@ -99,6 +99,7 @@ class BoundaryZone:
     face: int
     extent: Sequence[float]            # xmin, xmax for each dimension
     wall_velocity: Optional[Sequence[float]] = None   # slip-wall / noslip-wall
+    values: Optional[Sequence[float]] = None          # sponge: the reference state, one value per variable
 
 
 def write_boundary(path: str, zones: Sequence[BoundaryZone]) -> None:
@@ -110,6 +111,8 @@ def write_boundary(path: str, zones: Sequence[BoundaryZone]) -> None:
             f.write(line + "\n")
             if z.wall_velocity is not None:
                 f.write("  " + " ".join(repr(float(v)) for v in z.wall_velocity) + "\n")
+            if z.values is not None:
+                f.write("  " + " ".join(repr(float(v)) for v in z.values) + "\n")
 
 
 def read_boundary(path: str, ndims: int) -> List[BoundaryZone]:

@@ -19,13 +19,20 @@ def interp_type(d):
     return "characteristic"
 
 
-def golden_cases(components_only=False):
+def has_sponge(d):
+    return "sponge" in open(os.path.join(d, "boundary.inp")).read().split()
+
+
+def golden_cases(components_only=False, no_sponge=False):
     """Golden fixture names; components_only leaves out the decks that
     interpolate characteristic variables (the CPU oracle and the mixed
-    precision path restate component-wise interpolation only)."""
+    precision path restate component-wise interpolation only), no_sponge the
+    decks with sponge zones (not restated by the CPU oracle)."""
     names = sorted(d for d in os.listdir(GOLDEN) if os.path.isfile(os.path.join(GOLDEN, d, "ref_final.bin")))
     if components_only:
         names = [n for n in names if interp_type(os.path.join(GOLDEN, n)) == "components"]
+    if no_sponge:
+        names = [n for n in names if not has_sponge(os.path.join(GOLDEN, n))]
     return names
 
 

@@ -55,6 +55,12 @@ CASES = {
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", interp="characteristic")),
     "ns2d_chem_weno5char_rf_32x24": (cases.ns2d_photochem_beam, dict(
         N=32, NY=24, n_iter=60, dt=DT2D, scheme="weno5", upwinding="rf-char", interp="characteristic")),
+    # sponge zones (BCSponge.c): relaxation towards a reference state in a box
+    "euler1d_weno5_roe_sponge_n200": (cases.euler1d_density_wave, dict(
+        N=200, n_iter=100, dt=1e-3, sponge=dict(dim=0, face=1, extent=[0.7, 1.0], values=[1.0, 1.0, 3.0]))),
+    "ns2d_shear_weno5_llf_sponge_40x32": (cases.ns2d_shear_layer, dict(
+        N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5",
+        sponge=dict(dim=1, face=-1, extent=[-1e9, 1e9, 0.0, 0.25], values=[1.0, 0.0, 0.0, 2.5]))),
     "ns2d_shear_crweno5_llf_re200_48x40": (cases.ns2d_shear_layer, dict(N=48, NY=40, n_iter=30, dt=2e-3)),
     "ns2d_shear_weno5_roe_re200_40x32": (cases.ns2d_shear_layer, dict(
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", upwinding="roe")),
