@@ -304,7 +304,7 @@ int piafs_gpu_reciprocal(const double* x, double* y, long long n);
  * the GPU race and must be serialised by the caller.  The call runs on
  * `stream` (a cudaStream_t, 0 for the default stream) and waits for it. */
 enum { PIAFS_MODEL_EULER1D = 0, PIAFS_MODEL_NS2D = 1 };
-enum { PIAFS_SCHEME_WENO5 = 0, PIAFS_SCHEME_CRWENO5 = 1 };
+enum { PIAFS_SCHEME_WENO5 = 0, PIAFS_SCHEME_CRWENO5 = 1, PIAFS_SCHEME_UPW5 = 2 };
 enum { PIAFS_UPWIND_ROE = 0, PIAFS_UPWIND_RF = 1, PIAFS_UPWIND_LLF = 2, PIAFS_UPWIND_RUSANOV = 3 };
 enum { PIAFS_WENO_JS = 0, PIAFS_WENO_MAPPED = 1, PIAFS_WENO_BORGES = 2, PIAFS_WENO_YC = 3 };
 typedef struct {

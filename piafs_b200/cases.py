@@ -27,7 +27,7 @@ from __future__ import annotations
 
 import math
 import os
-from typing import Dict, Optional
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -61,8 +61,9 @@ def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float
                          amp: float = 0.2, scheme: str = "weno5", upwinding: str = "roe",
                          time_scheme_type: str = "ssprk3", file_op_iter: Optional[int] = None,
                          op_file_format: str = "binary", weno: Optional[Dict] = None, interp: str = "components",
-                         sponge: Optional[Dict] = None,
+                         sponge: Optional[Dict] = None, zones: Optional[List[deck.BoundaryZone]] = None,
                          screen_op_iter: int = 0) -> Dict:
+    """``zones`` replaces the periodic boundary zones."""
     os.makedirs(path, exist_ok=True)
     gamma = 1.4
     x = np.arange(N, dtype=np.float64) / N
@@ -78,11 +79,10 @@ def euler1d_density_wave(path: str, N: int = 1024, n_iter: int = 1000, dt: float
         "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
         "model": "euler1d",
     })
-    deck.write_boundary(os.path.join(path, "boundary.inp"), [
+    deck.write_boundary(os.path.join(path, "boundary.inp"), (zones if zones is not None else [
         deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0]),
         deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0]),
-    ] + _sponge_zones(sponge) + [
-    ])
+    ]) + _sponge_zones(sponge))
     deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding})
     if weno:
         deck.write_keyfile(os.path.join(path, "weno.inp"), weno)
@@ -98,10 +98,14 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
                         op_file_format: str = "binary", chemistry: bool = True,
                         noise: float = 1e-6, weno: Optional[Dict] = None, extra_chem: Optional[Dict] = None,
                         interp: str = "components",
-                        screen_op_iter: int = 0, write_output: str = "no", layers: int = 1) -> Dict:
+                        screen_op_iter: int = 0, write_output: str = "no", layers: int = 1,
+                        zones: Optional[List[deck.BoundaryZone]] = None, par: str = "2",
+                        flow: Sequence[float] = (0.0, 0.0)) -> Dict:
     """``layers`` is the number of simulated z-layers, z_i + 1 with
     z_i = ceil(z_mm 1e-3 nz / Lz) from chemistry.inp (ChemistryInitialize.c:353);
-    each layer carries its own 7 species."""
+    each layer carries its own 7 species.  ``zones`` replaces the boundary
+    zones (periodic in x, slip walls in y), ``par`` is par_space_scheme and
+    ``flow`` the initial velocity (u, v)."""
     os.makedirs(path, exist_ok=True)
     NX = N
     NY = NY or N
@@ -113,8 +117,11 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
     rho = 1.0 + rng.uniform(-noise, noise, size=(NY, NX))
     p = 1.0 / gamma
     u = np.zeros((NY, NX, nvars))
+    u0, v0 = float(flow[0]), float(flow[1])
     u[..., 0] = rho
-    u[..., 3] = p / (gamma - 1.0)
+    u[..., 1] = rho * u0
+    u[..., 2] = rho * v0
+    u[..., 3] = p / (gamma - 1.0) + 0.5 * rho * (u0 * u0 + v0 * v0)
     if chemistry:
         for iz in range(layers):
             u[..., 4 + 7 * iz] = 1.0            # O2 (normalised by n_O2)
@@ -129,13 +136,13 @@ def ns2d_photochem_beam(path: str, N: int = 2048, NY: Optional[int] = None, n_it
         "ndims": 2, "nvars": nvars, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
         "time_scheme": "rk", "time_scheme_type": time_scheme_type,
         "hyp_space_scheme": scheme, "hyp_interp_type": interp,
-        "par_space_scheme": "2", "dt": dt,
+        "par_space_scheme": par, "dt": dt,
         "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
         "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
         "model": "navierstokes2d",
     })
     big = 1e99
-    deck.write_boundary(os.path.join(path, "boundary.inp"), [
+    deck.write_boundary(os.path.join(path, "boundary.inp"), zones if zones is not None else [
         deck.BoundaryZone("periodic", 0, 1, [0.0, 0.0, -big, big]),
         deck.BoundaryZone("periodic", 0, -1, [0.0, 0.0, -big, big]),
         deck.BoundaryZone("slip-wall", 1, 1, [-big, big, 0.0, 0.0], [0.0, 0.0]),
@@ -240,6 +247,47 @@ def ns2d_density_wave(path: str, N: int = 64, NY: Optional[int] = None, axis: in
     ])
     deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding, "Re": Re,
                                                            "Pr": 0.72})
+    deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, 4))
+    return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}
+
+
+def ns2d_channel(path: str, zones: List[deck.BoundaryZone], N: int = 48, NY: Optional[int] = None,
+                 L: Sequence[float] = (1.0, 1.0), n_iter: int = 50, dt: float = 2e-3, scheme: str = "weno5",
+                 upwinding: str = "roe", interp: str = "components", Re: float = 1000.0, Pr: float = 0.72,
+                 par: str = "4", time_scheme_type: str = "44", flow: Sequence[float] = (0.3, 0.0),
+                 rho0: float = 1.0, bump: float = 0.05, bump_at: Sequence[float] = (0.5, 0.5),
+                 bump_radius: float = 0.1, file_op_iter: Optional[int] = None, op_file_format: str = "binary",
+                 screen_op_iter: int = 0) -> Dict:
+    """2D Navier-Stokes (no chemistry) on [0, L0] x [0, L1] with x_i = (i+1/2) L0/N
+    and the given boundary zones: a uniform flow (rho0, u, v, p = 1/gamma)
+    with a Gaussian density bump of relative height ``bump`` at ``bump_at``
+    (pressure uniform), as in the reference's wall, inflow and outflow
+    examples (flat plate, lid-driven cavity)."""
+    os.makedirs(path, exist_ok=True)
+    NX, NY = N, NY or N
+    gamma = 1.4
+    x = (np.arange(NX, dtype=np.float64) + 0.5) * (L[0] / NX)
+    y = (np.arange(NY, dtype=np.float64) + 0.5) * (L[1] / NY)
+    X, Y = np.meshgrid(x, y)
+    rho = rho0 * (1.0 + bump * np.exp(-((X - bump_at[0]) ** 2 + (Y - bump_at[1]) ** 2) / bump_radius ** 2))
+    uu, vv = float(flow[0]), float(flow[1])
+    p = 1.0 / gamma
+    u = np.zeros((NY, NX, 4))
+    u[..., 0] = rho
+    u[..., 1] = rho * uu
+    u[..., 2] = rho * vv
+    u[..., 3] = p / (gamma - 1.0) + 0.5 * rho * (uu * uu + vv * vv)
+    deck.write_keyfile(os.path.join(path, "solver.inp"), {
+        "ndims": 2, "nvars": 4, "size": [NX, NY], "ghost": 3, "n_iter": n_iter,
+        "time_scheme": "rk", "time_scheme_type": time_scheme_type,
+        "hyp_space_scheme": scheme, "hyp_interp_type": interp, "par_space_scheme": par,
+        "dt": dt, "screen_op_iter": screen_op_iter or n_iter, "file_op_iter": file_op_iter or n_iter,
+        "op_file_format": op_file_format, "ip_file_type": "binary", "op_overwrite": "no",
+        "model": "navierstokes2d",
+    })
+    deck.write_boundary(os.path.join(path, "boundary.inp"), zones)
+    deck.write_keyfile(os.path.join(path, "physics.inp"), {"gamma": gamma, "upwinding": upwinding, "Re": Re,
+                                                           "Pr": Pr})
     deck.write_array_binary(os.path.join(path, "initial.inp"), [x, y], u.reshape(-1, 4))
     return {"ndims": 2, "nvars": 4, "size": [NX, NY], "n_iter": n_iter, "dt": dt}
 

@@ -65,6 +65,7 @@ struct piafs_gpu_sim {
   struct SpongeDev { int dim; int is[2], ie[2]; size_t sig_off, ref_off; };
   std::vector<SpongeDev> sponges;
   double* sponge_buf = nullptr;
+  double* zone_buf = nullptr;              // boundary zones' values (Zone::val)
   // host mirror of the clock
   double t = 0.0;
   int iter = 0;
@@ -96,6 +97,7 @@ static void free_sim(piafs_gpu_sim* s) {
   cudaFree(s->aos);
   cudaFree(s->hnu);
   cudaFree(s->sponge_buf);
+  cudaFree(s->zone_buf);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -119,8 +121,8 @@ static void enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* cons
   }
   launch_flux(P, U, s->fC, d, s->stream);
   mark();
-  if (P.scheme == WENO5 && P.char_interp) launch_weno5_char(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
-  else if (P.scheme == WENO5) launch_weno5(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
+  if (P.scheme != CRWENO5 && P.char_interp) launch_weno5_char(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
+  else if (P.scheme != CRWENO5) launch_weno5(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->stream);
   else launch_crweno(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->err, s->stream);
   mark();
 }
@@ -307,6 +309,15 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
     }
     e = alloc(&s->sponge_buf, hb.size());
     if (e == cudaSuccess) e = cudaMemcpy(s->sponge_buf, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) {
+    std::vector<size_t> off;
+    const std::vector<double> hv = pack_zone_values(d, off);
+    if (!hv.empty()) {
+      e = alloc(&s->zone_buf, hv.size());
+      if (e == cudaSuccess) e = cudaMemcpy(s->zone_buf, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) bind_zone_values(d, off, s->zone_buf, s->deck.zones.data());
+    }
   }
   if (e == cudaSuccess) e = cudaMemcpy(s->dxinv, d.dxinv.data(), d.dxinv.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(s->imap, d.imap.data(), d.imap.size() * sizeof(double), cudaMemcpyHostToDevice);
@@ -627,9 +638,9 @@ int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* s, double* fI, const doubl
   P.mixed = 0;   // operator-level entry points are FP64
   to_soa(s, u, s->scratch);
   to_soa(s, fC, s->fC);
-  if (P.scheme == WENO5 && P.char_interp)
+  if (P.scheme != CRWENO5 && P.char_interp)
     launch_weno5_char(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);
-  else if (P.scheme == WENO5)
+  else if (P.scheme != CRWENO5)
     launch_weno5(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);
   else
     launch_crweno(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->err, s->stream);

@@ -311,7 +311,8 @@ int parse_member(const char* deck_dir, HostMember& hm, DevParams& P, std::string
   int r = read_deck(deck_dir, hm.deck, err);
   if (!r) r = make_params(hm.deck, P, err);
   if (r) return r;
-  if (P.scheme != WENO5) { err = "batched members use hyp_space_scheme weno5"; return PIAFS_ERR_UNSUPPORTED; }
+  if (P.scheme == CRWENO5) { err = "batched members use hyp_space_scheme weno5 or upw5"; return PIAFS_ERR_UNSUPPORTED; }
+  if (P.viscous && P.par4) { err = "batched members use par_space_scheme 2"; return PIAFS_ERR_UNSUPPORTED; }
   if (P.char_interp) { err = "batched members use hyp_interp_type components"; return PIAFS_ERR_UNSUPPORTED; }
   if (!hm.deck.sponges.empty()) { err = "batched members have no sponge zones"; return PIAFS_ERR_UNSUPPORTED; }
   if (!((P.ndims == 2 && P.model == NS2D) || (P.ndims == 1 && P.model == EULER1D && !P.chem))) {
@@ -337,7 +338,9 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   const int ns = d.nstages;
   const size_t planes = (size_t)P.nvars * P.ps;
   const size_t ndx = d.dxinv.size(), nim = req ? (P.chem ? (size_t)P.npg : 0) : d.imap.size();
-  const size_t bytes = ((3 + ns) * planes + ndx + nim) * sizeof(double);
+  std::vector<size_t> zoff;
+  const std::vector<double> zvals = pack_zone_values(d, zoff);
+  const size_t bytes = ((3 + ns) * planes + ndx + nim + zvals.size()) * sizeof(double);
   if (B->budget && B->used + bytes > B->budget)
     return nfail(PIAFS_ERR_MEMORY, "the batch's device memory budget cannot hold this member now");
   // slot
@@ -360,8 +363,10 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   double* im = dx + ndx;
   bm.dxinv = dx;
   bm.imap = nim ? im : nullptr;
+  double* zv = im + nim;
   bm.nzones = (int)d.zones.size();
   for (int z = 0; z < bm.nzones; z++) bm.zones[z] = d.zones[z];
+  bind_zone_values(d, zoff, zv, bm.zones);
   bm.nstages = ns;
   for (int s = 0; s < MAX_STAGES; s++) {
     for (int j = 0; j < MAX_STAGES; j++) bm.a[s * MAX_STAGES + j] = d.dt * d.A[s * MAX_STAGES + j];
@@ -394,6 +399,8 @@ int admit_member(piafs_gpu_batch* B, HostMember&& hm, DevParams P, int nsteps, i
   if (e == cudaSuccess) e = cudaMemcpyAsync(dx, d.dxinv.data(), ndx * sizeof(double), cudaMemcpyHostToDevice, B->stream);
   if (e == cudaSuccess && nim && !req)
     e = cudaMemcpyAsync(im, d.imap.data(), nim * sizeof(double), cudaMemcpyHostToDevice, B->stream);
+  if (e == cudaSuccess && !zvals.empty())
+    e = cudaMemcpyAsync(zv, zvals.data(), zvals.size() * sizeof(double), cudaMemcpyHostToDevice, B->stream);
   BState st{};
   st.u = u; st.X = bm.X; st.t = d.restart_iter * d.dt; st.iter = 0; st.active = bm.nsteps > 0 ? 1 : 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(B->dstate + slot, &st, sizeof(BState), cudaMemcpyHostToDevice, B->stream);

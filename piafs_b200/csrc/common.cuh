@@ -14,10 +14,15 @@
 namespace piafs {
 
 enum Model { EULER1D = 0, NS2D = 1 };
-enum Scheme { WENO5 = 0, CRWENO5 = 1 };
+enum Scheme { WENO5 = 0, CRWENO5 = 1, UPW5 = 2 };   // UPW5: fifth-order upwind (hyp_space_scheme upw5)
 enum Upwind { UPW_ROE = 0, UPW_RF = 1, UPW_LLF = 2, UPW_RUSANOV = 3 };
 enum WenoType { W_JS = 0, W_MAPPED = 1, W_BORGES = 2, W_YC = 3 };
-enum BcType { BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_SLIPWALL = 2 };
+enum BcType {
+  BC_PERIODIC = 0, BC_EXTRAPOLATE = 1, BC_SLIPWALL = 2, BC_DIRICHLET = 3, BC_REFLECT = 4,
+  // flow boundaries of the Euler / Navier-Stokes models (2D in the reference)
+  BC_NOSLIP = 5, BC_SUB_INFLOW = 6, BC_SUB_OUTFLOW = 7, BC_SUB_AMBIVALENT = 8, BC_SUP_INFLOW = 9,
+  BC_SUP_OUTFLOW = 10
+};
 
 constexpr int MAX_ZONES = 16;
 constexpr int MAX_STAGES = 4;
@@ -42,7 +47,8 @@ struct DevParams {
   double chem_gamma, I0, ch_c, ch_h, ch_nu, n_O2, t_start_norm, t_pulse_norm, sO3, dz;
   double dt;
   int mixed;             // 1: FP32 inner arithmetic on FP64 state (mixed precision)
-  int char_interp;       // 1: WENO5 on characteristic variables (hyp_interp_type characteristic)
+  int char_interp;       // 1: WENO5 / upw5 on characteristic variables (hyp_interp_type characteristic)
+  int par4;              // 1: fourth-order central first derivatives in the viscous terms (par_space_scheme 4)
 };
 
 __host__ __device__ inline long long pidx(const DevParams& P, int i, int j) {
@@ -109,6 +115,8 @@ __device__ __forceinline__ float rcp_nr(float x) {
 // scales all a_k of a stencil alike.  Quotients use rcp_nr (Newton-Raphson
 // reciprocal), so weights agree with the reference's divisions to rounding.
 constexpr int WT_NONE = 4;
+// the linear fifth-order upwind scheme in place of WENO5 (upw5)
+constexpr int WT_UPW5 = 5;
 
 // the unnormalised weights from the stencil's three (4x) smoothness
 // indicators and, for Z / YC, the reference indicator tau (4x)
@@ -174,6 +182,14 @@ __device__ __forceinline__ void weno_weights(int type, T c1, T c2, T c3, T m3, T
   }
 }
 
+// The fifth-order upwind value at an interface from the cells m3 .. p2 of its
+// bias (Interp1PrimFifthOrderUpwind.c:118-126, the same five products in the
+// same order)
+template <typename T>
+__device__ __forceinline__ T upw5_value(T m3, T m2, T m1, T p1, T p2) {
+  return T(1.0 / 30.0) * m3 - T(13.0 / 60.0) * m2 + T(47.0 / 60.0) * m1 + T(27.0 / 60.0) * p1 - T(1.0 / 20.0) * p2;
+}
+
 // 3-point candidate values of explicit WENO5 (Interp1PrimFifthOrderWENO.c:144-146)
 template <typename T>
 __device__ __forceinline__ T weno5_value(T w1, T w2, T w3, T m3, T m2, T m1, T p1, T p2) {
@@ -197,6 +213,11 @@ template <int WT, typename T>
 __device__ __forceinline__ void weno5_pair_t(const T* c, T eps, T& vL, T& vR) {
   const T c1 = T(0.1), c2 = T(0.6), c3 = T(0.3);
   T a1, a2, a3, inv;
+  if (WT == WT_UPW5) {
+    vL = upw5_value(c[0], c[1], c[2], c[3], c[4]);
+    vR = upw5_value(c[5], c[4], c[3], c[2], c[1]);
+    return;
+  }
   if (WT == WT_NONE) {
     vL = weno5_value(c1, c2, c3, c[0], c[1], c[2], c[3], c[4]);
     vR = weno5_value(c1, c2, c3, c[5], c[4], c[3], c[2], c[1]);
@@ -234,6 +255,12 @@ __device__ __forceinline__ void weno5_iface_t(const T* a, const T* b, T eps, T& 
   weno5_pair_t<WT>(b, eps, fL, fR);
 }
 
+// the reconstruction of the explicit schemes: upw5, WENO5 with the optimal
+// weights (no_limiting), or WENO5 with the deck's weights
+__host__ __device__ inline int weno_kind(const DevParams& P) {
+  return P.scheme == UPW5 ? WT_UPW5 : P.no_limiting ? WT_NONE : P.weno_type;
+}
+
 // weno5_iface_t for N independent interfaces with one branch on the weight
 // type (the straight-line code of the N interfaces can be interleaved);
 // o[n][0..3] = uL, uR, fL, fR of interface n.
@@ -242,7 +269,8 @@ __device__ __forceinline__ void weno5_iface_n(const DevParams& P, const T (*a)[6
   const T eps = (T)P.eps;
 #define PIAFS_WENO_N(WT) \
   _Pragma("unroll") for (int n = 0; n < N; n++) weno5_iface_t<WT>(a[n], b[n], eps, o[n][0], o[n][1], o[n][2], o[n][3])
-  switch (P.no_limiting ? WT_NONE : P.weno_type) {
+  switch (weno_kind(P)) {
+    case WT_UPW5: PIAFS_WENO_N(WT_UPW5); break;
     case WT_NONE: PIAFS_WENO_N(WT_NONE); break;
     case W_MAPPED: PIAFS_WENO_N(W_MAPPED); break;
     case W_BORGES: PIAFS_WENO_N(W_BORGES); break;
@@ -256,7 +284,8 @@ __device__ __forceinline__ void weno5_iface_n(const DevParams& P, const T (*a)[6
 template <typename T>
 __device__ __forceinline__ void weno5_pair(const DevParams& P, const T* c, T& vL, T& vR) {
   const T eps = (T)P.eps;
-  switch (P.no_limiting ? WT_NONE : P.weno_type) {
+  switch (weno_kind(P)) {
+    case WT_UPW5: weno5_pair_t<WT_UPW5>(c, eps, vL, vR); break;
     case WT_NONE: weno5_pair_t<WT_NONE>(c, eps, vL, vR); break;
     case W_MAPPED: weno5_pair_t<W_MAPPED>(c, eps, vL, vR); break;
     case W_BORGES: weno5_pair_t<W_BORGES>(c, eps, vL, vR); break;

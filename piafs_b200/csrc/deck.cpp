@@ -300,16 +300,16 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
   }
   if (d.input_mode != "serial") { err = "only input_mode serial is supported"; return PIAFS_ERR_UNSUPPORTED; }
   // schemes on the GPU path
-  if (d.hyp_space_scheme != "weno5" && d.hyp_space_scheme != "crweno5") {
-    err = "hyp_space_scheme " + d.hyp_space_scheme + " is not on the GPU path (weno5, crweno5)";
+  if (d.hyp_space_scheme != "weno5" && d.hyp_space_scheme != "crweno5" && d.hyp_space_scheme != "upw5") {
+    err = "hyp_space_scheme " + d.hyp_space_scheme + " is not on the GPU path (weno5, crweno5, upw5)";
     return PIAFS_ERR_UNSUPPORTED;
   }
-  // characteristic interpolation: WENO5 only (CRWENO5 on characteristic
-  // variables needs the block-tridiagonal solver, blocktridiagLU.c)
+  // characteristic interpolation: the explicit schemes only (CRWENO5 on
+  // characteristic variables needs the block-tridiagonal solver, blocktridiagLU.c)
   if (d.hyp_interp_type != "components" && d.nvars > 1 &&
-      !(d.hyp_interp_type == "characteristic" && d.hyp_space_scheme == "weno5")) {
+      !(d.hyp_interp_type == "characteristic" && d.hyp_space_scheme != "crweno5")) {
     err = "hyp_interp_type " + d.hyp_interp_type + " with " + d.hyp_space_scheme +
-          " is not on the GPU path (components; characteristic with weno5)";
+          " is not on the GPU path (components; characteristic with weno5 or upw5)";
     return PIAFS_ERR_UNSUPPORTED;
   }
   if (d.ghosts < 3) { err = "WENO5/CRWENO5 need ghost >= 3"; return PIAFS_ERR_INPUT; }
@@ -321,8 +321,8 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
     err = "ndims does not match the model";
     return PIAFS_ERR_INPUT;
   }
-  if (d.model == "navierstokes2d" && d.par_space_scheme != "2") {
-    err = "par_space_scheme " + d.par_space_scheme + " is not on the GPU path (2)";
+  if (d.model == "navierstokes2d" && d.par_space_scheme != "2" && d.par_space_scheme != "4") {
+    err = "par_space_scheme " + d.par_space_scheme + " is not a PIAFS parabolic scheme (2, 4)";
     return PIAFS_ERR_UNSUPPORTED;
   }
   if (int r = set_tableau(d, err)) return r;
@@ -433,6 +433,7 @@ boundaries:
   int nb = std::atoi(t[i++].c_str());
   if (nb < 0 || nb > MAX_ZONES) { err = "too many boundary zones"; return PIAFS_ERR_UNSUPPORTED; }
   d.zones.clear();
+  d.zone_vals.clear();
   d.sponges.clear();
   for (int n = 0; n < nb; n++) {
     if (i + 3 + 2 * d.ndims > t.size()) { err = "boundary.inp: truncated"; return PIAFS_ERR_INPUT; }
@@ -470,14 +471,43 @@ boundaries:
       if (sz.ie[0] > sz.is[0] && sz.ie[1] > sz.is[1]) d.sponges.push_back(sz);
       continue;
     }
+    // zone data, in the order the reference reads it (InitializeBoundaries.c:106-168)
+    std::vector<double> vals;
+    auto next = [&]() { return i < t.size() ? std::atof(t[i++].c_str()) : 0.0; };
+    const int nscalars = d.nvars - (2 + d.ndims);
     if (type == "periodic") z.type = BC_PERIODIC;
     else if (type == "extrapolate") z.type = BC_EXTRAPOLATE;
-    else if (type == "slip-wall") {
-      z.type = BC_SLIPWALL;
-      for (int k = 0; k < d.ndims; k++) z.vel[k] = std::atof(t[i++].c_str());
+    else if (type == "reflect") z.type = BC_REFLECT;
+    else if (type == "dirichlet") {
+      z.type = BC_DIRICHLET;
+      for (int v = 0; v < d.nvars; v++) vals.push_back(next());
+    } else if (type == "slip-wall" || type == "noslip-wall") {
+      z.type = type == "slip-wall" ? BC_SLIPWALL : BC_NOSLIP;
+      for (int k = 0; k < d.ndims; k++) z.vel[k] = next();
+    } else if (type == "subsonic-inflow") {
+      z.type = BC_SUB_INFLOW;
+      z.rho = next();
+      for (int k = 0; k < d.ndims; k++) z.vel[k] = next();
+      for (int v = 0; v < nscalars; v++) vals.push_back(next());
+    } else if (type == "subsonic-outflow") {
+      z.type = BC_SUB_OUTFLOW;
+      z.pres = next();
+    } else if (type == "subsonic-ambivalent") {
+      z.type = BC_SUB_AMBIVALENT;
+      z.rho = next();
+      for (int k = 0; k < d.ndims; k++) z.vel[k] = next();
+      z.pres = next();
+    } else if (type == "supersonic-inflow") {
+      z.type = BC_SUP_INFLOW;
+      z.rho = next();
+      for (int k = 0; k < d.ndims; k++) z.vel[k] = next();
+      z.pres = next();
+      for (int v = 0; v < nscalars; v++) vals.push_back(next());
+    } else if (type == "supersonic-outflow") {
+      z.type = BC_SUP_OUTFLOW;
     } else {
-      err = "boundary type " + type + " is not on the GPU path (periodic, extrapolate, slip-wall, sponge)";
-      return PIAFS_ERR_UNSUPPORTED;
+      err = "boundary type " + type + " is not a PIAFS boundary condition (BCInitialize.c:19-35)";
+      return PIAFS_ERR_INPUT;
     }
     if (z.dim < 0 || z.dim >= d.ndims || (z.face != 1 && z.face != -1)) {
       err = "boundary.inp: bad dimension or face";
@@ -495,6 +525,7 @@ boundaries:
       xoff += d.size[k];
     }
     d.zones.push_back(z);
+    d.zone_vals.push_back(vals);
   }
   return 0;
 }
@@ -528,7 +559,8 @@ int make_params(const Deck& d, DevParams& P, std::string& err) {
   long long nmax = P.nint[0] > P.nint[1] ? P.nint[0] : P.nint[1];
   P.pis = (nmax + 31) / 32 * 32;
   P.model = d.model == "navierstokes2d" ? NS2D : EULER1D;
-  P.scheme = d.hyp_space_scheme == "crweno5" ? CRWENO5 : WENO5;
+  P.scheme = d.hyp_space_scheme == "crweno5" ? CRWENO5 : d.hyp_space_scheme == "upw5" ? UPW5 : WENO5;
+  P.par4 = d.par_space_scheme == "4" ? 1 : 0;
   P.char_interp = (d.hyp_interp_type == "characteristic" && d.nvars > 1) ? 1 : 0;
   P.upwind = d.upwinding == "roe" ? UPW_ROE : d.upwinding == "rf-char" ? UPW_RF
            : d.upwinding == "llf-char" ? UPW_LLF : UPW_RUSANOV;

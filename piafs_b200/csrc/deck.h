@@ -57,8 +57,25 @@ struct Deck {
   std::vector<double> u0;       // AoS with ghosts
   std::vector<double> imap;     // ghosted (chemistry only)
   std::vector<Zone> zones;
+  std::vector<std::vector<double>> zone_vals;   // per zone: the values Zone::val points to on the device
   std::vector<SpongeZone> sponges;
 };
+
+// The zones' values (Zone::val) packed in one array; off[z] is zone z's offset.
+inline std::vector<double> pack_zone_values(const Deck& d, std::vector<size_t>& off) {
+  std::vector<double> v;
+  off.assign(d.zone_vals.size(), 0);
+  for (size_t z = 0; z < d.zone_vals.size(); z++) {
+    off[z] = v.size();
+    v.insert(v.end(), d.zone_vals[z].begin(), d.zone_vals[z].end());
+  }
+  return v;
+}
+// Point each zone that has values at its place in `dev` (device copy of
+// pack_zone_values).
+inline void bind_zone_values(const Deck& d, const std::vector<size_t>& off, const double* dev, Zone* zones) {
+  for (size_t z = 0; z < d.zone_vals.size(); z++) zones[z].val = d.zone_vals[z].empty() ? nullptr : dev + off[z];
+}
 
 // Parse the deck in `dir`.  Returns 0 on success, otherwise a PIAFS_ERR_*
 // code with a message in `err`.

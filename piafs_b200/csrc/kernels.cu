@@ -523,6 +523,22 @@ __global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double*
 }
 
 // ===================================================== viscous + chemistry
+// FirstDerivativeFourthOrderCentral (FirstDerivativeFourthOrder.c:68-127) at
+// index i of a line with N interior points and g ghosts, f(k) the value at
+// i + k: the central stencil inside, the reference's biased ones at the two
+// outermost points of each end (not divided by the grid spacing).  The
+// reference writes the left rows, then the interior, then the right rows, so
+// the right rows are tested first.
+template <typename T, typename Fn>
+__device__ __forceinline__ T d4(int i, int N, int g, Fn f) {
+  const T c = T(1.0 / 12.0);
+  if (i == N + g - 1) return (T(3) * f(-4) - T(16) * f(-3) + T(36) * f(-2) - T(48) * f(-1) + T(25) * f(0)) * c;
+  if (i == N + g - 2) return (-f(-3) + T(6) * f(-2) - T(18) * f(-1) + T(10) * f(0) + T(3) * f(1)) * c;
+  if (i == -g) return (T(-25) * f(0) + T(48) * f(1) - T(36) * f(2) + T(16) * f(3) - T(3) * f(4)) * c;
+  if (i == -g + 1) return (T(-3) * f(-1) - T(10) * f(0) + T(18) * f(1) - T(6) * f(2) + f(3)) * c;
+  return (f(-2) - T(8) * f(-1) + T(8) * f(1) - f(2)) * c;
+}
+
 // NavierStokes2DParabolicFunction (NavierStokes2DParabolicFunction.c:41-204)
 // with FirstDerivativeFirstOrder (bias +1 on Q, -1 on the fluxes), fused with
 // SourceFunction -> ChemistrySource (ChemistrySolve.c:18-115) and the RHS
@@ -622,6 +638,112 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
   }
 }
 
+// k_visc_source with par_space_scheme 4: the first derivatives of Q and of
+// the viscous fluxes by FirstDerivativeFourthOrderCentral (d4; the bias is
+// ignored), NavierStokes2DParabolicFunction.c:41-204 otherwise unchanged.
+// Tile: 32 x 8 interior points; the viscous fluxes reach two points beyond
+// it, their derivatives of Q two more.  As in the reference, QDerivX exists on
+// interior rows and QDerivY on interior columns only (zero elsewhere), so no
+// corner ghost is read.
+template <bool MX>
+__global__ void __launch_bounds__(256) k_visc4_source(DevParams P, const double* __restrict__ U,
+                                                      const double* __restrict__ dxinv,
+                                                      const double* __restrict__ imap,
+                                                      const double* __restrict__ tdev, double cstage,
+                                                      double* __restrict__ rhs, int do_chem,
+                                                      double* __restrict__ hnu) {
+  typedef typename std::conditional<MX, float, double>::type T;
+  constexpr int BX = 32, BY = 8, HQ = 4, HF = 2;
+  constexpr int QX = BX + 2 * HQ, QY = BY + 2 * HQ, FXW = BX + 2 * HF, FYH = BY + 2 * HF;
+  __shared__ T su[QY][QX], sv[QY][QX], sT[QY][QX];
+  __shared__ T fx[3][BY][FXW];   // FVx at i in [i0-2, i0+BX+2), rows j0..j0+BY-1
+  __shared__ T fy[3][FYH][BX];   // FVy at j in [j0-2, j0+BY+2), cols i0..i0+BX-1
+  const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+  const int tid = threadIdx.x + BX * threadIdx.y;
+  const long long ps = P.ps;
+  const int g = P.ghosts, N0 = P.N0, N1 = P.N1;
+  double Tref = 0.0;
+  if (MX) {
+    const long long p0 = pidx(P, i0, j0);
+    double rho, uu, vv, e_, pr;
+    ns_flowvar(U[p0], U[ps + p0], U[2 * ps + p0], U[3 * ps + p0], P.gamma, rho, uu, vv, e_, pr);
+    Tref = P.gamma * pr / rho;
+  }
+  // Q = (u, v, T = gamma p / rho) on [i0-4, i0+BX+4) x [j0-4, j0+BY+4)
+  for (int e = tid; e < QX * QY; e += BX * BY) {
+    const int a = e % QX, b = e / QX;
+    const int i = i0 - HQ + a, j = j0 - HQ + b;
+    double uu = 0.0, vv = 0.0, TT = Tref;
+    if (i >= -g && i < N0 + g && j >= -g && j < N1 + g) {
+      const long long p = pidx(P, i, j);
+      double rho, e_, pr;
+      ns_flowvar(U[p], U[ps + p], U[2 * ps + p], U[3 * ps + p], P.gamma, rho, uu, vv, e_, pr);
+      TT = P.gamma * pr / rho;
+    }
+    su[b][a] = (T)uu; sv[b][a] = (T)vv; sT[b][a] = (T)(TT - Tref);
+  }
+  __syncthreads();
+  const T two_third = T(2.0 / 3.0), inv_Re = (T)(1.0 / P.Re), inv_Pr = (T)(1.0 / P.Pr);
+  const T igm1 = (T)(1.0 / (P.gamma - 1.0));
+  // the viscous flux of direction `dir` at (i, j) from the scaled first
+  // derivatives of Q (QDerivX on interior rows, QDerivY on interior columns)
+  auto vflux = [&](int i, int j, int dir, T* out, int ostride) {
+    const int qa = i - (i0 - HQ), qb = j - (j0 - HQ);
+    const bool row_int = (j >= 0 && j < N1), col_int = (i >= 0 && i < N0);
+    T ux = T(0), vx = T(0), Tx = T(0), uy = T(0), vy = T(0), Ty = T(0);
+    if (row_int) {
+      const T dxi = (T)dxinv[g + i];
+      ux = d4<T>(i, N0, g, [&](int k) { return su[qb][qa + k]; }) * dxi;
+      vx = d4<T>(i, N0, g, [&](int k) { return sv[qb][qa + k]; }) * dxi;
+      Tx = d4<T>(i, N0, g, [&](int k) { return sT[qb][qa + k]; }) * dxi;
+    }
+    if (col_int) {
+      const T dyi = (T)dxinv[P.W0 + g + j];
+      uy = d4<T>(j, N1, g, [&](int k) { return su[qb + k][qa]; }) * dyi;
+      vy = d4<T>(j, N1, g, [&](int k) { return sv[qb + k][qa]; }) * dyi;
+      Ty = d4<T>(j, N1, g, [&](int k) { return sT[qb + k][qa]; }) * dyi;
+    }
+    const T uc = su[qb][qa], vc = sv[qb][qa], Tc = sT[qb][qa];
+    T mu, kappa;
+    visc_coeffs<T>(P, MX ? (T)Tref + Tc : Tc, mu, kappa);
+    const T mre = mu * inv_Re, kre = kappa * inv_Re * igm1 * inv_Pr;
+    if (dir == 0) {
+      const T txx = two_third * mre * (T(2) * ux - vy), txy = mre * (uy + vx);
+      out[0] = txx; out[ostride] = txy; out[2 * ostride] = uc * txx + vc * txy + kre * Tx;
+    } else {
+      const T tyx = mre * (uy + vx), tyy = two_third * mre * (-ux + T(2) * vy);
+      out[0] = tyx; out[ostride] = tyy; out[2 * ostride] = uc * tyx + vc * tyy + kre * Ty;
+    }
+  };
+  for (int e = tid; e < BY * FXW; e += BX * BY) {        // x fluxes on interior rows
+    const int a = e % FXW, b = e / FXW;
+    const int i = i0 - HF + a, j = j0 + b;
+    if (j < N1 && i >= -g && i < N0 + g) vflux(i, j, 0, &fx[0][b][a], BY * FXW);
+  }
+  for (int e = tid; e < FYH * BX; e += BX * BY) {        // y fluxes on interior columns
+    const int a = e % BX, b = e / BX;
+    const int i = i0 + a, j = j0 - HF + b;
+    if (i < N0 && j >= -g && j < N1 + g) vflux(i, j, 1, &fy[0][b][a], FYH * BX);
+  }
+  __syncthreads();
+  const int a = threadIdx.x, b = threadIdx.y;
+  const int i = i0 + a, j = j0 + b;
+  if (i >= N0 || j >= N1) return;
+  const long long p = pidx(P, i, j);
+  const T dxi = (T)dxinv[g + i], dyi = (T)dxinv[P.W0 + g + j];
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    const T dfx = d4<T>(i, N0, g, [&](int k) { return fx[m][b][a + HF + k]; });
+    const T dfy = d4<T>(j, N1, g, [&](int k) { return fy[m][b + HF + k][a]; });
+    const T par = dxi * dfx + dyi * dfy;
+    rhs[(m + 1) * ps + p] += (double)par;
+  }
+  if (do_chem) {
+    const double t = *tdev + cstage * P.dt;
+    chem_source_point<T>(P, U, p, pulse_factor(P, t), imap[p], rhs, hnu);
+  }
+}
+
 // BCSpongeSource (BCSponge.c:42-73) added to the RHS: at the interior points
 // of the box [is0, ie0) x [is1, ie1), rhs_v -= sigma (u_v - uref_v), sigma the
 // ramp value at the point's index along the sponge dimension.
@@ -710,9 +832,10 @@ __global__ void k_upwind_iface(DevParams P, const double* __restrict__ U, const 
     fI[m * P.pis + q] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q], fR[m * P.pis + q]);
 }
 
-// FirstDerivativeFirstOrder (FirstDerivativeFirstOrder.c:40-100) on an AoS
-// array with nv values per point: lines along dir that are interior in the
-// other dimension, one-sided at the two extreme ghost points.
+// FirstDerivativeFirstOrder (FirstDerivativeFirstOrder.c:40-100), or with
+// P.par4 FirstDerivativeFourthOrderCentral (d4), on an AoS array with nv
+// values per point: lines along dir that are interior in the other
+// dimension, one-sided at the extreme ghost points.
 __global__ void k_first_deriv(DevParams P, double* __restrict__ Df, const double* __restrict__ f, int dir,
                               int bias, int nv) {
   const int N = dir == 0 ? P.N0 : P.N1, nl = P.ndims == 1 ? 1 : (dir == 0 ? P.N1 : P.N0);
@@ -722,6 +845,11 @@ __global__ void k_first_deriv(DevParams P, double* __restrict__ Df, const double
   int ii = (int)(idx % len) - P.ghosts, l = (int)(idx / len);
   auto at = [&](int i) -> long long { return dir == 0 ? pidx(P, i, l) : pidx(P, l, i); };
   const int mx = bias > 0 ? bias : 0, mn = bias < 0 ? bias : 0;
+  if (P.par4) {
+    for (int v = 0; v < nv; v++)
+      Df[at(ii) * nv + v] = d4<double>(ii, N, P.ghosts, [&](int k) { return f[at(ii + k) * nv + v]; });
+    return;
+  }
   for (int v = 0; v < nv; v++) {
     double r;
     if (ii == -P.ghosts) r = f[at(ii + 1) * nv + v] - f[at(ii) * nv + v];
@@ -905,7 +1033,10 @@ void launch_visc_source(const DevParams& P, const double* U, const double* dxinv
   do_chem = do_chem && P.chem;
   if (do_visc) {
     dim3 grid(nblk(P.N0, 32), nblk(P.N1, 8)), blk(32, 8);
-    if (P.mixed) k_visc_source<true><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
+    if (P.par4) {
+      if (P.mixed) k_visc4_source<true><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
+      else k_visc4_source<false><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
+    } else if (P.mixed) k_visc_source<true><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
     else k_visc_source<false><<<grid, blk, 0, s>>>(P, U, dxinv, imap, tdev, cstage, rhs, do_chem, hnu);
   } else if (do_chem) {
     const unsigned nb = nblk((long long)P.N0 * P.N1, 256);

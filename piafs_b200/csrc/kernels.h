@@ -20,19 +20,25 @@ inline void raise_smem_limit(int bytes) {
 
 // One boundary zone with its index extents resolved (single rank):
 // [is[d], ie[d]) per dimension, ghost slab along `dim`
-// (InitializeBoundaries.c:296-378).
+// (InitializeBoundaries.c:296-378), and its data
+// (InitializeBoundaries.c:106-168): wall or inflow velocity, inflow density,
+// outflow / inflow pressure, and in device memory the Dirichlet state (one
+// value per variable) or the inflow passive scalars (variables 4..nvars-1).
 struct Zone {
   int type, dim, face;
   int is[2], ie[2];
   double vel[2];
+  double rho, pres;
+  const double* val;
 };
 
 #ifdef __CUDACC__
 // Boundary values at ghost point (g0, g1) of zone z (BCPeriodic.c,
-// BCExtrapolate.c, BCSlipWall.c): reads the zone's source point of u (SoA
-// planes) and writes the ghost's variables to out[v * ostride] -- all of
-// them, or for a slip wall the flow variables only (the wall leaves the
-// others untouched).  The periodic source keeps the zone-relative index in
+// BCExtrapolate.c, BCSlipWall.c and the boundaries below): reads the zone's
+// source point of u (SoA planes) and writes the ghost's variables to
+// out[v * ostride] -- all of them, or for the flow boundaries of the
+// Euler / Navier-Stokes models the flow variables (and the passive scalars
+// of an inflow) only; the others stay untouched.  The periodic source keeps the zone-relative index in
 // the other dimension, as the reference does.
 __device__ __forceinline__ void bc_point(const DevParams& P, const Zone& z, const double* u, int g0, int g1,
                                          double* out, long long ostride) {
@@ -47,6 +53,59 @@ __device__ __forceinline__ void bc_point(const DevParams& P, const Zone& z, cons
     src[d] = z.face == 1 ? P.ghosts - 1 - b : Nd - b - 1;
   }
   const long long p2 = pidx(P, src[0], src[1]);
+  if (z.type == BC_DIRICHLET) {        // BCDirichlet.c:26-39
+    for (int v = 0; v < P.nvars; v++) out[v * ostride] = z.val[v];
+    return;
+  }
+  if (z.type == BC_REFLECT) {          // BCReflect.c:27-50
+    for (int v = 0; v < P.nvars; v++) out[v * ostride] = -1.0 * u[v * P.ps + p2];
+    return;
+  }
+  if (z.type >= BC_NOSLIP) {
+    // BCNoslipWall.c:41-78, BCSubsonicInflow.c:41-88, BCSubsonicOutflow.c:41-80,
+    // BCSubsonicAmbivalent.c:46-132, BCSupersonicInflow.c:38-68,
+    // BCSupersonicOutflow.c:41-82: the ghost's density, velocity and pressure
+    // from the mirrored interior point and the zone's data; energy from them
+    // with the boundary gamma; inflows also set the passive scalars, the
+    // others leave them.  The reference has these for 2D only and leaves the
+    // ghosts of other dimensionalities as they are.
+    if (P.ndims != 2) return;
+    const double g = P.bc_gamma, igm1 = 1.0 / (g - 1.0);
+    double rho = 0.0, uv = 0.0, vv = 0.0, e, pr = 0.0;
+    if (z.type != BC_SUP_INFLOW)
+      ns_flowvar(u[p2], u[P.ps + p2], u[2 * P.ps + p2], u[3 * P.ps + p2], g, rho, uv, vv, e, pr);
+    int type = z.type;
+    if (type == BC_SUB_AMBIVALENT) {
+      // inflow or outflow by the sign of the normal velocity at the face,
+      // extrapolated from the first two interior points (BCSubsonicAmbivalent.c:70-86)
+      int a[2] = {g0, g1}, b2[2] = {g0, g1};
+      a[d] = z.face == 1 ? 0 : Nd - 1;
+      b2[d] = z.face == 1 ? 1 : Nd - 2;
+      const long long q1 = pidx(P, a[0], a[1]), q2 = pidx(P, b2[0], b2[1]);
+      double r1, u1, v1, e1, p1, r2, u2, v2, e2, pq2;
+      ns_flowvar(u[q1], u[P.ps + q1], u[2 * P.ps + q1], u[3 * P.ps + q1], g, r1, u1, v1, e1, p1);
+      ns_flowvar(u[q2], u[P.ps + q2], u[2 * P.ps + q2], u[3 * P.ps + q2], g, r2, u2, v2, e2, pq2);
+      const double ub = 1.5 * u1 - 0.5 * u2, vb = 1.5 * v1 - 0.5 * v2;
+      const double nx = (d == 0 ? 1.0 : 0.0) * (double)z.face, ny = (d == 1 ? 1.0 : 0.0) * (double)z.face;
+      type = (ub * nx + vb * ny > 0) ? BC_SUB_INFLOW : BC_SUB_OUTFLOW;
+    }
+    double rg, ug, vg, pg;
+    switch (type) {
+      case BC_NOSLIP: rg = rho; pg = pr; ug = 2.0 * z.vel[0] - uv; vg = 2.0 * z.vel[1] - vv; break;
+      case BC_SUB_INFLOW: rg = z.rho; pg = pr; ug = z.vel[0]; vg = z.vel[1]; break;
+      case BC_SUB_OUTFLOW: rg = rho; pg = z.pres; ug = uv; vg = vv; break;
+      case BC_SUP_INFLOW: rg = z.rho; pg = z.pres; ug = z.vel[0]; vg = z.vel[1]; break;
+      default: rg = rho; pg = pr; ug = uv; vg = vv; break;   // supersonic outflow
+    }
+    out[0] = rg;
+    out[ostride] = rg * ug;
+    out[2 * ostride] = rg * vg;
+    out[3 * ostride] = igm1 * pg + 0.5 * rg * (ug * ug + vg * vg);
+    // the ambivalent zone reads no scalars (BCSubsonicAmbivalent.c:118-127)
+    if ((z.type == BC_SUB_INFLOW || z.type == BC_SUP_INFLOW) && z.val)
+      for (int v = 4; v < P.nvars; v++) out[v * ostride] = z.val[v - 4];
+    return;
+  }
   if (z.type == BC_SLIPWALL) {
     const double g = P.bc_gamma, igm1 = 1.0 / (g - 1.0);
     if (P.ndims == 1) {

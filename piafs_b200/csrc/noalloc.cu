@@ -59,7 +59,8 @@ extern "C" int piafs_gpu_HyperbolicFunction_noalloc(const piafs_gpu_hyp_params* 
   if ((q.model == NS2D) != (q.ndims == 2) || (q.model != NS2D && q.model != EULER1D))
     return nfail(PIAFS_ERR_ARGUMENT, "model does not match ndims");
   if (q.model == NS2D ? q.nvars < 4 : q.nvars < 3) return nfail(PIAFS_ERR_ARGUMENT, "nvars too small for the model");
-  if (q.scheme != WENO5 && q.scheme != CRWENO5) return nfail(PIAFS_ERR_ARGUMENT, "scheme must be WENO5 or CRWENO5");
+  if (q.scheme != WENO5 && q.scheme != CRWENO5 && q.scheme != UPW5)
+    return nfail(PIAFS_ERR_ARGUMENT, "scheme must be WENO5, CRWENO5 or UPW5");
   if (q.upwind < UPW_ROE || q.upwind > UPW_RUSANOV) return nfail(PIAFS_ERR_ARGUMENT, "bad upwinding scheme");
   if (q.weno_type < W_JS || q.weno_type > W_YC) return nfail(PIAFS_ERR_ARGUMENT, "bad WENO weight type");
 
@@ -123,7 +124,7 @@ extern "C" int piafs_gpu_HyperbolicFunction_noalloc(const piafs_gpu_hyp_params* 
   launch_aos_to_soa(u, U, P.npg, P.nvars, P.ps, s);
   for (int d = 0; d < P.ndims; d++) {
     launch_flux(P, U, F, d, s);
-    if (P.scheme == WENO5) launch_weno5(P, U, F, I[0], I[1], I[2], I[3], d, s);
+    if (P.scheme != CRWENO5) launch_weno5(P, U, F, I[0], I[1], I[2], I[3], d, s);
     else launch_crweno(P, U, F, I[0], I[1], I[2], I[3], d, err, s);
     launch_upwind_div(P, U, I[0], I[1], I[2], I[3], dxinv, H, d, d == 0 ? 2 : 3, s);
   }

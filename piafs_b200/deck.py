@@ -99,7 +99,12 @@ class BoundaryZone:
     face: int
     extent: Sequence[float]            # xmin, xmax for each dimension
     wall_velocity: Optional[Sequence[float]] = None   # slip-wall / noslip-wall
-    values: Optional[Sequence[float]] = None          # sponge: the reference state, one value per variable
+    # the zone's data in the order the reference reads it
+    # (InitializeBoundaries.c:106-168): dirichlet / sponge one value per
+    # variable; subsonic-inflow density, velocity, passive scalars;
+    # subsonic-outflow pressure; subsonic-ambivalent density, velocity,
+    # pressure; supersonic-inflow density, velocity, pressure, passive scalars
+    values: Optional[Sequence[float]] = None
 
 
 def write_boundary(path: str, zones: Sequence[BoundaryZone]) -> None:
@@ -115,7 +120,16 @@ def write_boundary(path: str, zones: Sequence[BoundaryZone]) -> None:
                 f.write("  " + " ".join(repr(float(v)) for v in z.values) + "\n")
 
 
-def read_boundary(path: str, ndims: int) -> List[BoundaryZone]:
+def _zone_value_count(bctype: str, ndims: int, nvars: int) -> int:
+    nscalars = nvars - (2 + ndims)
+    return {"dirichlet": nvars, "sponge": nvars, "subsonic-inflow": 1 + ndims + nscalars,
+            "subsonic-outflow": 1, "subsonic-ambivalent": 2 + ndims,
+            "supersonic-inflow": 2 + ndims + nscalars}.get(bctype, 0)
+
+
+def read_boundary(path: str, ndims: int, nvars: int = 0) -> List[BoundaryZone]:
+    """Read ``boundary.inp``; ``nvars`` is needed for the zone types whose data
+    depends on it (dirichlet, sponge and the inflows with passive scalars)."""
     toks = open(path).read().split()
     n = int(toks[0])
     i = 1
@@ -129,7 +143,10 @@ def read_boundary(path: str, ndims: int) -> List[BoundaryZone]:
         if bctype in ("slip-wall", "noslip-wall"):
             wv = [float(t) for t in toks[i:i + ndims]]
             i += ndims
-        zones.append(BoundaryZone(bctype, dim, face, ext, wv))
+        nval = _zone_value_count(bctype, ndims, nvars)
+        vals = [float(t) for t in toks[i:i + nval]] if nval else None
+        i += nval
+        zones.append(BoundaryZone(bctype, dim, face, ext, wv, vals))
     return zones
 
 

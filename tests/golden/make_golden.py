@@ -19,10 +19,14 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from piafs_b200 import cases  # noqa: E402
+from piafs_b200 import cases, deck  # noqa: E402
 
 REF = os.path.join(ROOT, "oracle", "_ref", "PIAFS")
 DT2D = 0.4 / 2048   # CFL 0.4 at 2048^2 (sound speed 1 in the quiescent gas)
+Z = deck.BoundaryZone
+BIG = 1e99
+# free stream rho = 1, u = 0.2, v = 0, p = 1/1.4 in conserved variables
+FREE_02 = [1.0, 0.2, 0.0, (1 / 1.4) / 0.4 + 0.5 * 0.2 * 0.2]
 
 CASES = {
     # the 1D Euler workload itself (N=1024, WENO5, Roe, SSPRK3, 1000 steps)
@@ -61,6 +65,46 @@ CASES = {
     "ns2d_shear_weno5_llf_sponge_40x32": (cases.ns2d_shear_layer, dict(
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5",
         sponge=dict(dim=1, face=-1, extent=[-1e9, 1e9, 0.0, 0.25], values=[1.0, 0.0, 0.0, 2.5]))),
+    # the reference's remaining boundary conditions, fourth-order viscous
+    # derivatives and the fifth-order upwind scheme, as its wall, inflow and
+    # outflow examples use them (LidDrivenCavity, FlatPlateLaminar,
+    # Uniform_Subsonic_Jet, Uniform_Supersonic_Jet)
+    "ns2d_cavity_noslip_upw5_par4_32x32": (cases.ns2d_channel, dict(
+        zones=[Z("noslip-wall", 0, 1, [0, 0, -BIG, BIG], [0.0, 0.0]),
+               Z("noslip-wall", 0, -1, [0, 0, -BIG, BIG], [0.0, 0.0]),
+               Z("noslip-wall", 1, 1, [-BIG, BIG, 0, 0], [0.0, 0.0]),
+               Z("noslip-wall", 1, -1, [-BIG, BIG, 0, 0], [0.1, 0.0])],
+        N=32, n_iter=100, dt=5e-3, scheme="upw5", Re=100.0, flow=(0.0, 0.0), bump=0.02)),
+    "ns2d_flatplate_subsonic_weno5_par4_48x24": (cases.ns2d_channel, dict(
+        zones=[Z("slip-wall", 1, 1, [0.0, 0.25, 0, 0], [0.0, 0.0]),
+               Z("noslip-wall", 1, 1, [0.25, BIG, 0, 0], [0.0, 0.0]),
+               Z("subsonic-outflow", 1, -1, [-BIG, BIG, 0, 0], values=[1 / 1.4]),
+               Z("subsonic-inflow", 0, 1, [0, 0, -BIG, BIG], values=[1.0, 0.3, 0.0]),
+               Z("subsonic-outflow", 0, -1, [0, 0, -BIG, BIG], values=[1 / 1.4])],
+        N=48, NY=24, L=(1.0, 0.5), n_iter=60, dt=2e-3, bump_at=(0.5, 0.25))),
+    "ns2d_ambivalent_dirichlet_weno5_llf_40x32": (cases.ns2d_channel, dict(
+        zones=[Z("subsonic-ambivalent", 0, 1, [0, 0, -BIG, BIG], values=[1.0, 0.2, 0.0, 1 / 1.4]),
+               Z("subsonic-ambivalent", 0, -1, [0, 0, -BIG, BIG], values=[1.0, 0.2, 0.0, 1 / 1.4]),
+               Z("dirichlet", 1, 1, [-BIG, BIG, 0, 0], values=FREE_02),
+               Z("dirichlet", 1, -1, [-BIG, BIG, 0, 0], values=FREE_02)],
+        N=40, NY=32, n_iter=60, dt=2e-3, upwinding="llf-char", Re=500.0, par="2", time_scheme_type="ssprk3",
+        flow=(0.2, 0.0))),
+    "ns2d_chem_subsonic_jet_weno5char_rf_par4_24x32": (cases.ns2d_photochem_beam, dict(
+        zones=[Z("periodic", 0, 1, [0, 0, -BIG, BIG]), Z("periodic", 0, -1, [0, 0, -BIG, BIG]),
+               Z("subsonic-inflow", 1, 1, [-BIG, BIG, 0, 0], values=[1.0, 0.0, 0.05, 1.0, 0.01, 0, 0, 0, 0, 0]),
+               Z("extrapolate", 1, -1, [-BIG, BIG, 0, 0])],
+        N=24, NY=32, n_iter=60, dt=1e-3, scheme="weno5", upwinding="rf-char", interp="characteristic", par="4",
+        flow=(0.0, 0.05))),
+    "ns2d_chem_supersonic_jet_weno5_rf_24x32": (cases.ns2d_photochem_beam, dict(
+        zones=[Z("periodic", 0, 1, [0, 0, -BIG, BIG]), Z("periodic", 0, -1, [0, 0, -BIG, BIG]),
+               Z("supersonic-inflow", 1, 1, [-BIG, BIG, 0, 0],
+                 values=[1.0, 0.0, 1.5, 1 / cases.chem_gamma(), 1.0, 0.005, 0, 0, 0, 0, 0]),
+               Z("supersonic-outflow", 1, -1, [-BIG, BIG, 0, 0])],
+        N=24, NY=32, n_iter=60, dt=1e-3, scheme="weno5", upwinding="rf-char", flow=(0.0, 1.5))),
+    "euler1d_weno5_roe_dirichlet_n128": (cases.euler1d_density_wave, dict(
+        zones=[Z("dirichlet", 0, 1, [0.0, 0.0], values=[1.0, 1.0, 1.0 / 0.4 + 0.5]),
+               Z("extrapolate", 0, -1, [0.0, 0.0])],
+        N=128, n_iter=100, dt=1e-3)),
     "ns2d_shear_crweno5_llf_re200_48x40": (cases.ns2d_shear_layer, dict(N=48, NY=40, n_iter=30, dt=2e-3)),
     "ns2d_shear_weno5_roe_re200_40x32": (cases.ns2d_shear_layer, dict(
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", upwinding="roe")),

@@ -24,6 +24,26 @@ def test_boundary_roundtrip(tmp_path):
     assert back[1].face == -1 and back[1].wall_velocity == [0.0, 0.25]
 
 
+def test_boundary_roundtrip_flow_zones(tmp_path):
+    # zone data as InitializeBoundaries.c:106-168 reads it, 2D with 11 variables
+    p = tmp_path / "boundary.inp"
+    big = 1e99
+    sc = [1.0, 0.005, 0, 0, 0, 0, 0]
+    z = [deck.BoundaryZone("subsonic-inflow", 1, 1, [-big, big, 0, 0], values=[1.0, 0.0, 0.3] + sc),
+         deck.BoundaryZone("subsonic-outflow", 1, -1, [-big, big, 0, 0], values=[0.7]),
+         deck.BoundaryZone("noslip-wall", 0, 1, [0, 0, -big, big], [0.0, 0.1]),
+         deck.BoundaryZone("supersonic-inflow", 0, -1, [0, 0, -big, big], values=[2.0, -1.5, 0.0, 3.0] + sc),
+         deck.BoundaryZone("subsonic-ambivalent", 0, 1, [0, 0, -big, big], values=[1.0, 0.2, 0.0, 0.7]),
+         deck.BoundaryZone("supersonic-outflow", 0, -1, [0, 0, -big, big]),
+         deck.BoundaryZone("dirichlet", 1, 1, [-big, big, 0, 0], values=list(range(11)))]
+    deck.write_boundary(str(p), z)
+    back = deck.read_boundary(str(p), 2, nvars=11)
+    assert [b.bctype for b in back] == [b.bctype for b in z]
+    for a, b in zip(back, z):
+        assert a.values == (None if b.values is None else [float(v) for v in b.values])
+        assert a.wall_velocity == b.wall_velocity
+
+
 def test_op_file_roundtrip(tmp_path):
     x, y = np.linspace(0, 1, 5), np.linspace(0, 2, 3)
     u = np.arange(15 * 4, dtype=np.float64).reshape(15, 4)

@@ -15,7 +15,7 @@ from oracle import oracle
 from piafs_b200 import deck
 
 
-@pytest.mark.parametrize("name", golden_cases(components_only=True, no_sponge=True))
+@pytest.mark.parametrize("name", golden_cases(oracle_scope=True))
 def test_oracle_matches_reference_bitwise(name):
     d = os.path.join(GOLDEN, name)
     case = oracle.load(d)
