@@ -66,6 +66,7 @@ struct piafs_gpu_sim {
   std::vector<SpongeDev> sponges;
   double* sponge_buf = nullptr;
   double* zone_buf = nullptr;              // boundary zones' values (Zone::val)
+  double* crwchar = nullptr;               // block rows of the characteristic CRWENO5 line solves
   // host mirror of the clock
   double t = 0.0;
   int iter = 0;
@@ -98,6 +99,7 @@ static void free_sim(piafs_gpu_sim* s) {
   cudaFree(s->hnu);
   cudaFree(s->sponge_buf);
   cudaFree(s->zone_buf);
+  cudaFree(s->crwchar);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -111,6 +113,13 @@ static void free_sim(piafs_gpu_sim* s) {
 static void enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* const* I, cudaEvent_t* ev, int* k) {
   const DevParams& P = s->P;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[++*k], s->stream); };
+  if (P.scheme == CRWENO5 && P.char_interp) {
+    launch_flux(P, U, s->fC, d, s->stream);
+    mark();
+    launch_crweno_char(P, U, s->fC, I[0], I[1], I[2], I[3], d, s->crwchar, s->err, s->stream);
+    mark();
+    return;
+  }
   if (d == 1 && s->ut) {
     launch_transpose(P, U, s->ut, s->stream);
     launch_flux(P, s->ut, s->fC, 1, s->stream);
@@ -277,7 +286,9 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   // column-strided kernels instead in the FP64 path; the mixed path has only
   // the transposed one)
   const char* noyt = std::getenv("PIAFS_GPU_NO_YTRANSPOSE");
-  if (e == cudaSuccess && P.ndims == 2 && P.scheme == CRWENO5 && (P.mixed || !(noyt && noyt[0] == '1'))) {
+  if (e == cudaSuccess && P.scheme == CRWENO5 && P.char_interp) e = alloc(&s->crwchar, crweno_char_scratch(P));
+  if (e == cudaSuccess && P.ndims == 2 && P.scheme == CRWENO5 && !P.char_interp &&
+      (P.mixed || !(noyt && noyt[0] == '1'))) {
     e = alloc(&s->ut, planes);
     s->PT = transposed_params(P);
   }
@@ -638,7 +649,10 @@ int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* s, double* fI, const doubl
   P.mixed = 0;   // operator-level entry points are FP64
   to_soa(s, u, s->scratch);
   to_soa(s, fC, s->fC);
-  if (P.scheme != CRWENO5 && P.char_interp)
+  if (P.scheme == CRWENO5 && P.char_interp)
+    launch_crweno_char(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->crwchar,
+                       s->err, s->stream);
+  else if (P.scheme != CRWENO5 && P.char_interp)
     launch_weno5_char(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);
   else if (P.scheme != CRWENO5)
     launch_weno5(P, s->scratch, s->fC, s->iface[0], s->iface[1], s->iface[2], s->iface[3], dir, s->stream);

@@ -304,12 +304,9 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
     err = "hyp_space_scheme " + d.hyp_space_scheme + " is not on the GPU path (weno5, crweno5, upw5)";
     return PIAFS_ERR_UNSUPPORTED;
   }
-  // characteristic interpolation: the explicit schemes only (CRWENO5 on
-  // characteristic variables needs the block-tridiagonal solver, blocktridiagLU.c)
-  if (d.hyp_interp_type != "components" && d.nvars > 1 &&
-      !(d.hyp_interp_type == "characteristic" && d.hyp_space_scheme != "crweno5")) {
-    err = "hyp_interp_type " + d.hyp_interp_type + " with " + d.hyp_space_scheme +
-          " is not on the GPU path (components; characteristic with weno5 or upw5)";
+  // interpolation on components or on characteristic variables
+  if (d.hyp_interp_type != "components" && d.hyp_interp_type != "characteristic" && d.nvars > 1) {
+    err = "hyp_interp_type " + d.hyp_interp_type + " is not a PIAFS interpolation type (components, characteristic)";
     return PIAFS_ERR_UNSUPPORTED;
   }
   if (d.ghosts < 3) { err = "WENO5/CRWENO5 need ghost >= 3"; return PIAFS_ERR_INPUT; }
@@ -360,6 +357,14 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
   // it, so its walls see the zero of a calloc'd boundary object.
   d.bc_gamma = d.model == "navierstokes2d" ? d.gamma : 0.0;
   const int nflow = d.model == "navierstokes2d" ? 4 : 3;
+  // CRWENO5 on characteristic variables with photochemistry: the reference's
+  // 11x11 block inverses (_MatrixInvert_, no pivoting) meet zero pivots on the
+  // species rows and its solution is not finite
+  if (d.hyp_space_scheme == "crweno5" && d.hyp_interp_type == "characteristic" && d.include_chem == "yes") {
+    err = "crweno5 with hyp_interp_type characteristic and photochemistry: the reference's block solve is "
+          "singular (use components)";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
   if (d.include_chem == "yes") {
     if (int r = setup_chemistry(dir, d, nflow, err)) return r;
     // PhysicsOutput: Euler1DWriteChem always (Euler1DInitialize.c:144-145),

@@ -161,6 +161,13 @@ void launch_weno5(const DevParams& P, const double* U, const double* F, void* uL
 int crweno_rows_per_thread(int N);
 int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
                   int dir, int* err, cudaStream_t s);
+// CRWENO5 on characteristic variables (crweno_char.cu; 1D Euler and 2D
+// Navier-Stokes without chemistry, FP64): all four interface arrays of
+// direction dir; scratch holds crweno_char_scratch(P) doubles; *err is set on
+// a zero pivot of a block inverse
+long long crweno_char_scratch(const DevParams& P);
+void launch_crweno_char(const DevParams& P, const double* U, const double* F, double* uL, double* uR, double* fL,
+                        double* fR, int dir, double* scratch, int* err, cudaStream_t s);
 // mode 0: rhs = -hyp_x; 1: rhs = -((-rhs) + hyp_y); 2: out = hyp_x; 3: out += hyp_y
 // (interface arrays as written by launch_weno5 / launch_crweno; the mixed
 // variant covers the 1D x direction, 2D goes through launch_upwind_div2d)

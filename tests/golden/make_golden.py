@@ -59,6 +59,17 @@ CASES = {
         N=40, NY=32, n_iter=30, dt=2e-3, scheme="weno5", interp="characteristic")),
     "ns2d_chem_weno5char_rf_32x24": (cases.ns2d_photochem_beam, dict(
         N=32, NY=24, n_iter=60, dt=DT2D, scheme="weno5", upwinding="rf-char", interp="characteristic")),
+    # CRWENO5 on characteristic variables (block-tridiagonal line solves;
+    # models without photochemistry, where the reference's blocks invert)
+    "euler1d_crweno5char_roe_n128": (cases.euler1d_density_wave, dict(
+        N=128, n_iter=100, dt=2e-3, scheme="crweno5", interp="characteristic")),
+    "euler1d_crweno5char_llf_mapped_n97": (cases.euler1d_density_wave, dict(
+        N=97, n_iter=60, dt=2e-3, amp=0.3, scheme="crweno5", upwinding="llf-char", weno={"mapped": 1},
+        interp="characteristic")),
+    "ns2d_shear_crweno5char_llf_re200_40x32": (cases.ns2d_shear_layer, dict(
+        N=40, NY=32, n_iter=30, dt=2e-3, interp="characteristic")),
+    "ns2d_shear_crweno5char_rf_borges_36x28": (cases.ns2d_shear_layer, dict(
+        N=36, NY=28, n_iter=30, dt=2e-3, upwinding="rf-char", weno={"borges": 1}, interp="characteristic")),
     # sponge zones (BCSponge.c): relaxation towards a reference state in a box
     "euler1d_weno5_roe_sponge_n200": (cases.euler1d_density_wave, dict(
         N=200, n_iter=100, dt=1e-3, sponge=dict(dim=0, face=1, extent=[0.7, 1.0], values=[1.0, 1.0, 3.0]))),

@@ -99,10 +99,11 @@ def test_species_files_match_the_reference(tmp_path):
 
 
 def test_characteristic_interpolation_refusals(tmp_path):
-    """WENO5 on characteristic variables runs in FP64 single simulations; the
-    mixed-precision path and batched members refuse it, as the solver refuses
-    CRWENO5 on characteristic variables (the block-tridiagonal solve); batched
-    members refuse sponge zones too."""
+    """Interpolation on characteristic variables runs in FP64 single
+    simulations; the mixed-precision path and batched members refuse it, and
+    CRWENO5 on characteristic variables with photochemistry is refused (the
+    reference's block inverses are singular there); batched members refuse
+    sponge zones too."""
     from piafs_b200 import Batch, PiafsError
     d = os.path.join(GOLDEN, "ns2d_chem_weno5char_rf_32x24")
     with pytest.raises(PiafsError) as ex:
@@ -115,9 +116,12 @@ def test_characteristic_interpolation_refusals(tmp_path):
         b.add(os.path.join(GOLDEN, "euler1d_weno5_roe_sponge_n200"))
     assert ex.value.code == 3
     c = str(tmp_path / "crwchar")
-    cases.ns2d_shear_layer(c, N=24, NY=20, n_iter=2, interp="characteristic")
+    cases.ns2d_photochem_beam(c, N=24, NY=20, n_iter=2, interp="characteristic")
     with pytest.raises(PiafsError) as ex:
         Simulation(c)
+    assert ex.value.code == 3
+    with pytest.raises(PiafsError) as ex:
+        Simulation(os.path.join(GOLDEN, "ns2d_shear_crweno5char_llf_re200_40x32"), precision="mixed")
     assert ex.value.code == 3
 
 
