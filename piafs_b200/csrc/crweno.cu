@@ -22,14 +22,25 @@
 //   * every row is recovered from its two separators and the results are
 //     staged in shared memory so that the x-direction stores are coalesced.
 //
+// Lines longer than one CTA serves (T M + 1 interfaces, 4097 at M = 8) run as
+// a thread-block cluster of up to 8 CTAs per line (CL): each CTA reduces a
+// segment of consecutive chunks, the separator system of the whole line is
+// solved by the same parallel cyclic reduction across the cluster, each step
+// reading the neighbours' rows from the other CTAs' shared memory
+// (distributed shared memory) between cluster barriers, and every CTA
+// recovers and stores its own segment.
+//
 // Rows 0 and N are the WENO5 rows with the WENO5 optimal weights (physical
 // boundaries, also on periodic domains, Interp1PrimFifthOrderCRWENO.c:164-175);
 // they are computed directly and folded into rows 1 and N-1.  Rows past N-1
 // are identity rows.  Divisions are reciprocals by Newton-Raphson refinement
 // (rcp_nr), so results agree with the reference to rounding, not bit for bit.
+#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "kernels.h"
+
+namespace cg = cooperative_groups;
 
 namespace piafs {
 
@@ -117,7 +128,9 @@ __device__ __forceinline__ int stg(int i) { return i + (i >> 4); }
 // otherwise
 __host__ __device__ constexpr int crweno_max_threads(int M) { return M == 8 ? 512 : 256; }
 
-template <int M, int DIR, int WT, bool MX>
+// CL: the line is shared by the CTAs of a cluster (blockIdx.x = line x
+// cluster size + rank), the separator index of a thread is rank x Pt + k.
+template <int M, int DIR, int WT, bool MX, bool CL = false>
 __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     k_crweno_pair(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
                   void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
@@ -129,8 +142,31 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
   double* pc = sm;               // PCR rows, [2 buffers][2 biases][a, c, d][Pt]
   double* tp = sm + 12 * Pt;     // last-row coefficients per chunk, [2][3][Pt]
   double* sy = sm + 18 * Pt;     // separator values, [2][Pt]
-  double* so = sm + 20 * Pt;     // output staging, [2][stg(N) + 1]
-  const int line = blockIdx.x, v = blockIdx.y;
+  double* so = sm + 20 * Pt;     // output staging, [2][stg(rows of the segment) + 1]
+  // cluster: rank of this CTA, separators of the line, first row of the segment
+  int rank = 0, ncta = 1;
+  if constexpr (CL) {
+    rank = (int)cg::this_cluster().block_rank();
+    ncta = (int)cg::this_cluster().num_blocks();
+  }
+  const int K = rank * Pt + k, Ptot = ncta * Pt;
+  const int rowbase = rank * Pt * M;
+  auto sync = [&]() {
+    if constexpr (CL) cg::this_cluster().sync();
+    else __syncthreads();
+  };
+  // a shared-memory value of separator index j of the line (this CTA or,
+  // in a cluster, the CTA that owns it)
+  auto at = [&](double* arr, int j) -> double {
+    if constexpr (CL) {
+      const int r = j / Pt;
+      if (r != rank) return *cg::this_cluster().map_shared_rank(arr + (j - r * Pt), r);
+      return arr[j - r * Pt];
+    } else {
+      return arr[j];
+    }
+  };
+  const int line = CL ? (int)blockIdx.x / ncta : (int)blockIdx.x, v = blockIdx.y;
   const bool isF = blockIdx.z != 0;
   const int N = DIR == 0 ? P.N0 : P.N1;
   const long long st = DIR == 0 ? 1 : P.W0;
@@ -140,8 +176,8 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
   const double* src = (isF ? F : U) + (long long)v * P.ps + base;
   O* oL = (O*)(isF ? fL : uL) + (long long)v * P.pis + ibase;
   O* oR = (O*)(isF ? fR : uR) + (long long)v * P.pis + ibase;
-  const int s = 1 + k * M;          // separator row (interface) of this thread
-  const int kN = (N - 2) / M;       // thread owning row N-1
+  const int s = 1 + K * M;          // separator row (interface) of this thread
+  const int kN = (N - 2) / M;       // separator index owning row N-1
   const R eps = R(4) * (R)P.eps;   // with the smoothness indicators at 4x (below)
   const double ref = MX ? src[0] : 0.0;
 
@@ -154,11 +190,11 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
   }
   R x0[2] = {R(0), R(0)}, xN[2] = {R(0), R(0)};
   if (MX) {
-    if (k == 0) { x0[0] = crw_edge_f(P, src, st, 0, 1, ref); x0[1] = crw_edge_f(P, src, st, 0, -1, ref); }
-    if (k == kN) { xN[0] = crw_edge_f(P, src, st, N, 1, ref); xN[1] = crw_edge_f(P, src, st, N, -1, ref); }
+    if (K == 0) { x0[0] = crw_edge_f(P, src, st, 0, 1, ref); x0[1] = crw_edge_f(P, src, st, 0, -1, ref); }
+    if (K == kN) { xN[0] = crw_edge_f(P, src, st, N, 1, ref); xN[1] = crw_edge_f(P, src, st, N, -1, ref); }
   } else {
-    if (k == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
-    if (k == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
+    if (K == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
+    if (K == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
   }
 
   // smoothness indicators of the windows centred at cells s-2+t (t = 0..M+2),
@@ -247,7 +283,7 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     tp[(q * 3 + 1) * Pt + k] = cg[q][M - 1];
     tp[(q * 3 + 2) * Pt + k] = rh[q][M - 1];
   }
-  __syncthreads();
+  sync();
 
   // ---- separator equations As x_{s-1} + Bs X_k + Cs x_{s+1} = Rs, with
   //      x_{s-1} from the previous chunk's last row and x_{s+1} from row 1
@@ -255,7 +291,10 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     double alp = 0.0, gap = 0.0, rhp = 0.0;
-    if (k > 0) { alp = tp[(q * 3 + 0) * Pt + k - 1]; gap = tp[(q * 3 + 1) * Pt + k - 1]; rhp = tp[(q * 3 + 2) * Pt + k - 1]; }
+    if (K > 0) {
+      alp = at(tp + (q * 3 + 0) * Pt, K - 1); gap = at(tp + (q * 3 + 1) * Pt, K - 1);
+      rhp = at(tp + (q * 3 + 2) * Pt, K - 1);
+    }
     const double b = Bs[q] - As[q] * gap - Cs[q] * al[q][1];
     bad |= (b == 0.0);
     const double rb = rcp_nr(b);
@@ -267,17 +306,23 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     pc[(q * 3 + 2) * Pt + k] = d[q];
   }
   if (bad) atomicOr(err, 1);
-  __syncthreads();
+  sync();
   // ---- parallel cyclic reduction on unit-diagonal rows a x_{k-dl} + x_k + c x_{k+dl} = d
   int buf = 0;
-  for (int dl = 1; dl < Pt; dl <<= 1) {
-    const double* cur = pc + buf * 6 * Pt;
+  for (int dl = 1; dl < Ptot; dl <<= 1) {
+    double* cur = pc + buf * 6 * Pt;
     double* nxt = pc + (buf ^ 1) * 6 * Pt;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       double am = 0.0, cm = 0.0, dm = 0.0, ap = 0.0, cp = 0.0, dp = 0.0;
-      if (k - dl >= 0) { am = cur[(q * 3 + 0) * Pt + k - dl]; cm = cur[(q * 3 + 1) * Pt + k - dl]; dm = cur[(q * 3 + 2) * Pt + k - dl]; }
-      if (k + dl < Pt) { ap = cur[(q * 3 + 0) * Pt + k + dl]; cp = cur[(q * 3 + 1) * Pt + k + dl]; dp = cur[(q * 3 + 2) * Pt + k + dl]; }
+      if (K - dl >= 0) {
+        am = at(cur + (q * 3 + 0) * Pt, K - dl); cm = at(cur + (q * 3 + 1) * Pt, K - dl);
+        dm = at(cur + (q * 3 + 2) * Pt, K - dl);
+      }
+      if (K + dl < Ptot) {
+        ap = at(cur + (q * 3 + 0) * Pt, K + dl); cp = at(cur + (q * 3 + 1) * Pt, K + dl);
+        dp = at(cur + (q * 3 + 2) * Pt, K + dl);
+      }
       const double bn = 1.0 - a[q] * cm - cq[q] * ap;
       const double rb = rcp_nr(bn);
       const double an = -(a[q] * am) * rb, cn = -(cq[q] * cp) * rb;
@@ -288,31 +333,63 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
       nxt[(q * 3 + 2) * Pt + k] = d[q];
     }
     buf ^= 1;
-    __syncthreads();
+    sync();
   }
   sy[k] = d[0];
   sy[Pt + k] = d[1];
-  __syncthreads();
+  sync();
 
   // ---- recover every row
+  if constexpr (!CL) {
 #pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const double Xk = d[q];
-    const double Xn = k + 1 < Pt ? sy[q * Pt + k + 1] : 0.0;
-    double* o = so + q * (stg(N) + 1);
-    if (s <= N - 1) o[stg(s)] = Xk;
+    for (int q = 0; q < 2; q++) {
+      const double Xk = d[q];
+      const double Xn = k + 1 < Pt ? sy[q * Pt + k + 1] : 0.0;
+      double* o = so + q * (stg(N) + 1);
+      if (s <= N - 1) o[stg(s)] = Xk;
 #pragma unroll
-    for (int r = 1; r < M; r++) {
-      const int i = s + r;
-      if (i <= N - 1) o[stg(i)] = rh[q][r] - al[q][r] * Xk - cg[q][r] * Xn;
+      for (int r = 1; r < M; r++) {
+        const int i = s + r;
+        if (i <= N - 1) o[stg(i)] = rh[q][r] - al[q][r] * Xk - cg[q][r] * Xn;
+      }
+      if (k == 0) o[0] = x0[q];
+      if (k == kN) o[stg(N)] = xN[q];
     }
-    if (k == 0) o[0] = x0[q];
-    if (k == kN) o[stg(N)] = xN[q];
-  }
-  __syncthreads();
-  for (int i = k; i <= N; i += Pt) {
-    oL[i * ist] = (O)so[stg(i)];
-    oR[i * ist] = (O)so[stg(N) + 1 + stg(i)];
+    __syncthreads();
+    for (int i = k; i <= N; i += Pt) {
+      oL[i * ist] = (O)so[stg(i)];
+      oR[i * ist] = (O)so[stg(N) + 1 + stg(i)];
+    }
+  } else {
+    // staged at the row's index in this CTA's segment
+    const int nst = min(N, rowbase + Pt * M + 1) - rowbase;   // last staged row of the segment
+    double Xn2[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) Xn2[q] = K + 1 < Ptot ? at(sy + q * Pt, K + 1) : 0.0;
+    sync();     // the last reads of other CTAs' shared memory are done
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const double Xk = d[q];
+      const double Xn = Xn2[q];
+      double* o = so + q * (stg(nst) + 1);
+      if (s <= N - 1) o[stg(s - rowbase)] = Xk;
+#pragma unroll
+      for (int r = 1; r < M; r++) {
+        const int i = s + r;
+        if (i <= N - 1) o[stg(i - rowbase)] = rh[q][r] - al[q][r] * Xk - cg[q][r] * Xn;
+      }
+      if (K == 0) o[0] = x0[q];
+      if (K == kN) o[stg(N - rowbase)] = xN[q];
+    }
+    __syncthreads();
+    // rows of this segment: [rowbase + 1, rowbase + Pt M] within [1, N - 1],
+    // with row 0 in the first segment and row N in the segment holding N - 1
+    const int lo = rank == 0 ? 0 : rowbase + 1;
+    const int hi = (kN / Pt == rank) ? N : min(N - 1, rowbase + Pt * M);
+    for (int i = lo + k; i <= hi; i += Pt) {
+      oL[i * ist] = (O)so[stg(i - rowbase)];
+      oR[i * ist] = (O)so[stg(nst) + 1 + stg(i - rowbase)];
+    }
   }
 }
 
@@ -328,13 +405,58 @@ int crweno_rows_per_thread(int N) {
   return -1;
 }
 
+// CTAs per line: 1 while one CTA serves the line, else the cluster size at
+// M = 8 and 512 threads per CTA (at most 8, the portable cluster size: lines
+// of up to 32769 interfaces); -1 beyond
+int crweno_cluster_size(int N) {
+  if (crweno_rows_per_thread(N) > 0) return 1;
+  constexpr int per_cta = 8 * crweno_max_threads(8);
+  const int n = (N - 1 + per_cta - 1) / per_cta;
+  return n <= 8 ? n : -1;
+}
+
 namespace {
+
+// a line shared by a cluster of CTAs (M = 8): the separators split evenly,
+// each CTA staging its segment
+template <int DIR, int WT, bool MX>
+void crweno_launch_cluster(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
+                           void* fR, int* err, int ncta, cudaStream_t s) {
+  constexpr int M = 8;
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const int nlines = DIR == 0 ? P.N1 : P.N0;
+  const int chunks = (N - 1 + M - 1) / M;
+  int Pt = (chunks + ncta - 1) / ncta;
+  Pt = ((Pt + 31) / 32) * 32;
+  const int seg = Pt * M + 1;
+  const size_t smem = (size_t)(20 * Pt + 2 * (seg + (seg >> 4) + 1)) * sizeof(double);
+  constexpr int T = crweno_max_threads(M);
+  raise_smem_limit<k_crweno_pair<M, DIR, WT, MX, true>>(
+      (20 * T + 2 * (T * M + 1 + ((T * M + 1) >> 4) + 1)) * (int)sizeof(double));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nlines * ncta), (unsigned)P.nvars, 2);
+  cfg.blockDim = dim3((unsigned)Pt, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)ncta;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_crweno_pair<M, DIR, WT, MX, true>, P, U, F, uL, uR, fL, fR, err);
+}
 
 template <int M, int DIR, int WT, bool MX>
 void crweno_launch(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
                    int* err, cudaStream_t s) {
   const int N = DIR == 0 ? P.N0 : P.N1;
   const int nlines = DIR == 0 ? P.N1 : P.N0;
+  if constexpr (M == 8) {
+    const int ncta = crweno_cluster_size(N);
+    if (ncta > 1) return crweno_launch_cluster<DIR, WT, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+  }
   int Pt = (N - 1 + M - 1) / M;
   Pt = ((Pt + 31) / 32) * 32;
   const size_t smem = (size_t)(20 * Pt + 2 * (N + (N >> 4) + 1)) * sizeof(double);
@@ -374,6 +496,10 @@ int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL
                   int dir, int* err, cudaStream_t s) {
   const int N = dir == 0 ? P.N0 : P.N1;
   if (P.mixed && dir != 0) return -1;
+  if (crweno_cluster_size(N) > 1) {
+    crweno_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s);
+    return 0;
+  }
   switch (crweno_rows_per_thread(N)) {
     case 2: crweno_launch_m<2>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
     case 4: crweno_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s); break;

@@ -586,8 +586,8 @@ int make_params(const Deck& d, DevParams& P, std::string& err) {
   P.dt = d.dt;
   if (P.scheme == CRWENO5) {
     for (int k = 0; k < d.ndims; k++) {
-      if (crweno_rows_per_thread(d.size[k]) < 0 || d.size[k] < 3) {
-        err = "crweno5 lines of " + std::to_string(d.size[k]) + " points are outside the GPU path (3..4097)";
+      if (crweno_cluster_size(d.size[k]) < 0 || d.size[k] < 3) {
+        err = "crweno5 lines of " + std::to_string(d.size[k]) + " points are outside the GPU path (3..32769)";
         return PIAFS_ERR_UNSUPPORTED;
       }
     }

@@ -159,6 +159,9 @@ void launch_weno5(const DevParams& P, const double* U, const double* F, void* uL
 // interface arrays hold doubles, or floats relative to each line's first
 // value when P.mixed (x-direction lines only).
 int crweno_rows_per_thread(int N);
+// CTAs per line (a thread-block cluster beyond one CTA's 4097 interfaces);
+// -1 if a line is too long
+int crweno_cluster_size(int N);
 int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
                   int dir, int* err, cudaStream_t s);
 // CRWENO5 on characteristic variables (crweno_char.cu; 1D Euler and 2D

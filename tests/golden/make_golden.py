@@ -70,6 +70,15 @@ CASES = {
         N=40, NY=32, n_iter=30, dt=2e-3, interp="characteristic")),
     "ns2d_shear_crweno5char_rf_borges_36x28": (cases.ns2d_shear_layer, dict(
         N=36, NY=28, n_iter=30, dt=2e-3, upwinding="rf-char", weno={"borges": 1}, interp="characteristic")),
+    # CRWENO5 lines longer than one CTA serves (thread-block clusters of 2-5
+    # CTAs per line), 1D and 2D (long x lines; long y lines, the transposed pass)
+    "euler1d_crweno5_roe_n6000": (cases.euler1d_density_wave, dict(N=6000, n_iter=100, dt=2e-5, scheme="crweno5")),
+    "euler1d_crweno5_llf_yc_n20000": (cases.euler1d_density_wave, dict(
+        N=20000, n_iter=60, dt=5e-6, scheme="crweno5", upwinding="llf-char", weno={"yc": 1})),
+    "ns2d_shear_crweno5_llf_inviscid_4200x4": (cases.ns2d_shear_layer, dict(
+        N=4200, NY=4, n_iter=20, dt=4e-5, Re=-1.0)),
+    "ns2d_shear_crweno5_rf_inviscid_4x4500": (cases.ns2d_shear_layer, dict(
+        N=4, NY=4500, n_iter=20, dt=4e-5, Re=-1.0, upwinding="rf-char")),
     # sponge zones (BCSponge.c): relaxation towards a reference state in a box
     "euler1d_weno5_roe_sponge_n200": (cases.euler1d_density_wave, dict(
         N=200, n_iter=100, dt=1e-3, sponge=dict(dim=0, face=1, extent=[0.7, 1.0], values=[1.0, 1.0, 3.0]))),
