@@ -51,7 +51,7 @@ CPU_SAMPLE_N = 512                          # sample grid of the CPU arms
 # chunks from the initial state keep every timed step a finite step of the
 # workload (and the mixed-precision error a comparison of smooth states).
 def chunk_steps(n):
-    return 12 if n <= 2048 else 4
+    return 12 if n <= 2048 else 4 if n <= 4096 else 2
 
 
 def parse():
