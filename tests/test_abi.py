@@ -48,6 +48,23 @@ def test_unsupported_options_are_rejected(tmp_path):
     assert lib.piafs_gpu_create(str(d).encode(), 0, ctypes.byref(h)) == 3
 
 
+def test_line_length_and_singular_options_are_rejected(tmp_path):
+    """Host-side checks before any device call: CRWENO5 lines beyond a
+    cluster of 8 CTAs (32769 interfaces) and CRWENO5 on characteristic
+    variables with photochemistry (the reference's block solve is singular)."""
+    from piafs_b200 import cases
+    lib = piafs_b200.load_library()
+    h = ctypes.c_void_p()
+    d = tmp_path / "long"
+    cases.euler1d_density_wave(str(d), N=40000, n_iter=1, scheme="crweno5")
+    assert lib.piafs_gpu_create(str(d).encode(), 0, ctypes.byref(h)) == 3
+    assert b"32769" in lib.piafs_gpu_last_error()
+    c = tmp_path / "chem"
+    cases.ns2d_photochem_beam(str(c), N=16, NY=12, n_iter=1, interp="characteristic")
+    assert lib.piafs_gpu_create(str(c).encode(), 0, ctypes.byref(h)) == 3
+    assert b"singular" in lib.piafs_gpu_last_error()
+
+
 def test_cli_binary_is_built():
     assert os.access(piafs_b200.CLI_PATH, os.X_OK)
 
