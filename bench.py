@@ -423,11 +423,24 @@ def serving_bench(a):
 
 
 # --------------------------------------------------------------------- main
+def relaunch_under_torchrun(a):
+    """--gpus N > 1 started as a plain process: run the same command as N
+    ranks (one per GPU) under torch.distributed.run and return its status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={a.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", os.environ.get("MASTER_PORT", "29533"),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch_under_torchrun(a)
+    if a.impl == "gpu" and world != a.gpus:
+        sys.exit(f"bench.py: --gpus {a.gpus} but {world} rank(s) were launched")
     n_gpus = max(world, 1)
     metric = "pt-stage updates/s"
 

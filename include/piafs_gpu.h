@@ -289,20 +289,25 @@ int piafs_gpu_reciprocal(const double* x, double* y, long long n);
 
 /* ---- allocation-free hyperbolic term ----
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory when they need the hyperbolic term -- code running while a stream
- * it shares is being captured into a CUDA graph, or a plugin inside an
- * application whose memory manager owns the whole device -- this computes
- * what piafs_gpu_HyperbolicFunction computes, from the caller's u (ghosted,
- * ghosts filled, reference layout) and dxinv (ghosted 1/dx of each dimension,
- * concatenated), into the caller's hyp, with no simulation object and no
- * device allocation.  Its working arrays live in one 64 MiB __device__ array
- * that every GPU loading this library holds until exit; problems whose
- * working set (about 7 x nvars x ghosted points x 8 bytes) exceeds it are
- * rejected with PIAFS_ERR_ARGUMENT.  The first call on a device looks up that
- * array's address with the device current and should come before any stream
- * capture; all calls on a device share the array, so calls that overlap on
- * the GPU race and must be serialised by the caller.  The call runs on
- * `stream` (a cudaStream_t, 0 for the default stream) and waits for it. */
+ * memory when they need the hyperbolic term: a plugin inside an application
+ * whose memory manager owns the whole device and forbids allocations behind
+ * its back, or a host loop that must not pay cudaMalloc's implicit device
+ * synchronisation or risk an out-of-memory failure in the middle of a run.
+ * It computes what piafs_gpu_HyperbolicFunction computes (component-wise
+ * WENO5, CRWENO5 or upw5 interpolation; characteristic interpolation is not
+ * available through piafs_gpu_hyp_params), from the caller's u (ghosted,
+ * ghosts filled, reference layout) and dxinv (ghosted 1/dx of each
+ * dimension, concatenated), into the caller's hyp, with no simulation object
+ * and no device allocation.  Its working arrays live in one 64 MiB
+ * __device__ array that every GPU loading this library holds until exit;
+ * problems whose working set (about 7 x nvars x ghosted points x 8 bytes)
+ * exceeds it are rejected with PIAFS_ERR_ARGUMENT.  The first call on a
+ * device looks up that array's address with the device current (make it
+ * before any stream capture begins); all calls on a device share the array,
+ * so calls that overlap on the GPU race and must be serialised by the
+ * caller.  The call runs on `stream` (a cudaStream_t, 0 for the default
+ * stream), then copies the zero-pivot flag to the host and synchronises that
+ * stream before it returns. */
 enum { PIAFS_MODEL_EULER1D = 0, PIAFS_MODEL_NS2D = 1 };
 enum { PIAFS_SCHEME_WENO5 = 0, PIAFS_SCHEME_CRWENO5 = 1, PIAFS_SCHEME_UPW5 = 2 };
 enum { PIAFS_UPWIND_ROE = 0, PIAFS_UPWIND_RF = 1, PIAFS_UPWIND_LLF = 2, PIAFS_UPWIND_RUSANOV = 3 };

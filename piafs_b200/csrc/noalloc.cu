@@ -1,16 +1,16 @@
 // Hyperbolic term without any device allocation.
 //
 // Some callers cannot allocate device memory at the point where they need the
-// hyperbolic term: a host code that evaluates the right-hand side inside a
-// region where cudaMalloc is not permitted (while a stream it shares is being
-// captured into a CUDA graph), or a plugin embedded in an application whose
-// memory manager owns every byte of the device and forbids allocations
-// behind its back.  piafs_gpu_HyperbolicFunction_noalloc serves them: it runs
-// the same kernels as piafs_gpu_HyperbolicFunction, but the working arrays
-// those kernels need (the structure-of-arrays copy of the state, the
-// cell-centred flux, the four reconstructed interface arrays and the result)
-// live in one file-scope __device__ array of fixed size instead of buffers
-// obtained from cudaMalloc.
+// hyperbolic term: a plugin embedded in an application whose memory manager
+// owns every byte of the device and forbids allocations behind its back, or
+// a host loop that must not pay cudaMalloc's implicit device synchronisation
+// or risk an out-of-memory failure in the middle of a run.
+// piafs_gpu_HyperbolicFunction_noalloc serves them: it runs the same kernels
+// as piafs_gpu_HyperbolicFunction (component-wise interpolation), but the
+// working arrays those kernels need (the structure-of-arrays copy of the
+// state, the cell-centred flux, the four reconstructed interface arrays and
+// the result) live in one file-scope __device__ array of fixed size instead
+// of buffers obtained from cudaMalloc.
 //
 // Rules of use
 //   - The array is PIAFS_NOALLOC_SCRATCH_BYTES (64 MiB) on every GPU that
@@ -23,6 +23,8 @@
 //     behind.  The call clears what must start at zero; calls whose work
 //     overlaps on the GPU (other streams, other host threads) race on the
 //     array and must be serialised by the caller.
+//   - The call copies the zero-pivot flag to the host and synchronises its
+//     stream before it returns.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -78,8 +80,8 @@ extern "C" int piafs_gpu_HyperbolicFunction_noalloc(const piafs_gpu_hyp_params* 
   P.no_limiting = q.no_limiting; P.eps = q.weno_eps; P.gamma = q.gamma; P.bc_gamma = q.gamma;
   if (P.scheme == CRWENO5)
     for (int d = 0; d < P.ndims; d++)
-      if (crweno_rows_per_thread(d == 0 ? P.N0 : P.N1) < 0)
-        return nfail(PIAFS_ERR_UNSUPPORTED, "crweno5 lines longer than 4097 points are outside the GPU path");
+      if (crweno_cluster_size(d == 0 ? P.N0 : P.N1) < 0)
+        return nfail(PIAFS_ERR_UNSUPPORTED, "crweno5 lines longer than 32769 points are outside the GPU path");
 
   // working set: state, flux and result planes, four interface plane sets,
   // the zero-pivot flag

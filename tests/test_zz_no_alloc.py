@@ -1,9 +1,10 @@
 """The allocation-free hyperbolic term (piafs_gpu_HyperbolicFunction_noalloc).
 
 Callers that cannot allocate device memory when they need the hyperbolic term
-(code running during a stream capture, plugins inside an application that
-owns all device memory) use this entry point; its working arrays live in a
-fixed 64 MiB __device__ array instead of cudaMalloc'd buffers.  These checks
+(plugins inside an application whose memory manager owns the whole device,
+host loops that must not pay cudaMalloc's implicit synchronisation or risk an
+out-of-memory failure mid-run) use this entry point; its working arrays live
+in a fixed 64 MiB __device__ array instead of cudaMalloc'd buffers.  These checks
 call it through the C ABI and hold it to the allocating entry point
 (piafs_gpu_HyperbolicFunction) on the same state, twice in a row so that the
 second call runs on the scratch the first one left behind.  This file is
@@ -24,7 +25,7 @@ torch = pytest.importorskip("torch")
 TOL = 1e-12
 
 MODEL = {"euler1d": 0, "navierstokes2d": 1}
-SCHEME = {"weno5": 0, "crweno5": 1}
+SCHEME = {"weno5": 0, "crweno5": 1, "upw5": 2}
 UPWIND = {"roe": 0, "rf-char": 1, "llf-char": 2, "rusanov": 3}
 
 
@@ -78,7 +79,9 @@ def rel_l2(got, want, nv):
 
 
 @pytest.mark.parametrize("name", ["ns2d_chem_crweno5_llf_64x48", "ns2d_shear_weno5_roe_re200_40x32",
-                                  "euler1d_crweno5_rusanov_mapped_n200"])
+                                  "euler1d_crweno5_rusanov_mapped_n200", "ns2d_cavity_noslip_upw5_par4_32x32",
+                                  "ns2d_chem_supersonic_jet_weno5_rf_24x32", "euler1d_weno5_llf_yc_rk4_n128",
+                                  "euler1d_crweno5_roe_n6000"])
 def test_noalloc_matches_allocating_entry_point(name):
     d = os.path.join(GOLDEN, name)
     with Simulation(d) as sim:
