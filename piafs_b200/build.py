@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libpiafs_gpu.so")
 CLI = os.path.join(HERE, "bin", "piafs-gpu")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-SOURCES = ["kernels.cu", "crweno.cu", "crweno_char.cu", "api.cu", "deck.cpp", "noalloc.cu", "batch.cu", "batch_stage_fp64.cu",
+SOURCES = ["kernels.cu", "crweno.cu", "crweno_line.cu", "crweno_char.cu", "api.cu", "deck.cpp", "noalloc.cu", "batch.cu", "batch_stage_fp64.cu",
            "batch_stage_mixed.cu"]
 
 

@@ -77,20 +77,22 @@ __device__ __forceinline__ void eu_flowvar(T rho_in, T ru, T e_in, T gamma, T& r
 }
 
 // Reciprocal 1/x of a finite, nonzero, normal x whose reciprocal is normal.
-// Newton-Raphson iteration for f(y) = 1/y - x, y <- y + y (1 - x y), each
-// step squaring the relative error (P. Markstein, "Computation of elementary
+// From the hardware estimate y of PTX rcp.approx.ftz.f64, with relative
+// error d (y = (1 - d)/x, so e = 1 - x y = d), one step of the third-order
+// iteration y <- y + y (e + e^2) gives (1 - d)(1 + d + d^2)/x = (1 - d^3)/x:
+// the estimate's error cubed, far below a unit in the last place, and the
+// two rounded multiply-adds leave the result within a unit or two in the
+// last place.  The step is the series 1/x = y / (1 - e) = y (1 + e + e^2 +
+// ...) cut after e^2, a third-order relative of the Newton-Raphson
+// refinement y <- y + y e (P. Markstein, "Computation of elementary
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34
-// (1990) 111-119), started from the hardware estimate of PTX
-// rcp.approx.ftz.f64; two steps take the estimate to within a unit or two in
-// the last place.  x = 0 gives NaN, which callers detect separately.
+// (1990) 111-119).  x = 0 gives NaN, which callers detect separately.
 #ifdef __CUDACC__
 __device__ __forceinline__ double rcp_nr(double x) {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
 }
 // FP32 reciprocal of the mixed-precision inner arithmetic: the hardware
 // approximation of PTX rcp.approx.ftz.f32 (within about 1 ulp of FP32).

@@ -164,6 +164,12 @@ int crweno_rows_per_thread(int N);
 int crweno_cluster_size(int N);
 int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
                   int dir, int* err, cudaStream_t s);
+// the same for lines of up to 4097 interfaces, one CTA per line
+// (crweno_line.cu): true if it serves lines of N points; -1 from the
+// launcher otherwise
+bool crweno_line_fits(int N);
+int launch_crweno_line(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
+                       void* fR, int dir, int* err, cudaStream_t s);
 // CRWENO5 on characteristic variables (crweno_char.cu; 1D Euler and 2D
 // Navier-Stokes without chemistry, FP64): all four interface arrays of
 // direction dir; scratch holds crweno_char_scratch(P) doubles; *err is set on
