@@ -99,8 +99,24 @@ int piafs_gpu_TimeRK_host(piafs_gpu_sim* sim, double* u_host, double t);
 /* The reference's Solve() loop (src/Simulation/Solve.cpp:29-123): n_iter
  * steps from the initial solution with op_NNNNN.bin written to `output_dir`
  * at iteration 0, every file_op_iter steps and at the end (binary output
- * format only). */
+ * format only); every screen_op_iter-th step prints the reference's
+ * TimePrintStep line (iteration, time, CFL before the step, residual norm,
+ * wall time; TimePrintStep.c:25-37) on stdout. */
 int piafs_gpu_Solve(piafs_gpu_sim* sim, const char* output_dir);
+
+/* piafs_gpu_TimeRK that also returns the residual norm of the last step,
+ * sqrt(sum over interior points and variables of (u_new - u_old)^2 / points)
+ * (TimePostStep.c:36-54). */
+int piafs_gpu_TimeRK_norm(piafs_gpu_sim* sim, int nsteps, double* norm);
+
+/* After a Solve: the reference's end-of-run files in `dir`, as SimWriteErrors
+ * writes them for one simulation (SimulationWriteErrors.c:65-80) --
+ * errors.dat (grid, processes, dt, the L1 / L2 / Linf errors against
+ * exact.inp when `dir` holds one (CalculateError.c:30-120), else -1, and the
+ * two runtimes), conservation.dat (-1 per variable: conservation_check is
+ * not on the GPU path) and function_counts.dat -- and the runtime lines it
+ * prints. */
+int piafs_gpu_WriteErrors(piafs_gpu_sim* sim, const char* dir, double solver_runtime, double main_runtime);
 
 /* Asynchronous form of piafs_gpu_TimeRK: enqueues nsteps steps on the
  * simulation's CUDA stream and returns without waiting (diagnostics and the
@@ -119,6 +135,12 @@ int piafs_gpu_synchronize(piafs_gpu_sim* sim);
  * solve), then [2 ndims] upwinding + divergence of all directions and
  * [2 ndims + 1] viscous + source.  nphases (in/out) is the capacity / count. */
 int piafs_gpu_profile_rhs(piafs_gpu_sim* sim, int reps, double* ms, int* nphases);
+
+/* Photon density of the last RK stage evaluated (the reference's
+ * Chemistry::nv_hnu, ChemistrySolve.c:46-58, as the species output writes it):
+ * into nv_hnu[nz * p + iz] for every ghosted point p and simulated layer iz.
+ * Only simulations that write species files keep it. */
+int piafs_gpu_get_photon_density(piafs_gpu_sim* sim, double* nv_hnu);
 
 /* max CFL of the current state (NavierStokes2DComputeCFL.c /
  * Euler1DComputeCFL.c). */

@@ -46,6 +46,9 @@ SIGNATURES = {
     "piafs_gpu_get_state": (C.c_int, [_vp, _dp]),
     "piafs_gpu_get_solution": (C.c_int, [_vp, _dp]),
     "piafs_gpu_TimeRK": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_TimeRK_norm": (C.c_int, [_vp, C.c_int, _dp]),
+    "piafs_gpu_WriteErrors": (C.c_int, [_vp, C.c_char_p, C.c_double, C.c_double]),
+    "piafs_gpu_get_photon_density": (C.c_int, [_vp, _dp]),
     "piafs_gpu_TimeRK_host": (C.c_int, [_vp, _dp, C.c_double]),
     "piafs_gpu_Solve": (C.c_int, [_vp, C.c_char_p]),
     "piafs_gpu_ComputeCFL": (C.c_int, [_vp, _dp]),
@@ -229,6 +232,19 @@ class Simulation:
     def time_rk(self, nsteps: int = 1):
         """TimeIntegrate on the device-resident state (TimeRK.c:34)."""
         _check(_lib.piafs_gpu_TimeRK(self._h, int(nsteps)))
+
+    def time_rk_norm(self, nsteps: int = 1) -> float:
+        """Advance nsteps steps; the residual norm of the last one
+        (TimePostStep.c:36-54)."""
+        n = C.c_double()
+        _check(_lib.piafs_gpu_TimeRK_norm(self._h, int(nsteps), C.byref(n)))
+        return n.value
+
+    def write_errors(self, directory: str, solver_runtime: float = 0.0, main_runtime: float = 0.0):
+        """errors.dat, conservation.dat and function_counts.dat in directory
+        (SimulationWriteErrors.c:65-80)."""
+        _check(_lib.piafs_gpu_WriteErrors(self._h, os.fsencode(directory), float(solver_runtime),
+                                          float(main_runtime)))
 
     def time_rk_host(self, u: np.ndarray, t: float) -> np.ndarray:
         """One step on a host array in the reference layout, in place."""

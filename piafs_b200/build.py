@@ -3,6 +3,12 @@
 Produces, in-tree:
   piafs_b200/libpiafs_gpu.so   the C-ABI library (include/piafs_gpu.h)
   piafs_b200/bin/piafs-gpu     command-line drop-in for the reference binary
+  piafs_b200/libpiafs_hypar.so the entry points on the reference's own
+                               simulation objects (include/piafs_hypar.h);
+                               built when the reference's include/ is found
+                               (PIAFS_REF names its source tree), because it
+                               takes the layout of HyPar and the other
+                               structures from those headers
 """
 from __future__ import annotations
 
@@ -16,6 +22,8 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libpiafs_gpu.so")
 CLI = os.path.join(HERE, "bin", "piafs-gpu")
+HYPAR_LIB = os.path.join(HERE, "libpiafs_hypar.so")
+CUDA_INC = "/usr/local/cuda/include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 SOURCES = ["kernels.cu", "crweno.cu", "crweno_line.cu", "crweno_char.cu", "api.cu", "deck.cpp", "noalloc.cu", "batch.cu", "batch_stage_fp64.cu",
@@ -67,7 +75,38 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(CLI, [main, LIB]):
         run([nvcc] + ARCH + ["-O2", "-std=c++17", "-o", CLI, main, "-L" + HERE, "-lpiafs_gpu",
                              "-Xlinker", "-rpath,$ORIGIN/.."])
+    build_hypar(force, verbose)
     return LIB
+
+
+def reference_include():
+    """The reference's include/ directory, if its source tree is named by
+    PIAFS_REF and present."""
+    ref = os.environ.get("PIAFS_REF")
+    if ref and os.path.exists(os.path.join(ref, "include", "hypar.h")):
+        return os.path.join(ref, "include")
+    return None
+
+
+def build_hypar(force: bool = False, verbose: bool = False):
+    """libpiafs_hypar.so from csrc/hypar_attach.cpp, compiled with the
+    reference's headers in their single-rank (-Dserial) layout."""
+    inc = reference_include()
+    if inc is None:
+        return None
+    src = os.path.join(CSRC, "hypar_attach.cpp")
+    deps = [src, LIB, os.path.join(HERE, "..", "include", "piafs_hypar.h"), os.path.join(CSRC, "deck.h")]
+    if not (force or _stale(HYPAR_LIB, deps)):
+        return HYPAR_LIB
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Dserial", "-I" + inc, "-I" + CUDA_INC, src,
+           "-o", HYPAR_LIB, "-L" + HERE, "-lpiafs_gpu", "-L/usr/local/cuda/lib64", "-lcudart",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    if verbose:
+        sys.stdout.write(r.stdout + r.stderr)
+    return HYPAR_LIB
 
 
 if __name__ == "__main__":

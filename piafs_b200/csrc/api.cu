@@ -1,6 +1,8 @@
 // C ABI of the PIAFS GPU path (include/piafs_gpu.h): simulation object,
 // time stepping with CUDA-graph replay, Solve() loop with reference-format
 // output, and the operator-level entry points.
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -250,12 +252,25 @@ const char* piafs_gpu_last_error(void) { return g_err.c_str(); }
 int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   if (!deck_dir || !out) return fail(PIAFS_ERR_ARGUMENT, "null argument");
   *out = nullptr;
+  Deck d;
+  std::string err;
+  if (int r = read_deck(deck_dir, d, err)) return fail(r, err);
+  return piafs::create_sim(std::move(d), precision, out);
+}
+
+}  // extern "C"
+
+// A simulation from a parsed (or otherwise filled) deck: device arrays,
+// initial state, simulation time restart_iter x dt.
+int piafs::create_sim(Deck&& deck, int precision, piafs_gpu_sim** out) {
+  if (!out) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  *out = nullptr;
   if (precision != PIAFS_PRECISION_FP64 && precision != PIAFS_PRECISION_MIXED)
     return fail(PIAFS_ERR_ARGUMENT, "precision must be PIAFS_PRECISION_FP64 or PIAFS_PRECISION_MIXED");
   auto* s = new piafs_gpu_sim();
+  s->deck = std::move(deck);
   std::string err;
-  int r = read_deck(deck_dir, s->deck, err);
-  if (!r) r = make_params(s->deck, s->P, err);
+  int r = make_params(s->deck, s->P, err);
   if (r) { delete s; return fail(r, err); }
   s->precision = precision;
   s->P.mixed = precision == PIAFS_PRECISION_MIXED ? 1 : 0;
@@ -347,7 +362,21 @@ int piafs_gpu_create(const char* deck_dir, int precision, piafs_gpu_sim** out) {
   return PIAFS_OK;
 }
 
+extern "C" {
+
 void piafs_gpu_destroy(piafs_gpu_sim* s) { free_sim(s); }
+
+int piafs_gpu_get_photon_density(piafs_gpu_sim* s, double* nv_hnu) {
+  if (!s || !nv_hnu) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  if (!s->hnu) return fail(PIAFS_ERR_ARGUMENT, "this simulation keeps no photon density (no species output)");
+  const DevParams& P = s->P;
+  std::vector<double> h((size_t)P.nz * P.ps);
+  CK(cudaMemcpyAsync(h.data(), s->hnu, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (long long p = 0; p < P.npg; p++)
+    for (int iz = 0; iz < P.nz; iz++) nv_hnu[(size_t)P.nz * p + iz] = h[(size_t)iz * P.ps + p];
+  return PIAFS_OK;
+}
 
 int piafs_gpu_get_info(piafs_gpu_sim* s, piafs_gpu_info* info) {
   if (!s || !info) return fail(PIAFS_ERR_ARGUMENT, "null argument");
@@ -549,19 +578,105 @@ int piafs_gpu_Solve(piafs_gpu_sim* s, const char* output_dir) {
     if (!overwrite) index++;
     return PIAFS_OK;
   };
-  // Solve.cpp:54-95
+  // Solve.cpp:54-95; on screen steps the CFL before the step
+  // (TimePreStep.c:54-65), the residual norm after it (TimePostStep.c:36-54)
+  // and the TimePrintStep line (TimePrintStep.c:25-37)
   for (int it = s->iter; it < d.n_iter; it++) {
     if (it == 0) if (int r = output()) return r;
+    const auto w0 = std::chrono::steady_clock::now();
     const bool screen = ((it + 1) % d.screen_op_iter) == 0;
     if (screen) {
       double c;
       if (int r = piafs_gpu_ComputeCFL(s, &c)) return r;
     }
     if (int r = run_steps(s, 1, screen)) return r;
+    if (screen) {
+      const double wct = std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+      std::printf("iter=%7d  t=%1.3E  CFL=%1.3E  norm=%1.4E  wctime: %1.1E (s)  \n", it + 1, s->t, s->last_cfl,
+                  s->last_norm, wct);
+      std::fflush(stdout);
+    }
     if (((it + 1) % d.file_op_iter == 0) && (it + 1 < d.n_iter))
       if (int r = output()) return r;
   }
   return output();
+}
+
+int piafs_gpu_TimeRK_norm(piafs_gpu_sim* s, int nsteps, double* norm) {
+  if (!s || nsteps < 1 || !norm) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
+  if (int r = run_steps(s, nsteps, true)) return r;
+  *norm = s->last_norm;
+  return PIAFS_OK;
+}
+
+// SimWriteErrors (SimulationWriteErrors.c:65-80) for one simulation, after
+// CalculateError (CalculateError.c:30-120) against exact.inp when the deck
+// directory holds one
+int piafs_gpu_WriteErrors(piafs_gpu_sim* s, const char* dir, double solver_runtime, double main_runtime) {
+  if (!s || !dir) return fail(PIAFS_ERR_ARGUMENT, "null argument");
+  const Deck& d = s->deck;
+  const DevParams& P = s->P;
+  const long long npts = (long long)P.N0 * P.N1;
+  std::vector<double> u((size_t)npts * d.nvars);
+  if (int r = piafs_gpu_get_solution(s, u.data())) return r;
+  double err3[3] = {-1.0, -1.0, -1.0};
+  std::vector<double> ex;
+  bool found = false;
+  std::string msg;
+  if (int r = read_exact(dir, d, ex, found, msg)) return fail(r, msg);
+  if (found) {
+    double nrm[3] = {0, 0, 0}, e[3] = {0, 0, 0};
+    for (size_t k = 0; k < u.size(); k++) {
+      const double x = ex[k], dd = u[k] - ex[k];
+      nrm[0] += std::fabs(x); nrm[1] += x * x; nrm[2] = std::max(nrm[2], std::fabs(x));
+      e[0] += std::fabs(dd); e[1] += dd * dd; e[2] = std::max(e[2], std::fabs(dd));
+    }
+    nrm[0] /= (double)npts; nrm[1] = std::sqrt(nrm[1] / (double)npts);
+    e[0] /= (double)npts; e[1] = std::sqrt(e[1] / (double)npts);
+    const double tol = 1e-15;
+    const bool rel = nrm[0] > tol && nrm[1] > tol && nrm[2] > tol;
+    for (int k = 0; k < 3; k++) err3[k] = rel ? e[k] / nrm[k] : e[k];
+  }
+  const std::string base(dir);
+  FILE* f = std::fopen((base + "/errors.dat").c_str(), "w");
+  if (!f) return fail(PIAFS_ERR_IO, "cannot write errors.dat");
+  for (int k = 0; k < d.ndims; k++) std::fprintf(f, "%4d ", d.size[k]);
+  for (int k = 0; k < d.ndims; k++) std::fprintf(f, "%4d ", 1);
+  std::fprintf(f, "%1.16E  ", d.dt);
+  std::fprintf(f, "%1.16E %1.16E %1.16E   ", err3[0], err3[1], err3[2]);
+  std::fprintf(f, "%1.16E %1.16E\n", solver_runtime, main_runtime);
+  std::fclose(f);
+  // conservation errors: -1 per variable, as the reference leaves them
+  // without conservation_check (Initialize.c:195-196)
+  f = std::fopen((base + "/conservation.dat").c_str(), "w");
+  if (!f) return fail(PIAFS_ERR_IO, "cannot write conservation.dat");
+  for (int k = 0; k < d.ndims; k++) std::fprintf(f, "%4d ", d.size[k]);
+  for (int k = 0; k < d.ndims; k++) std::fprintf(f, "%4d ", 1);
+  std::fprintf(f, "%1.16E  ", d.dt);
+  for (int v = 0; v < d.nvars; v++) std::fprintf(f, "%1.16E ", -1.0);
+  std::fprintf(f, "\n");
+  std::fclose(f);
+  // calls of the hyperbolic, parabolic and source functions: one each per
+  // RK stage, the parabolic one only for viscous Navier-Stokes
+  // (NavierStokes2DParabolicFunction.c:64-65), the source one when the model
+  // has a source (both models do, SourceFunction.c:37-39)
+  const long long steps = (long long)s->iter - d.restart_iter;
+  f = std::fopen((base + "/function_counts.dat").c_str(), "w");
+  if (!f) return fail(PIAFS_ERR_IO, "cannot write function_counts.dat");
+  std::fprintf(f, "%d\n", d.n_iter);
+  std::fprintf(f, "%lld\n", steps * d.nstages);
+  std::fprintf(f, "%lld\n", (P.ndims == 2 && P.viscous) ? steps * d.nstages : 0);
+  std::fprintf(f, "%lld\n", steps * d.nstages);
+  std::fclose(f);
+  if (err3[0] >= 0) {
+    std::printf("Computed errors for domain %d:\n", 0);
+    std::printf("  L1         Error           : %1.16E\n", err3[0]);
+    std::printf("  L2         Error           : %1.16E\n", err3[1]);
+    std::printf("  Linfinity  Error           : %1.16E\n", err3[2]);
+  }
+  std::printf("Solver runtime (in seconds): %1.16E\n", solver_runtime);
+  std::printf("Total  runtime (in seconds): %1.16E\n", main_runtime);
+  return PIAFS_OK;
 }
 
 // ------------------------------------------------- operator-level calls

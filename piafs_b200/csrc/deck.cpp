@@ -299,6 +299,11 @@ int read_deck(const std::string& dir, Deck& d, std::string& err) {
     return PIAFS_ERR_INPUT;
   }
   if (d.input_mode != "serial") { err = "only input_mode serial is supported"; return PIAFS_ERR_UNSUPPORTED; }
+  if (d.conservation_check == "yes") {
+    err = "conservation_check yes (boundary flux integrals, TimeRK.c:76-81, TimePostStep.c:66-78) is not on the "
+          "GPU path";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
   // schemes on the GPU path
   if (d.hyp_space_scheme != "weno5" && d.hyp_space_scheme != "crweno5" && d.hyp_space_scheme != "upw5") {
     err = "hyp_space_scheme " + d.hyp_space_scheme + " is not on the GPU path (weno5, crweno5, upw5)";
@@ -531,6 +536,61 @@ boundaries:
     }
     d.zones.push_back(z);
     d.zone_vals.push_back(vals);
+  }
+  return 0;
+}
+
+int read_exact(const std::string& dir, const Deck& d, std::vector<double>& u, bool& found, std::string& err) {
+  std::vector<double> xs;
+  return read_field(dir + "/exact.inp", d, d.nvars, d.ip_file_type == "ascii", xs, u, found, err);
+}
+
+int check_deck(const Deck& d, std::string& err) {
+  if (d.ndims < 1 || d.ndims > 2 || (int)d.size.size() != d.ndims) {
+    err = "ndims must be 1 or 2 with one size per dimension";
+    return PIAFS_ERR_INPUT;
+  }
+  if (d.restart_iter != 0 && d.op_file_format != "binary" && d.op_file_format != "bin") {
+    err = "restart is supported only with binary output files";
+    return PIAFS_ERR_INPUT;
+  }
+  if (d.conservation_check == "yes") {
+    err = "conservation_check yes (boundary flux integrals, TimeRK.c:76-81, TimePostStep.c:66-78) is not on the "
+          "GPU path";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if (d.hyp_space_scheme != "weno5" && d.hyp_space_scheme != "crweno5" && d.hyp_space_scheme != "upw5") {
+    err = "hyp_space_scheme " + d.hyp_space_scheme + " is not on the GPU path (weno5, crweno5, upw5)";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if (d.hyp_interp_type != "components" && d.hyp_interp_type != "characteristic" && d.nvars > 1) {
+    err = "hyp_interp_type " + d.hyp_interp_type + " is not a PIAFS interpolation type (components, characteristic)";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if (d.ghosts < 3) { err = "WENO5/CRWENO5 need ghost >= 3"; return PIAFS_ERR_INPUT; }
+  if (d.model != "euler1d" && d.model != "navierstokes2d") {
+    err = "model " + d.model + " is not on the GPU path (euler1d, navierstokes2d)";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if ((d.model == "euler1d") != (d.ndims == 1)) { err = "ndims does not match the model"; return PIAFS_ERR_INPUT; }
+  if (d.model == "navierstokes2d" && d.par_space_scheme != "2" && d.par_space_scheme != "4") {
+    err = "par_space_scheme " + d.par_space_scheme + " is not a PIAFS parabolic scheme (2, 4)";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if (d.nstages < 1 || d.nstages > MAX_STAGES) { err = "more RK stages than the GPU path holds"; return PIAFS_ERR_UNSUPPORTED; }
+  if (d.upwinding != "roe" && d.upwinding != "rf-char" && d.upwinding != "llf-char" && d.upwinding != "rusanov") {
+    err = "upwinding " + d.upwinding + " is not valid (roe, rf-char, llf-char, rusanov)";
+    return PIAFS_ERR_INPUT;
+  }
+  if (d.hyp_space_scheme == "crweno5" && d.hyp_interp_type == "characteristic" && d.chem) {
+    err = "crweno5 with hyp_interp_type characteristic and photochemistry: the reference's block solve is "
+          "singular (use components)";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  const int nflow = d.model == "navierstokes2d" ? 4 : 3;
+  if (d.nvars != (d.chem ? nflow + 7 * d.nz : nflow)) {
+    err = "nvars does not match the model and its chemistry layers";
+    return PIAFS_ERR_INPUT;
   }
   return 0;
 }

@@ -91,9 +91,25 @@ struct DeckMemory {
 int read_deck_memory(const DeckMemory& m, Deck& d, std::string& err);
 // Flat device parameters from a parsed deck.
 int make_params(const Deck& d, DevParams& P, std::string& err);
+// The exact solution exact.inp of a deck directory (ExactSolution.c: same
+// format as initial.inp), interior points in output order; found = false
+// when the file is absent.
+int read_exact(const std::string& dir, const Deck& d, std::vector<double>& u_interior, bool& found,
+               std::string& err);
+// The options of a filled deck that lie outside the GPU path, as read_deck
+// refuses them; 0 or a PIAFS_ERR_* code with a message in `err`.
+int check_deck(const Deck& d, std::string& err);
 // Write an op_*.bin file (WriteBinary.c:37-93) from the interior AoS field of
 // nvars variables (the deck's by default).
 int write_binary(const std::string& path, const Deck& d, const double* u_interior, std::string& err,
                  int nvars = -1);
 
+}  // namespace piafs
+
+// A simulation object (api.cu) from a filled deck: device arrays, initial
+// state u0 at time restart_iter x dt.  Returns PIAFS_OK or a PIAFS_ERR_*
+// code (message in piafs_gpu_last_error()).
+struct piafs_gpu_sim;
+namespace piafs {
+int create_sim(Deck&& deck, int precision, piafs_gpu_sim** out);
 }  // namespace piafs

@@ -80,3 +80,25 @@ def test_batch_entry_points_argument_checks():
         # no device: a CUDA error, reported, not a crash
         assert lib.piafs_gpu_batch_create(0, 0, ctypes.byref(h)) == 4
         assert lib.piafs_gpu_last_error()
+
+
+HYPAR_HEADER = os.path.join(ROOT, "include", "piafs_hypar.h")
+HYPAR_LIB = os.path.join(ROOT, "piafs_b200", "libpiafs_hypar.so")
+
+
+def test_hypar_library_exports_every_declared_symbol():
+    """libpiafs_hypar.so (built against the reference's headers) exports the
+    entry points of include/piafs_hypar.h with the reference's
+    function-pointer signatures."""
+    if not os.path.exists(HYPAR_LIB):
+        pytest.skip("libpiafs_hypar.so not built (the reference's headers were not available)")
+    txt = re.sub(r"/\*.*?\*/", "", open(HYPAR_HEADER).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(piafs_gpu_\w+)\s*\(", txt)))
+    assert "piafs_gpu_TimeRK_ts" in names and "piafs_gpu_attach" in names
+    piafs_b200.load_library()
+    lib = ctypes.CDLL(HYPAR_LIB)
+    for name in names:
+        assert isinstance(getattr(lib, name), ctypes._CFuncPtr), name
+    # no simulation object: argument errors before any device work
+    assert lib.piafs_gpu_attach(None, 1, 0, ctypes.c_double(0.0)) == 1
+    assert lib.piafs_gpu_TimeRK_ts(None) == 1

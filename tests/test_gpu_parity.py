@@ -134,8 +134,9 @@ def test_cli_drop_in(deck_copy):
     assert_close(got, deck.read_op(os.path.join(GOLDEN, name, "ref_final.bin")).u)
 
 
-def test_intermediate_outputs_and_restart(deck_copy, tmp_path):
-    # file_op_iter output cadence and restart from an op file
+def test_intermediate_outputs(deck_copy, tmp_path):
+    # file_op_iter output cadence: files at 0, 4, 8, 12 steps, the third one
+    # held to the oracle (restarts: tests/test_gpu_diagnostics.py)
     d = str(tmp_path / "r")
     cases.euler1d_density_wave(d, N=64, n_iter=12, dt=2e-3, file_op_iter=4)
     with Simulation(d) as sim:
