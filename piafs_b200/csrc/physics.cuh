@@ -177,6 +177,94 @@ __device__ __forceinline__ void euler1d_flux(double u0, double u1, double u2, do
   f[2] = __dmul_rn(__dadd_rn(e, pr), v);
 }
 
+// Reciprocal in the working precision: rcp_nr (common.cuh) for both types.
+template <typename T> __device__ __forceinline__ T rcpw(T x) { return rcp_nr(x); }
+
+// The characteristic-upwinding set-up of 2D Navier-Stokes at one interface
+// (NavierStokes2DUpwind.c:190-260 / 271-332): the Roe average of the two
+// interface states (_NavierStokes2DRoeAverage_, navierstokes2d.h:115-159),
+// its left / right eigenvectors (_NavierStokes2DLeftEigenvectors_ /
+// _RightEigenvectors_, :194-313) and the eigenvalues at the left, right and
+// averaged states (_NavierStokes2DEigenvalues_, :161-190).  The same
+// formulas as Flow<NS2D>::roe_avg / eigvec / eigvals, evaluated once per
+// state: each state's velocity, pressure and sound speed are formed once
+// and shared by the average and the eigenvalues, quotients by a density or by
+// a^2 are products with one reciprocal (rcp_nr), and the averaged state's
+// velocity, sound speed and enthalpy are used as computed rather than
+// re-derived from its conserved variables -- 4 reciprocals and 5 square
+// roots per interface where the per-macro form takes 25 divisions and 7
+// roots.  The results agree with the macro form to rounding.
+template <typename T>
+__device__ __forceinline__ void ns2d_char_setup(const T* uL, const T* uR, T g, int dir, T L[4][4], T R[4][4],
+                                                T* eL, T* eR, T* eC, T& vnL, T& vnR, T& vnC) {
+  const T gm1 = g - T(1), igm1 = rcpw(gm1);
+  // one side: rho, velocity, pressure (_NavierStokes2DGetFlowVar_,
+  // navierstokes2d.h:70-80), c^2 = gamma P / rho, enthalpy
+  auto side = [&](const T* u, T& rho, T& vx, T& vy, T& csq, T& H) {
+    rho = u[0];
+    const T ir = rho == T(0) ? T(0) : rcpw(rho);
+    vx = u[1] * ir;
+    vy = u[2] * ir;
+    const T vsq = vx * vx + vy * vy;
+    const T P = (u[3] - T(0.5) * rho * vsq) * gm1;
+    csq = g * P * ir;
+    H = T(0.5) * vsq + csq * igm1;
+  };
+  T rhoL, vxL, vyL, cLsq, HL, rhoR, vxR, vyR, cRsq, HR;
+  side(uL, rhoL, vxL, vyL, cLsq, HL);
+  side(uR, rhoR, vxR, vyR, cRsq, HR);
+  const T cL = sqrt(cLsq), cR = sqrt(cRsq);
+  // Roe average
+  const T tL = sqrt(rhoL), tR = sqrt(rhoR);
+  const T inv = rcpw(tL + tR);
+  const T vx = (tL * vxL + tR * vxR) * inv, vy = (tL * vyL + tR * vyR) * inv;
+  const T H = (tL * HL + tR * HR) * inv;
+  const T ek = T(0.5) * (vx * vx + vy * vy);
+  const T a = sqrt(gm1 * (H - ek));
+  // eigenvalues (x: u-c, u+c, u, u; y: v-c, v, v+c, v)
+  vnL = dir == 0 ? vxL : vyL;
+  vnR = dir == 0 ? vxR : vyR;
+  vnC = dir == 0 ? vx : vy;
+  auto eig = [&](T vn, T c, T* D) {
+    D[0] = vn - c;
+    if (dir == 0) { D[1] = vn + c; D[2] = vn; } else { D[1] = vn; D[2] = vn + c; }
+    D[3] = vn;
+  };
+  eig(vnL, cL, eL);
+  eig(vnR, cR, eR);
+  eig(vnC, a, eC);
+  // eigenvectors of the averaged state
+  const T a2 = a * a, ia2 = rcpw(a2), i2a2 = T(0.5) * ia2;
+  const T h0 = a2 * igm1 + ek;
+  if (dir == 0) {
+    const T un = vx;
+    L[0][0] = (gm1 * ek + a * un) * i2a2; L[0][1] = ((-gm1) * vx - a) * i2a2;
+    L[0][2] = ((-gm1) * vy) * i2a2;       L[0][3] = gm1 * i2a2;
+    L[3][0] = (a2 - gm1 * ek) * ia2;      L[3][1] = (gm1 * vx) * ia2;
+    L[3][2] = (gm1 * vy) * ia2;           L[3][3] = (-gm1) * ia2;
+    L[1][0] = (gm1 * ek - a * un) * i2a2; L[1][1] = ((-gm1) * vx + a) * i2a2;
+    L[1][2] = ((-gm1) * vy) * i2a2;       L[1][3] = gm1 * i2a2;
+    L[2][0] = vy; L[2][1] = T(0); L[2][2] = T(-1); L[2][3] = T(0);
+    R[0][0] = T(1); R[1][0] = vx - a; R[2][0] = vy; R[3][0] = h0 - a * un;
+    R[0][3] = T(1); R[1][3] = vx;     R[2][3] = vy; R[3][3] = ek;
+    R[0][1] = T(1); R[1][1] = vx + a; R[2][1] = vy; R[3][1] = h0 + a * un;
+    R[0][2] = T(0); R[1][2] = T(0);   R[2][2] = T(-1); R[3][2] = -vy;
+  } else {
+    const T un = vy;
+    L[0][0] = (gm1 * ek + a * un) * i2a2; L[0][1] = ((T(1) - g) * vx) * i2a2;
+    L[0][2] = ((T(1) - g) * vy - a) * i2a2; L[0][3] = gm1 * i2a2;
+    L[3][0] = (a2 - gm1 * ek) * ia2;      L[3][1] = gm1 * vx * ia2;
+    L[3][2] = gm1 * vy * ia2;             L[3][3] = (T(1) - g) * ia2;
+    L[2][0] = (gm1 * ek - a * un) * i2a2; L[2][1] = ((T(1) - g) * vx) * i2a2;
+    L[2][2] = ((T(1) - g) * vy + a) * i2a2; L[2][3] = gm1 * i2a2;
+    L[1][0] = -vx; L[1][1] = T(1); L[1][2] = T(0); L[1][3] = T(0);
+    R[0][0] = T(1); R[1][0] = vx; R[2][0] = vy - a; R[3][0] = h0 - a * un;
+    R[0][3] = T(1); R[1][3] = vx; R[2][3] = vy;     R[3][3] = ek;
+    R[0][2] = T(1); R[1][2] = vx; R[2][2] = vy + a; R[3][2] = h0 + a * un;
+    R[0][1] = T(0); R[1][1] = T(1); R[2][1] = T(0); R[3][1] = vx;
+  }
+}
+
 template <typename T> __device__ __forceinline__ T absv(T a) { return a < T(0) ? -a : a; }
 template <typename T> __device__ __forceinline__ T maxv(T a, T b) { return a > b ? a : b; }
 template <typename T> __device__ __forceinline__ T max3v(T a, T b, T c) { return maxv(maxv(a, b), maxv(b, c)); }
@@ -253,11 +341,7 @@ __device__ void upwind_flow(const T* uL, const T* uR, const T* fL, const T* fR, 
     // characteristic LLF / RF
     T L[4][4], R[4][4], eL[4], eR[4], eC[4], vnL, vnR, vnC;
     if (MODEL == NS2D) {
-      F::roe_avg(uL, uR, g, ua);
-      F::eigvec(ua, g, dir, L, R);
-      vnL = F::eigvals(uL, g, dir, eL);
-      vnR = F::eigvals(uR, g, dir, eR);
-      vnC = F::eigvals(ua, g, dir, eC);
+      ns2d_char_setup<T>(uL, uR, g, dir, L, R, eL, eR, eC, vnL, vnR, vnC);
     } else {
       // Euler1D averages and evaluates the eigenvalues at the cell centres
       F::roe_avg(uCL, uCR, g, ua);
@@ -318,11 +402,7 @@ __device__ void upwind_flow_dev(const T* uL, const T* uR, const T* fL, const T* 
   }
   T ua[4], L[4][4], R[4][4], eL[4], eR[4], eC[4], vnL, vnR, vnC;
   if (MODEL == NS2D) {
-    F::roe_avg(uAL, uAR, g, ua);
-    F::eigvec(ua, g, dir, L, R);
-    vnL = F::eigvals(uAL, g, dir, eL);
-    vnR = F::eigvals(uAR, g, dir, eR);
-    vnC = F::eigvals(ua, g, dir, eC);
+    ns2d_char_setup<T>(uAL, uAR, g, dir, L, R, eL, eR, eC, vnL, vnR, vnC);
   } else {
     F::roe_avg(uCL, uCR, g, ua);
     F::eigvec(ua, g, dir, L, R);
