@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the mixed-precision and small-ensemble figures of the default run")
     return ap.parse_args()
 
 
@@ -423,6 +425,87 @@ def serving_bench(a):
 
 
 # --------------------------------------------------------------------- main
+def mixed_figure(tmp, a, fp64_sim, u0, t0, N, fp64_ms_per_step):
+    """The same workload in mixed precision (FP32 reconstruction rows,
+    weights, fluxes, viscous and source terms on FP64 state, FP64 line
+    solves): device time per step over the same chunks as the FP64 timing,
+    the ratio over FP64, and the error against the FP64 path after one full
+    chunk of steps from the same initial state."""
+    import numpy as np
+    import torch
+    from piafs_b200 import Simulation
+    with Simulation(tmp, precision="mixed") as sim:
+        stream = torch.cuda.ExternalStream(sim.stream)
+        for _ in range(3):
+            sim.set_state(u0, t0)
+            sim.time_rk(chunk_steps(N))
+        ms, done = 0.0, 0
+        while done < a.steps:
+            n = min(chunk_steps(N), a.steps - done)
+            sim.set_state(u0, t0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.time_rk_async(n)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            done += n
+        k = chunk_steps(N)
+        sim.set_state(u0, t0)
+        sim.time_rk(k)
+        got = sim.solution()
+    fp64_sim.set_state(u0, t0)
+    fp64_sim.time_rk(k)
+    ref = fp64_sim.solution()
+    rms = np.sqrt((ref * ref).mean(axis=0))
+    sig = rms >= 1e-6 * rms.max()
+    l2 = np.sqrt(((got - ref) ** 2).sum(axis=0) / np.maximum((ref * ref).sum(axis=0), 1e-300))
+    linf = np.abs(got - ref).max(axis=0) / np.maximum(np.abs(ref).max(axis=0), 1e-300)
+    step = ms / a.steps
+    return {"ms_per_step": step, "speedup_over_fp64": fp64_ms_per_step / step,
+            "error_vs_fp64": {"steps": k, "rel_l2_max": float(l2[sig].max()), "rel_linf_max": float(linf[sig].max())}}
+
+
+def ensemble_figure(members=32, steps=20):
+    """A small instance of the batched ensemble (seeded members of the
+    ensemble workload, sides 64-512, WENO5/LLF/SSPRK3, FP64): complete solves
+    (deck read, device set-up, steps, solution back) in one batch against the
+    same members solved one at a time, and the batched step phase as
+    grid-point RK-stage updates per second."""
+    import torch
+    from piafs_b200 import Batch, Simulation, cases
+    tmp = tempfile.mkdtemp(prefix="piafs_bench_ens_")
+    try:
+        mem = cases.ensemble(tmp, n=members, steps=steps)
+        with Batch() as B:        # modules and context warm
+            B.add(mem[0]["dir"], 1)
+            B.step(1)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with Batch() as B:
+            ids = B.add_many([m["dir"] for m in mem], [steps] * len(mem))
+            t1 = time.perf_counter()
+            B.step(steps)
+            t2 = time.perf_counter()
+            for i in ids:
+                B.solution(i)
+        batched = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        for m in mem:
+            with Simulation(m["dir"]) as sim:
+                sim.time_rk(steps)
+                sim.solution()
+        single = time.perf_counter() - t0
+        pts = sum(m["side"] ** 2 for m in mem)
+        return {"members": members, "steps": steps, "sides": [min(m["side"] for m in mem), max(m["side"] for m in mem)],
+                "batched_solves_per_s": members / batched, "one_at_a_time_solves_per_s": members / single,
+                "speedup": single / batched, "step_phase_pt_stage_updates_per_s": 3 * steps * pts / (t2 - t1),
+                "precision": "fp64", "full_workload": "bench.py --workload ensemble (256 members, 100 steps)"}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def relaunch_under_torchrun(a):
     """--gpus N > 1 started as a plain process: run the same command as N
     ranks (one per GPU) under torch.distributed.run and return its status."""
@@ -609,7 +692,20 @@ def main():
                "steps": ne, "ms_per_step": e2e_ms / ne,
                "api": "piafs_gpu_TimeRK_host (pinned host state in, one step, state out)"}
         launches = info["launches_per_step"] * a.steps
+        # the mixed-precision and batched-ensemble figures of the same run
+        # (rank 0, after the timed regions)
+        extras = {}
+        if rank == 0 and a.precision == "fp64" and a.workload == "ns2d_photochem" and not a.no_extras:
+            try:
+                extras["mixed"] = mixed_figure(tmp, a, sim, u0, t0, N, step_ms)
+            except Exception as ex:  # reported, not fatal
+                extras["mixed"] = {"error": str(ex)[:200]}
         sim.close()
+        if rank == 0 and a.workload == "ns2d_photochem" and not a.no_extras:
+            try:
+                extras["ensemble"] = ensemble_figure()
+            except Exception as ex:  # reported, not fatal
+                extras["ensemble"] = {"error": str(ex)[:200]}
 
         base = None
         if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -627,6 +723,7 @@ def main():
                     "precision": a.precision}
             if err is not None:
                 line["error_vs_fp64"] = err
+            line.update(extras)
             print(json.dumps(line))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
