@@ -435,7 +435,19 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __r
   }
 #pragma unroll
   for (int m = 0; m < NF; m++) so[m * sm_stride] = fi[m];
-  for (int m = NF; m < P.nvars; m++)
+  // passive variables four at a time, their sixteen loads in flight together
+  int m = NF;
+  for (; m + 4 <= P.nvars; m += 4) {
+    T l[4], r[4], fl[4], fr[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const long long o = (long long)(m + k) * P.pis + q;
+      l[k] = uL[o]; r[k] = uR[o]; fl[k] = fL[o]; fr[k] = fR[o];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) so[(m + k) * sm_stride] = upwind_species(spm, spa, l[k], r[k], fl[k], fr[k]);
+  }
+  for (; m < P.nvars; m++)
     so[m * sm_stride] = upwind_species(spm, spa, uL[m * P.pis + q], uR[m * P.pis + q], fL[m * P.pis + q],
                                        fR[m * P.pis + q]);
 }
@@ -452,7 +464,7 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __r
 // interface values relative to their line's reference, FP32 fluxes and
 // differences, FP64 result).
 template <int UPW, bool YT, bool MX>
-__global__ void __launch_bounds__(256) k_upwind_div2d(DevParams P, const double* __restrict__ U,
+__global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const double* __restrict__ U,
                                                       const double* __restrict__ UT,
                                                       const void* __restrict__ xuL, const void* __restrict__ xuR,
                                                       const void* __restrict__ xfL, const void* __restrict__ xfR,
