@@ -483,7 +483,9 @@ int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) 
   std::vector<double> acc(np, 0.0);
   double* U = s->u;
   double* R = s->Ud[0];
-  for (int r = 0; r < reps; r++) {
+  // one untimed evaluation first: the first launches of a kernel outside the
+  // step graphs carry one-time set-up
+  for (int r = -1; r < reps; r++) {
     enqueue_bc(s, U);
     int k = 0;
     CK(cudaEventRecord(ev[0], s->stream));
@@ -492,6 +494,7 @@ int piafs_gpu_profile_rhs(piafs_gpu_sim* s, int reps, double* ms, int* nphases) 
     enqueue_sponge(s, U, R);
     CK(cudaEventRecord(ev[++k], s->stream));
     CK(cudaStreamSynchronize(s->stream));
+    if (r < 0) continue;
     for (int i = 0; i < np; i++) {
       float t = 0.f;
       CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));

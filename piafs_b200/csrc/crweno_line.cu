@@ -48,14 +48,14 @@ template <int M, int DIR, int WT, bool MX>
 __global__ void __launch_bounds__(line_threads_max(), 1)
     k_crw_line(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
                void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
-  typedef typename std::conditional<MX, float, double>::type R;   // row arithmetic
+  typedef typename std::conditional<MX, float, double>::type R;   // weights' arithmetic
   typedef typename std::conditional<MX, float, double>::type O;   // interface storage
   extern __shared__ double2 sm2[];
   const int Pt = blockDim.x, k = threadIdx.x;
   double2* pcA = sm2;              // PCR rows (a, c, d), both biases: [2 buffers][3][Pt]
   double2* tp = sm2 + 6 * Pt;      // last-row coefficients (al, cg, rh) of each chunk: [3][Pt]
   double2* sy = sm2 + 9 * Pt;      // separator values [Pt]
-  R* cs = (R*)(sm2 + 10 * Pt);     // staged cells; later the output staging
+  double* cs = (double*)(sm2 + 10 * Pt);   // staged cells; later the output staging
   O* so = (O*)(sm2 + 10 * Pt);
 
   const int line = blockIdx.x, v = blockIdx.y;
@@ -89,9 +89,9 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
 // and the larger of the staged cells and the output staging
 template <int M, bool MX>
 size_t line_smem(int N, int Pt) {
-  const size_t rsz = MX ? sizeof(float) : sizeof(double);
-  const size_t cells = (size_t)(Pt * M + 6 + (Pt * M + 6) / 8 + 1) * rsz;
-  const size_t outs = (size_t)2 * (N + N / 16 + 1) * rsz;
+  const size_t osz = MX ? sizeof(float) : sizeof(double);
+  const size_t cells = (size_t)(Pt * M + 6 + (Pt * M + 6) / 8 + 1) * sizeof(double);
+  const size_t outs = (size_t)2 * (N + N / 16 + 1) * osz;
   return (size_t)10 * Pt * sizeof(double2) + (cells > outs ? cells : outs);
 }
 

@@ -25,16 +25,21 @@ __host__ __device__ constexpr int line_threads_m(int N) {
 // chunk's separator: on return x_{s+r} = rh[q][r] - al[q][r] X_s -
 // cg[q][r] X_{s+M} for r = 1 .. M-1, and (As, Bs, Cs, Rs) is the separator
 // row s.  FULL: every row lies in [2, N-2] (no boundary folding, no identity
-// rows).  R: the row arithmetic (double, or float in mixed precision).
+// rows).  R: the arithmetic of the nonlinear weights (double, or float in
+// mixed precision); the rows' right-hand sides, the rows themselves and their
+// elimination are FP64 in both, and in mixed precision each weight product
+// is converted once and serves both biases' rows.
 template <int M, int WT, bool FULL, typename R>
-__device__ __forceinline__ void crw_chunk(const R* __restrict__ cs, int k, int s, int N, const R* x0, const R* xN,
-                                          R eps, double (&As)[2], double (&Bs)[2], double (&Cs)[2],
-                                          double (&Rs)[2], double (&al)[2][M], double (&cg)[2][M],
-                                          double (&rh)[2][M], int& bad) {
-  // cells s-3 .. s+M+1 (staged index = cell + 3)
-  R c[M + 5];
+__device__ __forceinline__ void crw_chunk(const double* __restrict__ cs, int k, int s, int N, const double* x0,
+                                          const double* xN, R eps, double (&As)[2], double (&Bs)[2],
+                                          double (&Cs)[2], double (&Rs)[2], double (&al)[2][M],
+                                          double (&cg)[2][M], double (&rh)[2][M], int& bad) {
+  // cells s-3 .. s+M+1 (staged index = cell + 3), and the same in the
+  // weights' arithmetic
+  double c[M + 5];
+  R cw[M + 5];
 #pragma unroll
-  for (int r = 0; r < M + 5; r++) c[r] = cs[cpad(k * M + 1 + r)];
+  for (int r = 0; r < M + 5; r++) { c[r] = cs[cpad(k * M + 1 + r)]; cw[r] = (R)c[r]; }
   // Per window t (cells s-3+t .. s-1+t): the smoothness indicators at 4x
   // (b1: 13/3 d^2 + (a-4b+3c)^2, b2: .. (a-c)^2, b3: .. (3a-4b+c)^2) and,
   // for Jiang-Shu, q = (beta + eps)^2.  Two-cell averages of the compact
@@ -42,10 +47,11 @@ __device__ __forceinline__ void crw_chunk(const R* __restrict__ cs, int k, int s
   // right, qq = 1/2 left + 5/2 right.  Everything is produced in the row
   // loop as the rows need it (row r reads windows up to r+3), which keeps
   // the live range of each value short.
-  R b1[M + 3], b2[M + 3], b3[M + 3], q1[M + 3], q2[M + 3], q3[M + 3], pp[M + 3], qq[M + 3];
+  R b1[M + 3], b2[M + 3], b3[M + 3], q1[M + 3], q2[M + 3], q3[M + 3];
+  double pp[M + 3], qq[M + 3];
   auto window = [&](int t) {
     if (WT != WT_NOLIM) {
-      const R a = c[t], b = c[t + 1], cc = c[t + 2];
+      const R a = cw[t], b = cw[t + 1], cc = cw[t + 2];
       const R d = (a + cc) - R(2) * b;
       const R e1 = a - R(4) * b + R(3) * cc, e2 = a - cc, e3 = R(3) * a - R(4) * b + cc;
       const R dd = R(13.0 / 3.0) * d * d;
@@ -58,19 +64,19 @@ __device__ __forceinline__ void crw_chunk(const R* __restrict__ cs, int k, int s
       }
     }
     if (t >= 1) {
-      pp[t] = R(2.5) * c[t] + R(0.5) * c[t + 1];
-      qq[t] = R(0.5) * c[t] + R(2.5) * c[t + 1];
+      pp[t] = 2.5 * c[t] + 0.5 * c[t + 1];
+      qq[t] = 0.5 * c[t] + 2.5 * c[t + 1];
     }
   };
   // Jiang-Shu products of left-row index j: P23 = q2[j+1] q3[j+2],
   // P13 = q1[j] q3[j+2] (kept at 5x), P12 = q1[j] q2[j+1]; the left row j
   // has the weights (0.2 P23, 0.5 P13, 0.3 P12), the right row j-1 (0.2 P12,
   // 0.5 P13, 0.3 P23)
-  R P23[M + 1], P13x5[M + 1], P12[M + 1];
+  double P23[M + 1], P13x5[M + 1], P12[M + 1];
   auto products = [&](int j) {
-    P23[j] = q2[j + 1] * q3[j + 2];
-    P13x5[j] = (R(5) * q1[j]) * q3[j + 2];
-    P12[j] = q1[j] * q2[j + 1];
+    P23[j] = (double)(q2[j + 1] * q3[j + 2]);
+    P13x5[j] = (double)((R(5) * q1[j]) * q3[j + 2]);
+    P12[j] = (double)(q1[j] * q2[j + 1]);
   };
   window(0); window(1); window(2);
   if (WT == W_JS) products(0);
@@ -82,43 +88,44 @@ __device__ __forceinline__ void crw_chunk(const R* __restrict__ cs, int k, int s
     if (WT == W_JS) products(r + 1);
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      R Ar, Br, Cr, Rr;
+      double Ar, Br, Cr, Rr;
       if (WT == W_JS) {
         // rows at 30x: weights (W1, W2, W3) = 10 (w1, w2, w3), the 3x rows
         // and right-hand side of the general branch times 10
-        const R W1 = q == 0 ? R(2) * P23[r] : R(2) * P12[r + 1];
-        const R W2 = q == 0 ? P13x5[r] : P13x5[r + 1];
-        const R W3 = q == 0 ? R(3) * P12[r] : R(3) * P23[r + 1];
-        const R lo = R(2) * W1 + W2;
-        Br = W1 + R(2) * (W2 + W3);
+        const double W1 = q == 0 ? 2.0 * P23[r] : 2.0 * P12[r + 1];
+        const double W2 = q == 0 ? P13x5[r] : P13x5[r + 1];
+        const double W3 = q == 0 ? 3.0 * P12[r] : 3.0 * P23[r + 1];
+        const double lo = 2.0 * W1 + W2;
+        Br = W1 + 2.0 * (W2 + W3);
         Ar = q == 0 ? lo : W3;
         Cr = q == 0 ? W3 : lo;
         Rr = q == 0 ? W1 * qq[r + 1] + W2 * pp[r + 2] + W3 * qq[r + 2]
                     : W1 * pp[r + 3] + W2 * qq[r + 2] + W3 * pp[r + 2];
       } else {
-        R w1, w2, w3, tau = R(0);
+        R v1, v2, v3, tau = R(0);
         if (q == 0) {
           if (WT == W_BORGES) tau = fabs(b3[r + 2] - b1[r]);
-          if (WT == W_YC) { const R t4 = c[r] - R(4) * c[r + 1] + R(6) * c[r + 2] - R(4) * c[r + 3] + c[r + 4]; tau = R(4) * t4 * t4; }
-          crw_weights<WT, R>(b1[r], b2[r + 1], b3[r + 2], tau, eps, w1, w2, w3);
+          if (WT == W_YC) { const R t4 = cw[r] - R(4) * cw[r + 1] + R(6) * cw[r + 2] - R(4) * cw[r + 3] + cw[r + 4]; tau = R(4) * t4 * t4; }
+          crw_weights<WT, R>(b1[r], b2[r + 1], b3[r + 2], tau, eps, v1, v2, v3);
         } else {
           if (WT == W_BORGES) tau = fabs(b1[r + 1] - b3[r + 3]);
-          if (WT == W_YC) { const R t4 = c[r + 5] - R(4) * c[r + 4] + R(6) * c[r + 3] - R(4) * c[r + 2] + c[r + 1]; tau = R(4) * t4 * t4; }
-          crw_weights<WT, R>(b3[r + 3], b2[r + 2], b1[r + 1], tau, eps, w1, w2, w3);
+          if (WT == W_YC) { const R t4 = cw[r + 5] - R(4) * cw[r + 4] + R(6) * cw[r + 3] - R(4) * cw[r + 2] + cw[r + 1]; tau = R(4) * t4 * t4; }
+          crw_weights<WT, R>(b3[r + 3], b2[r + 2], b1[r + 1], tau, eps, v1, v2, v3);
         }
+        const double w1 = v1, w2 = v2, w3 = v3;
         // rows at 3x: (2 w1 + w2, w1 + 2 w2 + 2 w3, w3) and 3x the
         // right-hand side (pp, qq above)
-        const R lo = R(2) * w1 + w2, hi = w3;
-        Br = w1 + R(2) * (w2 + w3);
+        const double lo = 2.0 * w1 + w2, hi = w3;
+        Br = w1 + 2.0 * (w2 + w3);
         Ar = q == 0 ? lo : hi;
         Cr = q == 0 ? hi : lo;
         Rr = q == 0 ? w1 * qq[r + 1] + w2 * pp[r + 2] + w3 * qq[r + 2]
                     : w1 * pp[r + 3] + w2 * qq[r + 2] + w3 * pp[r + 2];
       }
       if (!FULL) {
-        if (i > N - 1) { Ar = R(0); Br = R(1); Cr = R(0); Rr = R(0); }
-        if (i == 1) { Rr -= Ar * x0[q]; Ar = R(0); }
-        if (i == N - 1) { Rr -= Cr * xN[q]; Cr = R(0); }
+        if (i > N - 1) { Ar = 0.0; Br = 1.0; Cr = 0.0; Rr = 0.0; }
+        if (i == 1) { Rr -= Ar * x0[q]; Ar = 0.0; }
+        if (i == N - 1) { Rr -= Cr * xN[q]; Cr = 0.0; }
       }
       const double A = Ar, B = Br, C = Cr, Rv = Rr;
       if (r == 0) { As[q] = A; Bs[q] = B; Cs[q] = C; Rs[q] = Rv; continue; }
@@ -151,12 +158,12 @@ __device__ __forceinline__ void crw_chunk(const R* __restrict__ cs, int k, int s
 // interface i.  Called by every thread of the CTA (Pt = blockDim.x threads,
 // M rows each); returns after a barrier, with the staged values visible to
 // the whole CTA.  Shared memory: pcA [2][3][Pt], tp [3][Pt], sy [Pt]
-// (double2), the cells cs (cpad layout, Pt M + 6 entries of R) and the
-// staging so, which may alias cs.  Sets bad on a zero pivot.
+// (double2), the cells cs (cpad layout, Pt M + 6 doubles) and the staging
+// so, which may alias cs.  Sets bad on a zero pivot.
 template <int M, int WT, typename R, typename O>
 __device__ __forceinline__ void line_pair_solve(const DevParams& P, const double* __restrict__ src, long long st,
-                                                double ref, int N, R* cs, double2* pcA, double2* tp, double2* sy,
-                                                O* so, int& bad) {
+                                                double ref, int N, double* cs, double2* pcA, double2* tp,
+                                                double2* sy, O* so, int& bad) {
   constexpr bool MX = std::is_same<R, float>::value;
   const int Pt = blockDim.x, k = threadIdx.x, lane = k & 31;
   const int s = 1 + k * M;          // separator row (interface) of this thread
@@ -176,16 +183,16 @@ __device__ __forceinline__ void line_pair_solve(const DevParams& P, const double
 #pragma unroll
     for (int it = 0; it <= M; it++) {
       const int j = k + it * Pt;
-      if (j < ncell) cs[cpad(j)] = (R)cv[it];
+      if (j < ncell) cs[cpad(j)] = cv[it];
     }
   }
-  R x0[2] = {R(0), R(0)}, xN[2] = {R(0), R(0)};
+  double x0[2] = {0.0, 0.0}, xN[2] = {0.0, 0.0};
   if (MX) {
     if (k == 0) { x0[0] = crw_edge_f(P, src, st, 0, 1, ref); x0[1] = crw_edge_f(P, src, st, 0, -1, ref); }
     if (k == kN) { xN[0] = crw_edge_f(P, src, st, N, 1, ref); xN[1] = crw_edge_f(P, src, st, N, -1, ref); }
   } else {
-    if (k == 0) { x0[0] = (R)crw_edge(P, src, st, 0, 1); x0[1] = (R)crw_edge(P, src, st, 0, -1); }
-    if (k == kN) { xN[0] = (R)crw_edge(P, src, st, N, 1); xN[1] = (R)crw_edge(P, src, st, N, -1); }
+    if (k == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
+    if (k == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
   }
   __syncthreads();
 
