@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 BYTES_PER_UNIT = {11: 264, 4: 96, 3: 72}   # 3 * nvars * 8: read U_s, read u_n, write (FP64 state)
 # measured DRAM traffic of one CRWENO5 line-solve launch per interior point
 # (dram__bytes_read + dram__bytes_write, ncu at 1536^2, 11 variables)
-TRAFFIC_PER_POINT = {11: (417.0e6 + 774.2e6) / (1536 * 1536)}
+TRAFFIC_PER_POINT = {11: (417.0e6 + 776.5e6) / (1536 * 1536)}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 CPU_SAMPLE_N = 512                          # sample grid of the CPU arms
 # Steps timed back to back from the initial condition before the state is
@@ -654,7 +654,7 @@ def main():
         peak = peaks.get("hbm_gbs", 6650.0)
         achieved = bpu * npts / (phases[dom] / 1e3) / 1e9
         # DRAM bytes per launch of the dominant kernel from the ncu capture of
-        # k_crweno_pair at 1536^2 (read + write per interior point, scaled by
+        # k_crw_line at 1536^2 (read + write per interior point, scaled by
         # the points processed); known for the FP64 CRWENO5 line solve only
         traffic = None
         if dom.startswith("reconstruct") and a.precision == "fp64" and (a.scheme or "crweno5") == "crweno5" \
