@@ -13,7 +13,7 @@ CompareSolutions-style norm of tests/test_gpu_parity.py).
 
 oracle/_ref/PIAFS_gpu_check also holds each GPU operator, called through
 the HyPar-signature entry points on the reference's host arrays, to the
-reference's own operator on the first step's state.
+reference's own operator on the state before the last step.
 """
 import os
 import re
