@@ -302,6 +302,63 @@ int piafs_gpu_serve_trace(const piafs_gpu_request* reqs, const double* arrival_s
                           unsigned long long hbm_budget_bytes, unsigned long long max_resident_points,
                           int steps_per_round, piafs_gpu_serve_result* out);
 
+/* ---- a 2D grid decomposed along y, one GPU per row slab ----
+ * Replaces the reference's MPI decomposition of one grid
+ * (MPIExchangeBoundariesnD.c:45-177, the MPI-parallel tridiagLU.c:16-85,
+ * 155-240).  Rank r of nranks owns rows [r n1, (r+1) n1) of the grid (its row
+ * slab: a piafs_gpu_sim of its own, whose x lines are whole) and, for the y
+ * direction, columns [r n0, (r+1) n0) over every row (its column slab), so
+ * that each y line is solved whole on one GPU; n1 = N1 / nranks and
+ * n0 = N0 / nranks must be whole numbers.  The caller moves the data between
+ * the slabs at three points of every RK stage (piafs_b200/slab.py does it
+ * with all-to-all collectives):
+ *   piafs_gpu_slab_stage_begin(st)      U_st, boundary zones, x pass
+ *   halo: rows [0, g) and [n1-g, n1) of U_st to the neighbouring row slabs'
+ *         ghost rows (wrapping around when periodic_y)
+ *   columns: rows [-g, n1+g) of U_st, columns of slab c, to column slab c,
+ *         transposed (the column state `utc`, [var][col + g][row + g],
+ *         plane stride col_plane_stride; the first slab's lower and the last
+ *         slab's upper ghost rows included)
+ *   piafs_gpu_slab_y_pass(st)           y pass on the column slab -> hy_send
+ *   hy: block r of hy_send ([var][n1][n0] values of hy_value_bytes) to row
+ *         slab r, which stores block c (from column slab c) at block c of
+ *         its hy_recv
+ *   piafs_gpu_slab_stage_end(st)        x upwinding, divergence, viscous
+ *                                       terms and source
+ * and after the last stage piafs_gpu_slab_step_end.  The result equals the
+ * undecomposed simulation's bit for bit.  2D decks without sponge zones,
+ * characteristic interpolation or par_space_scheme 4, whose x-face boundary
+ * zones span every row; FP64, or mixed precision with CRWENO5.  The row
+ * slab's piafs_gpu_sim (piafs_gpu_slab_sim) gives its state, solution, CFL
+ * and stream; every call runs on that stream. */
+typedef struct piafs_gpu_slab piafs_gpu_slab;
+typedef struct {
+  int rank, nranks;
+  int dim[2];                  /* the whole grid's interior points          */
+  int slab_rows, slab_cols;    /* n1, n0                                    */
+  int ghosts, nvars, nstages;
+  int periodic_y;              /* ghost rows wrap around the last slab      */
+  long long plane_stride;      /* row slab state: [var][row + g][col + g]   */
+  long long col_plane_stride;  /* column slab state: [var][col + g][row + g] */
+  long long hy_bytes;          /* size of hy_send and of hy_recv            */
+  int hy_value_bytes;          /* 8 (FP64) or 4 (mixed precision)           */
+} piafs_gpu_slab_info;
+int piafs_gpu_slab_create(const char* deck_dir, int precision, int rank, int nranks, piafs_gpu_slab** slab);
+void piafs_gpu_slab_destroy(piafs_gpu_slab* slab);
+int piafs_gpu_slab_get_info(piafs_gpu_slab* slab, piafs_gpu_slab_info* info);
+int piafs_gpu_slab_sim(piafs_gpu_slab* slab, piafs_gpu_sim** row_slab);
+/* device pointers: U of stage st (row slab), the column state, the y-term buffers */
+int piafs_gpu_slab_state(piafs_gpu_slab* slab, int stage, double** U);
+int piafs_gpu_slab_buffers(piafs_gpu_slab* slab, double** utc, void** hy_send, void** hy_recv);
+int piafs_gpu_slab_stage_begin(piafs_gpu_slab* slab, int stage);
+int piafs_gpu_slab_y_pass(piafs_gpu_slab* slab, int stage);
+int piafs_gpu_slab_stage_end(piafs_gpu_slab* slab, int stage);
+/* TimeRK's completion of the step; with_norm: sum of the squared change of
+ * u over the slab's points, read by piafs_gpu_slab_norm_sum (which
+ * synchronises the stream) */
+int piafs_gpu_slab_step_end(piafs_gpu_slab* slab, int with_norm);
+int piafs_gpu_slab_norm_sum(piafs_gpu_slab* slab, double* sum);
+
 /* ---- diagnostics ----
  * No counterpart in the reference.  y[i] = 1/x[i] (device arrays) computed
  * by the Newton-Raphson reciprocal that the reconstruction and line-solve

@@ -87,6 +87,17 @@ SIGNATURES = {
     "piafs_gpu_batch_add_request": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
     "piafs_gpu_batch_checksum": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
     "piafs_gpu_serve_trace": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_ulonglong, C.c_ulonglong, C.c_int, _vp]),
+    "piafs_gpu_slab_create": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "piafs_gpu_slab_destroy": (None, [_vp]),
+    "piafs_gpu_slab_get_info": (C.c_int, [_vp, _vp]),
+    "piafs_gpu_slab_sim": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "piafs_gpu_slab_state": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "piafs_gpu_slab_buffers": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
+    "piafs_gpu_slab_stage_begin": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_slab_y_pass": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_slab_stage_end": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_slab_step_end": (C.c_int, [_vp, C.c_int]),
+    "piafs_gpu_slab_norm_sum": (C.c_int, [_vp, _dp]),
 }
 
 

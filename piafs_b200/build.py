@@ -27,7 +27,7 @@ CUDA_INC = "/usr/local/cuda/include"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 SOURCES = ["kernels.cu", "crweno.cu", "crweno_line.cu", "crweno_char.cu", "api.cu", "deck.cpp", "noalloc.cu", "batch.cu", "batch_stage_fp64.cu",
-           "batch_stage_mixed.cu"]
+           "batch_stage_mixed.cu", "slab.cu"]
 
 
 def _nvcc():

@@ -13,6 +13,7 @@
 #include "../../include/piafs_gpu.h"
 #include "deck.h"
 #include "kernels.h"
+#include "sim.h"
 
 using namespace piafs;
 
@@ -37,47 +38,6 @@ int set_last_error(int code, const std::string& msg) { return fail(code, msg); }
                   std::string(#call) + ": " + cudaGetErrorString(e_));                             \
   } while (0)
 
-struct piafs_gpu_sim {
-  Deck deck;
-  DevParams P;
-  int precision = 0;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  // device state (structure of arrays)
-  double* u = nullptr;
-  double* U[MAX_STAGES] = {nullptr};       // U[0] aliases u
-  double* Ud[MAX_STAGES] = {nullptr};
-  double* fC = nullptr;
-  double* iface[5] = {nullptr};            // uL, uR, fL, fR, operator scratch
-  double* iface_y[4] = {nullptr};          // uL, uR, fL, fR of the y direction (2D)
-  double* scratch = nullptr;               // ghosted plane set for operator calls
-  double* ut = nullptr;                    // transposed state of the y-direction CRWENO5 pass
-  DevParams PT;                            // the transposed grid
-  double* dxinv = nullptr;
-  double* imap = nullptr;
-  double* tdev = nullptr;                  // simulation time on the device
-  double* top_t = nullptr;                 // time for operator calls
-  double* norm_acc = nullptr;
-  unsigned long long* cfl_acc = nullptr;
-  int* err = nullptr;
-  double* aos = nullptr;                   // ghosted AoS staging (host transfers)
-  size_t aos_bytes = 0;
-  double* hnu = nullptr;                   // photon density [nz][ps] of the last RK stage (species output)
-  // sponge zones: extents on the host, ramp and reference state in sponge_buf
-  struct SpongeDev { int dim; int is[2], ie[2]; size_t sig_off, ref_off; };
-  std::vector<SpongeDev> sponges;
-  double* sponge_buf = nullptr;
-  double* zone_buf = nullptr;              // boundary zones' values (Zone::val)
-  double* crwchar = nullptr;               // block rows of the characteristic CRWENO5 line solves
-  // host mirror of the clock
-  double t = 0.0;
-  int iter = 0;
-  double last_cfl = -1.0, last_norm = 0.0;
-  int singular = 0;
-  // CUDA graphs of one step: [0] plain, [1] with residual norm
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  bool use_graph = true;
-};
 
 static void free_sim(piafs_gpu_sim* s) {
   if (!s) return;
@@ -112,7 +72,7 @@ static void free_sim(piafs_gpu_sim* s) {
 // U so that its lines, the tridiagonal systems, are contiguous in memory; its
 // interface arrays are then in the transposed layout.  If `ev` is given, an
 // event is recorded after the flux and after the reconstruction.
-static void enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* const* I, cudaEvent_t* ev, int* k) {
+void piafs::enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* const* I, cudaEvent_t* ev, int* k) {
   const DevParams& P = s->P;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[++*k], s->stream); };
   if (P.scheme == CRWENO5 && P.char_interp) {
@@ -175,7 +135,7 @@ static void enqueue_rhs(piafs_gpu_sim* s, double* rhs, const double* U, const do
   enqueue_sponge(s, U, rhs);
 }
 
-static void enqueue_bc(piafs_gpu_sim* s, double* u) {
+void piafs::enqueue_bc(piafs_gpu_sim* s, double* u) {
   for (const Zone& z : s->deck.zones) launch_bc(s->P, u, z, s->stream);
 }
 

@@ -49,6 +49,9 @@ struct DevParams {
   int mixed;             // 1: FP32 inner arithmetic on FP64 state (mixed precision)
   int char_interp;       // 1: WENO5 / upw5 on characteristic variables (hyp_interp_type characteristic)
   int par4;              // 1: fourth-order central first derivatives in the viscous terms (par_space_scheme 4)
+  // rows [jg0, jg0 + N1) of a grid of N1g rows (a row slab of a decomposed
+  // grid); 0 and N1 for a whole grid
+  int jg0, N1g;
 };
 
 __host__ __device__ inline long long pidx(const DevParams& P, int i, int j) {
@@ -88,6 +91,10 @@ __device__ __forceinline__ void eu_flowvar(T rho_in, T ru, T e_in, T gamma, T& r
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34
 // (1990) 111-119).  x = 0 gives NaN, which callers detect separately.
 #ifdef __CUDACC__
+// a product rounded on its own (never contracted into a following add), for
+// sums whose terms are formed in different kernels
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double rcp_nr(double x) {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));

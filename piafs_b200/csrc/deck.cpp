@@ -545,6 +545,70 @@ int read_exact(const std::string& dir, const Deck& d, std::vector<double>& u, bo
   return read_field(dir + "/exact.inp", d, d.nvars, d.ip_file_type == "ascii", xs, u, found, err);
 }
 
+int restrict_rows(const Deck& d, int rank, int nranks, Deck& out, bool& periodic_y, std::string& err) {
+  periodic_y = false;
+  if (d.ndims != 2) { err = "a row-slab decomposition needs a 2D grid"; return PIAFS_ERR_UNSUPPORTED; }
+  const int N0 = d.size[0], N1 = d.size[1], g = d.ghosts;
+  if (nranks < 2 || rank < 0 || rank >= nranks) { err = "bad rank / number of slabs"; return PIAFS_ERR_ARGUMENT; }
+  if (N1 % nranks || N0 % nranks) {
+    err = "the grid's sides (" + std::to_string(N0) + " x " + std::to_string(N1) + ") must be multiples of the " +
+          std::to_string(nranks) + " slabs";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  const int n1 = N1 / nranks, j0 = rank * n1;
+  if (n1 < g) { err = "slabs thinner than the ghost width"; return PIAFS_ERR_UNSUPPORTED; }
+  if (!d.sponges.empty()) { err = "sponge zones are not supported on a decomposed grid"; return PIAFS_ERR_UNSUPPORTED; }
+  if (d.model == "navierstokes2d" && d.Re > 0 && d.par_space_scheme == "4") {
+    err = "par_space_scheme 4 is not supported on a decomposed grid";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  if (d.hyp_interp_type == "characteristic" && d.nvars > 1) {
+    err = "hyp_interp_type characteristic is not supported on a decomposed grid";
+    return PIAFS_ERR_UNSUPPORTED;
+  }
+  for (const Zone& z : d.zones) {
+    if (z.dim == 0 && (z.is[1] != 0 || z.ie[1] != N1)) {
+      err = "x-face boundary zones must span every row on a decomposed grid";
+      return PIAFS_ERR_UNSUPPORTED;
+    }
+    if (z.dim == 1 && z.type == BC_PERIODIC) periodic_y = true;
+  }
+  out = d;
+  out.size[1] = n1;
+  out.slab_j0 = j0;
+  out.slab_N1 = N1;
+  const size_t W0 = (size_t)N0 + 2 * g, W1 = (size_t)N1 + 2 * g, w1 = (size_t)n1 + 2 * g;
+  // coordinates and 1/dx: x part whole, y part the slab's ghosted rows
+  out.x.assign(d.x.begin(), d.x.begin() + W0);
+  out.x.insert(out.x.end(), d.x.begin() + W0 + j0, d.x.begin() + W0 + j0 + w1);
+  out.dxinv.assign(d.dxinv.begin(), d.dxinv.begin() + W0);
+  out.dxinv.insert(out.dxinv.end(), d.dxinv.begin() + W0 + j0, d.dxinv.begin() + W0 + j0 + w1);
+  out.grid.assign(d.grid.begin(), d.grid.begin() + N0);
+  out.grid.insert(out.grid.end(), d.grid.begin() + N0 + j0, d.grid.begin() + N0 + j0 + n1);
+  // ghosted rows j0 .. j0 + n1 + 2g - 1 of the whole grid (ghosted index)
+  if (!d.u0.empty()) {
+    const size_t row = W0 * d.nvars;
+    out.u0.assign(d.u0.begin() + row * j0, d.u0.begin() + row * (j0 + w1));
+  }
+  if (!d.imap.empty() && d.imap.size() == W0 * W1) out.imap.assign(d.imap.begin() + W0 * j0, d.imap.begin() + W0 * (j0 + w1));
+  out.zones.clear();
+  out.zone_vals.clear();
+  for (size_t k = 0; k < d.zones.size(); k++) {
+    Zone z = d.zones[k];
+    if (z.dim == 0) {
+      z.ie[1] = n1;
+    } else {
+      if (z.type == BC_PERIODIC) continue;
+      if (z.face == 1 && rank != 0) continue;
+      if (z.face == -1 && rank != nranks - 1) continue;
+      if (z.face == -1) { z.is[1] = n1; z.ie[1] = n1 + g; }
+    }
+    out.zones.push_back(z);
+    out.zone_vals.push_back(d.zone_vals[k]);
+  }
+  return 0;
+}
+
 int check_deck(const Deck& d, std::string& err) {
   if (d.ndims < 1 || d.ndims > 2 || (int)d.size.size() != d.ndims) {
     err = "ndims must be 1 or 2 with one size per dimension";
@@ -612,6 +676,8 @@ int make_params(const Deck& d, DevParams& P, std::string& err) {
   P.W0 = P.N0 + 2 * P.ghosts;
   P.W1 = d.ndims == 2 ? P.N1 + 2 * P.ghosts : 1;
   P.g1 = d.ndims == 2 ? P.ghosts : 0;
+  P.jg0 = d.slab_j0;
+  P.N1g = d.slab_N1 > 0 ? d.slab_N1 : P.N1;
   P.npg = (long long)P.W0 * P.W1;
   P.ps = (P.npg + 31) / 32 * 32;
   if (d.ndims == 1) {

@@ -59,6 +59,9 @@ struct Deck {
   std::vector<Zone> zones;
   std::vector<std::vector<double>> zone_vals;   // per zone: the values Zone::val points to on the device
   std::vector<SpongeZone> sponges;
+  // row slab of a decomposed grid: its first row in the whole grid and the
+  // whole grid's rows (0, 0: not a slab)
+  int slab_j0 = 0, slab_N1 = 0;
 };
 
 // The zones' values (Zone::val) packed in one array; off[z] is zone z's offset.
@@ -99,6 +102,14 @@ int read_exact(const std::string& dir, const Deck& d, std::vector<double>& u_int
 // The options of a filled deck that lie outside the GPU path, as read_deck
 // refuses them; 0 or a PIAFS_ERR_* code with a message in `err`.
 int check_deck(const Deck& d, std::string& err);
+// Rows [rank n1, (rank + 1) n1) of a 2D deck's grid, n1 = N1 / nranks (a row
+// slab of a grid decomposed along y), as a deck of its own: coordinates,
+// 1/dx, initial state and intensity map of the slab's rows with their ghost
+// rows, the boundary zones that touch the slab (y-face zones on the first
+// and last slab only; periodic y-face zones dropped, as the neighbouring
+// slabs' rows fill those ghosts).  Sets periodic_y when the grid is periodic
+// along y.
+int restrict_rows(const Deck& d, int rank, int nranks, Deck& out, bool& periodic_y, std::string& err);
 // Write an op_*.bin file (WriteBinary.c:37-93) from the interior AoS field of
 // nvars variables (the deck's by default).
 int write_binary(const std::string& path, const Deck& d, const double* u_interior, std::string& err,

@@ -463,7 +463,7 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __r
 // standard one (q = i + N0 j, cell values from U).  MX: mixed precision (FP32
 // interface values relative to their line's reference, FP32 fluxes and
 // differences, FP64 result).
-template <int UPW, bool YT, bool MX>
+template <int UPW, bool YT, bool MX, bool HYIN>
 __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const double* __restrict__ U,
                                                       const double* __restrict__ UT,
                                                       const void* __restrict__ xuL, const void* __restrict__ xuR,
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
                                                       const void* __restrict__ yuL, const void* __restrict__ yuR,
                                                       const void* __restrict__ yfL, const void* __restrict__ yfR,
                                                       const double* __restrict__ dxinv, double* __restrict__ rhs,
-                                                      int neg) {
+                                                      int neg, const void* __restrict__ hyin, int n0) {
   typedef typename std::conditional<MX, float, double>::type T;
   extern __shared__ double sfd[];
   T* sf = (T*)sfd;
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
                                sx + jj * LX + ii, NX);
     }
   }
-  {                              // TI x (TJ + 1) y-interfaces
+  if (!HYIN) {                   // TI x (TJ + 1) y-interfaces
     int ii, jj;
     if (YT) { jj = tid % (TJ + 1); ii = tid / (TJ + 1); }
     else { ii = tid % TI; jj = tid / TI; }
@@ -526,12 +526,65 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
   if (i >= N0 || j >= N1) return;
   const long long p = pidx(P, i, j);
   const T dxi = (T)dxinv[g + i], dyi = (T)dxinv[P.W0 + g + j];
+  // HYIN: the y term of column i comes from the slab that owns it, as
+  // hyin[((i / n0) nvars + m) N1 + j) n0 + i % n0] (k_slab_upwind_y)
+  const T* hyv = (const T*)hyin;
+  const long long hbase = HYIN ? (long long)(i / n0) * nvars * N1 * n0 + (long long)j * n0 + i % n0 : 0;
   for (int m = 0; m < nvars; m++) {
-    const T hx = dxi * (sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii]);
-    const T hy = dyi * (sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
+    const T hx = mul_rn(dxi, sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii]);
+    const T hy = HYIN ? hyv[hbase + (long long)m * N1 * n0]
+                      : mul_rn(dyi, sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
     const double h = (double)(hx + hy);
     rhs[(long long)m * P.ps + p] = neg ? -h : h;
   }
+}
+
+// The y term of the 2D hyperbolic divergence on a column slab of a grid
+// decomposed along y (columns [c0, c0 + N0) of the whole grid, all N1 rows,
+// in the transposed layout: cell values from UT, interface q = j + (N1 + 1) c):
+// the upwind fluxes at the y interfaces of a 16 x 15 tile as in
+// k_upwind_div2d, then dyinv_j (fIy[j+1] - fIy[j]) for every variable,
+// written for the row slab that owns row j: hy[((r nvars + m) n1 + j - r n1)
+// N0 + c], r = j / n1.  The product is rounded on its own, as k_upwind_div2d
+// rounds it before adding the x term.
+template <int UPW, bool MX>
+__global__ void __launch_bounds__(256, 3) k_slab_upwind_y(DevParams P, const double* __restrict__ UT,
+                                                       const void* __restrict__ yuL, const void* __restrict__ yuR,
+                                                       const void* __restrict__ yfL, const void* __restrict__ yfR,
+                                                       const double* __restrict__ dyinv, void* __restrict__ hy,
+                                                       int n1) {
+  typedef typename std::conditional<MX, float, double>::type T;
+  extern __shared__ double sfd[];
+  T* sy = (T*)sfd;
+  constexpr int TI = 16, TJ = 15, LY = TJ + 2, NY = TI * LY;
+  const int nvars = P.nvars, N0 = P.N0, N1 = P.N1, g = P.ghosts;
+  const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
+  const int tid = threadIdx.x;
+  double uref[4];
+  {
+    const int jj = tid % (TJ + 1), ii = tid / (TJ + 1);
+    const int i = i0 + ii, j = j0 + jj;
+    if (ii < TI && j <= N1 && i < N0) {
+      const long long line = (long long)P.W1 * (i + g);
+      if (MX && (UPW == UPW_LLF || UPW == UPW_RF)) {
+#pragma unroll
+        for (int m = 0; m < 4; m++) uref[m] = UT[m * P.ps + g + line];
+      }
+      const long long pR = (long long)(j + g) + line;
+      iface_upwind<UPW, 1, MX>(P, yuL, yuR, yfL, yfR, j + (long long)(N1 + 1) * i, UT, pR - 1, pR, uref,
+                               sy + ii * LY + jj, NY);
+    }
+  }
+  __syncthreads();
+  if (tid >= TI * TJ) return;
+  const int ii = tid % TI, jj = tid / TI;
+  const int i = i0 + ii, j = j0 + jj;
+  if (i >= N0 || j >= N1) return;
+  const T dyi = (T)dyinv[g + j];
+  const int r = j / n1;
+  T* out = (T*)hy + ((long long)r * nvars * n1 + (j - (long long)r * n1)) * N0 + i;
+  for (int m = 0; m < nvars; m++)
+    out[(long long)m * n1 * N0] = mul_rn(dyi, sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
 }
 
 // ===================================================== viscous + chemistry
@@ -609,7 +662,9 @@ __global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* 
       if (!need_x && !need_y) continue;
       const int qa = a, qb = b;               // (i, j) in the Q tile
       const T dxi = (T)dxinv[P.ghosts + i], dyi = (T)dxinv[P.W0 + P.ghosts + j];
-      const bool row_int = (j >= 0 && j < P.N1), col_int = (i >= 0 && i < P.N0);
+      // interior rows of the whole grid (a row slab's ghost rows inside it are
+      // interior rows)
+      const bool row_int = (j + P.jg0 >= 0 && j + P.jg0 < P.N1g), col_int = (i >= 0 && i < P.N0);
       const T uc = su[qb][qa], vc = sv[qb][qa], Tc = sT[qb][qa];
       // first differences (QDerivX only on interior rows, QDerivY only on interior columns)
       const T ux = row_int ? dxi * (su[qb][qa + 1] - uc) : T(0);
@@ -1008,34 +1063,68 @@ void launch_upwind_div(const DevParams& P, const double* U, const void* uL, cons
   else upwind_div_model<EULER1D>(P, U, uL, uR, fL, fR, dxinv, rhs, dir, mode, s);
 }
 
-template <int UPW, bool YT, bool MX>
+template <int UPW, bool YT, bool MX, bool HYIN>
 static void upwind_div2d_u(const DevParams& P, const double* U, const double* UT, const void* const* xi,
-                           const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
-  raise_smem_limit<k_upwind_div2d<UPW, YT, MX>>(200 * 1024);
+                           const void* const* yi, const double* dxinv, double* rhs, int neg, const void* hyin,
+                           int n0, cudaStream_t s) {
+  raise_smem_limit<k_upwind_div2d<UPW, YT, MX, HYIN>>(200 * 1024);
   dim3 grid(nblk(P.N0, 16), nblk(P.N1, 15));
-  size_t smem = (size_t)P.nvars * (17 * 15 + 16 * 17) * (MX ? sizeof(float) : sizeof(double));
-  k_upwind_div2d<UPW, YT, MX><<<grid, 256, smem, s>>>(P, U, UT, xi[0], xi[1], xi[2], xi[3], yi[0], yi[1], yi[2],
-                                                       yi[3], dxinv, rhs, neg);
+  size_t smem = (size_t)P.nvars * (17 * 15 + (HYIN ? 0 : 16 * 17)) * (MX ? sizeof(float) : sizeof(double));
+  const void* none = nullptr;
+  k_upwind_div2d<UPW, YT, MX, HYIN><<<grid, 256, smem, s>>>(P, U, UT, xi[0], xi[1], xi[2], xi[3],
+                                                             HYIN ? none : yi[0], HYIN ? none : yi[1],
+                                                             HYIN ? none : yi[2], HYIN ? none : yi[3], dxinv, rhs,
+                                                             neg, hyin, n0);
 }
-template <bool YT, bool MX>
+template <bool YT, bool MX, bool HYIN>
 static void upwind_div2d_yt(const DevParams& P, const double* U, const double* UT, const void* const* xi,
-                            const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
+                            const void* const* yi, const double* dxinv, double* rhs, int neg, const void* hyin,
+                            int n0, cudaStream_t s) {
   switch (P.upwind) {
-    case UPW_ROE: upwind_div2d_u<UPW_ROE, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
-    case UPW_RF: upwind_div2d_u<UPW_RF, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
-    case UPW_RUSANOV: upwind_div2d_u<UPW_RUSANOV, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
-    default: upwind_div2d_u<UPW_LLF, YT, MX>(P, U, UT, xi, yi, dxinv, rhs, neg, s); break;
+    case UPW_ROE: upwind_div2d_u<UPW_ROE, YT, MX, HYIN>(P, U, UT, xi, yi, dxinv, rhs, neg, hyin, n0, s); break;
+    case UPW_RF: upwind_div2d_u<UPW_RF, YT, MX, HYIN>(P, U, UT, xi, yi, dxinv, rhs, neg, hyin, n0, s); break;
+    case UPW_RUSANOV: upwind_div2d_u<UPW_RUSANOV, YT, MX, HYIN>(P, U, UT, xi, yi, dxinv, rhs, neg, hyin, n0, s); break;
+    default: upwind_div2d_u<UPW_LLF, YT, MX, HYIN>(P, U, UT, xi, yi, dxinv, rhs, neg, hyin, n0, s); break;
   }
 }
 void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
                          const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s) {
   if (P.mixed) {
-    if (UT) upwind_div2d_yt<true, true>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
-    else upwind_div2d_yt<false, true>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+    if (UT) upwind_div2d_yt<true, true, false>(P, U, UT, xi, yi, dxinv, rhs, neg, nullptr, 0, s);
+    else upwind_div2d_yt<false, true, false>(P, U, UT, xi, yi, dxinv, rhs, neg, nullptr, 0, s);
   } else {
-    if (UT) upwind_div2d_yt<true, false>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
-    else upwind_div2d_yt<false, false>(P, U, UT, xi, yi, dxinv, rhs, neg, s);
+    if (UT) upwind_div2d_yt<true, false, false>(P, U, UT, xi, yi, dxinv, rhs, neg, nullptr, 0, s);
+    else upwind_div2d_yt<false, false, false>(P, U, UT, xi, yi, dxinv, rhs, neg, nullptr, 0, s);
   }
+}
+void launch_upwind_div2d_hy(const DevParams& P, const double* U, const void* const* xi, const double* dxinv,
+                            const void* hy, int n0, double* rhs, int neg, cudaStream_t s) {
+  const void* const* none = xi;   // y interface arrays are not read
+  if (P.mixed) upwind_div2d_yt<false, true, true>(P, U, nullptr, xi, none, dxinv, rhs, neg, hy, n0, s);
+  else upwind_div2d_yt<false, false, true>(P, U, nullptr, xi, none, dxinv, rhs, neg, hy, n0, s);
+}
+template <int UPW, bool MX>
+static void slab_upwind_y_u(const DevParams& P, const double* UT, const void* const* yi, const double* dyinv,
+                            void* hy, int n1, cudaStream_t s) {
+  raise_smem_limit<k_slab_upwind_y<UPW, MX>>(200 * 1024);
+  dim3 grid(nblk(P.N0, 16), nblk(P.N1, 15));
+  size_t smem = (size_t)P.nvars * (16 * 17) * (MX ? sizeof(float) : sizeof(double));
+  k_slab_upwind_y<UPW, MX><<<grid, 256, smem, s>>>(P, UT, yi[0], yi[1], yi[2], yi[3], dyinv, hy, n1);
+}
+template <bool MX>
+static void slab_upwind_y_m(const DevParams& P, const double* UT, const void* const* yi, const double* dyinv,
+                            void* hy, int n1, cudaStream_t s) {
+  switch (P.upwind) {
+    case UPW_ROE: slab_upwind_y_u<UPW_ROE, MX>(P, UT, yi, dyinv, hy, n1, s); break;
+    case UPW_RF: slab_upwind_y_u<UPW_RF, MX>(P, UT, yi, dyinv, hy, n1, s); break;
+    case UPW_RUSANOV: slab_upwind_y_u<UPW_RUSANOV, MX>(P, UT, yi, dyinv, hy, n1, s); break;
+    default: slab_upwind_y_u<UPW_LLF, MX>(P, UT, yi, dyinv, hy, n1, s); break;
+  }
+}
+void launch_slab_upwind_y(const DevParams& P, const double* UT, const void* const* yi, const double* dyinv, void* hy,
+                          int n1, cudaStream_t s) {
+  if (P.mixed) slab_upwind_y_m<true>(P, UT, yi, dyinv, hy, n1, s);
+  else slab_upwind_y_m<false>(P, UT, yi, dyinv, hy, n1, s);
 }
 
 void launch_visc_source(const DevParams& P, const double* U, const double* dxinv, const double* imap,

@@ -187,6 +187,15 @@ void launch_upwind_div(const DevParams& P, const double* U, const void* uL, cons
 // with cell values from UT when UT is given.  rhs = -hyp (neg) or hyp.
 void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
                          const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
+// the same with the y term given: hy from the column slabs of a grid
+// decomposed along y (launch_slab_upwind_y's layout, n0 columns per slab)
+void launch_upwind_div2d_hy(const DevParams& P, const double* U, const void* const* xi, const double* dxinv,
+                            const void* hy, int n0, double* rhs, int neg, cudaStream_t s);
+// the y term of the hyperbolic divergence on a column slab (P: its N0
+// columns, all N1 rows; UT and yi in the transposed layout; dyinv the whole
+// grid's ghosted 1/dy), laid out for the row slabs of n1 rows
+void launch_slab_upwind_y(const DevParams& P, const double* UT, const void* const* yi, const double* dyinv, void* hy,
+                          int n1, cudaStream_t s);
 // rhs += par (if do_visc) then rhs += source (if do_chem)
 // sponge zone source on the RHS (box [is, ie) per dimension, sigma per index
 // along dim, uref per variable; sigma and uref in device memory)

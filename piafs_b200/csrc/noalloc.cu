@@ -71,6 +71,7 @@ extern "C" int piafs_gpu_HyperbolicFunction_noalloc(const piafs_gpu_hyp_params* 
   P.ndims = q.ndims; P.nvars = q.nvars; P.ghosts = q.ghosts;
   P.N0 = q.dim[0]; P.N1 = q.ndims == 2 ? q.dim[1] : 1;
   P.W0 = P.N0 + 2 * P.ghosts; P.W1 = q.ndims == 2 ? P.N1 + 2 * P.ghosts : 1; P.g1 = q.ndims == 2 ? P.ghosts : 0;
+  P.N1g = P.N1;
   P.npg = (long long)P.W0 * P.W1;
   P.ps = round32(P.npg);
   P.nint[0] = q.ndims == 1 ? P.N0 + 1 : (long long)(P.N0 + 1) * P.N1;
