@@ -92,10 +92,16 @@ def build_hypar(force: bool = False, verbose: bool = False):
     """libpiafs_hypar.so from csrc/hypar_attach.cpp, compiled with the
     reference's headers in their single-rank (-Dserial) layout."""
     inc = reference_include()
-    if inc is None:
-        return None
     src = os.path.join(CSRC, "hypar_attach.cpp")
-    deps = [src, LIB, os.path.join(HERE, "..", "include", "piafs_hypar.h"), os.path.join(CSRC, "deck.h")]
+    deps = [src, LIB, os.path.join(HERE, "..", "include", "piafs_hypar.h"), os.path.join(CSRC, "deck.h"),
+            os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "kernels.h")]
+    if inc is None:
+        # without the reference's headers it cannot be rebuilt; one built
+        # against older library structures must not be loaded
+        if os.path.exists(HYPAR_LIB) and _stale(HYPAR_LIB, deps):
+            sys.stderr.write("removing " + HYPAR_LIB + ": older than the library and no PIAFS_REF to rebuild it\n")
+            os.remove(HYPAR_LIB)
+        return None
     if not (force or _stale(HYPAR_LIB, deps)):
         return HYPAR_LIB
     cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Dserial", "-I" + inc, "-I" + CUDA_INC, src,

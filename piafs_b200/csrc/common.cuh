@@ -91,10 +91,12 @@ __device__ __forceinline__ void eu_flowvar(T rho_in, T ru, T e_in, T gamma, T& r
 // functions on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34
 // (1990) 111-119).  x = 0 gives NaN, which callers detect separately.
 #ifdef __CUDACC__
-// a product rounded on its own (never contracted into a following add), for
-// sums whose terms are formed in different kernels
+// a product rounded on its own (never contracted into a following add), and
+// a fused multiply-add, for sums whose terms are formed in different kernels
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double rcp_nr(double x) {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));

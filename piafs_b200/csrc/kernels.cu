@@ -531,10 +531,12 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
   const T* hyv = (const T*)hyin;
   const long long hbase = HYIN ? (long long)(i / n0) * nvars * N1 * n0 + (long long)j * n0 + i % n0 : 0;
   for (int m = 0; m < nvars; m++) {
-    const T hx = mul_rn(dxi, sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii]);
+    // hyp = dxinv_x dfx + dxinv_y dfy as dxinv_x dfx fused onto the rounded y
+    // term, on both paths
+    const T dfx = sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii];
     const T hy = HYIN ? hyv[hbase + (long long)m * N1 * n0]
                       : mul_rn(dyi, sy[m * NY + ii * LY + jj + 1] - sy[m * NY + ii * LY + jj]);
-    const double h = (double)(hx + hy);
+    const double h = (double)fma_rn(dxi, dfx, hy);
     rhs[(long long)m * P.ps + p] = neg ? -h : h;
   }
 }
@@ -545,8 +547,8 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
 // the upwind fluxes at the y interfaces of a 16 x 15 tile as in
 // k_upwind_div2d, then dyinv_j (fIy[j+1] - fIy[j]) for every variable,
 // written for the row slab that owns row j: hy[((r nvars + m) n1 + j - r n1)
-// N0 + c], r = j / n1.  The product is rounded on its own, as k_upwind_div2d
-// rounds it before adding the x term.
+// N0 + c], r = j / n1.  The product is rounded on its own; k_upwind_div2d
+// fuses the x term's product onto it.
 template <int UPW, bool MX>
 __global__ void __launch_bounds__(256, 3) k_slab_upwind_y(DevParams P, const double* __restrict__ UT,
                                                        const void* __restrict__ yuL, const void* __restrict__ yuR,

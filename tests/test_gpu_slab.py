@@ -4,7 +4,8 @@ slab of the grid in one process (LocalSlabs), the exchanges as device
 copies.  The decomposed solution must equal the undecomposed one bit for
 bit: every value is formed by the same kernels from the same operands (the
 y lines are solved whole on their column slab; the y term of the divergence
-is rounded on its own before the x term is added, on both paths).
+is rounded on its own and the x term's product fused onto it, on both
+paths).
 """
 import os
 import shutil
