@@ -10,9 +10,10 @@ inputs of that shape.  A "step" is one SSPRK3 time step over the whole grid.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
 
 With N > 1 (torchrun, one process per GPU) every rank advances its own
-independent replica of the workload (a single grid does not shard without a
-halo exchange; replicas are the weakly scaled unit) and the timed region is
-bracketed by barriers with the max over ranks taken on the device clocks.
+independent replica of the workload (replicas are the weakly scaled unit)
+and the timed region is bracketed by barriers with the max over ranks taken
+on the device clocks.  --workload slab instead decomposes the one grid over
+the N ranks (row slabs with NCCL exchanges, strong scaling).
 
 --impl reference times the reference's own CPU implementation (the
 llnl/piafs binary built from source by oracle/Makefile, OpenMP on all host
@@ -61,7 +62,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="ns2d_photochem",
-                    choices=["ns2d_photochem", "euler1d", "ensemble", "serving"])
+                    choices=["ns2d_photochem", "euler1d", "ensemble", "serving", "slab"])
     ap.add_argument("--requests", type=int, default=1000, help="serving requests (the stream's first n)")
     ap.add_argument("--hbm-budget-gb", type=float, default=120.0)
     ap.add_argument("--max-resident-points", type=float, default=4e6,
@@ -506,6 +507,70 @@ def ensemble_figure(members=32, steps=20):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def slab_bench(a):
+    """One 2D photochemical grid decomposed over the N ranks (row slabs, NCCL
+    all-to-all exchanges; piafs_b200/slab.py): strong scaling of the default
+    workload's grid.  Needs N >= 2 GPUs.  Timed like the replicas: chunks of
+    steps from the initial condition, barrier-bracketed, CUDA events on each
+    rank's stream, max over ranks."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from piafs_b200.slab import SlabSimulation
+
+    rank, world, barrier = _dist_setup()
+    if world < 2:
+        sys.exit("bench.py --workload slab decomposes one grid over --gpus N >= 2 ranks")
+    tmp = tempfile.mkdtemp(prefix=f"piafs_slab_r{rank}_")
+    try:
+        a2 = argparse.Namespace(**{**vars(a), "workload": "ns2d_photochem"})
+        meta = make_deck(tmp, a2, a.warmup + a.steps)
+        sl = SlabSimulation(tmp, precision=a.precision)
+        N0, N1 = meta["size"]
+        stream = torch.cuda.ExternalStream(sl.stream)
+        u0 = sl.state()
+        t0 = 0.0
+
+        def chunks(n):
+            while n > 0:
+                k = min(chunk_steps(max(N0, N1)), n)
+                yield k
+                n -= k
+
+        for k in chunks(a.warmup):
+            sl.set_state(u0, t0)
+            sl.step(k)
+        total_ms = 0.0
+        for k in chunks(a.steps):
+            sl.set_state(u0, t0)
+            barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sl.step(k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            barrier()
+            total_ms += e0.elapsed_time(e1)
+        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        units = 3 * N0 * N1 * a.steps
+        if rank == 0:
+            line = {"metric": "pt-stage updates/s", "value": units / (ms / 1e3), "unit": "pt-stage updates/s",
+                    "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+                    "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic (seeded deck of the workload's shape)",
+                    "config": {"workload": f"ns2d_photochem_crweno5_llf_ssprk3_{N0}x{N1}_slabs{world}",
+                               "parallelism": f"row slabs x {world}", "precision": a.precision},
+                    "gpu_launches": None}
+            print(json.dumps(line))
+        sl.close()
+        return 0
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def relaunch_under_torchrun(a):
     """--gpus N > 1 started as a plain process: run the same command as N
     ranks (one per GPU) under torch.distributed.run and return its status."""
@@ -531,6 +596,8 @@ def main():
         return ensemble_bench(a)
     if a.workload == "serving" and a.impl == "gpu":
         return serving_bench(a)
+    if a.workload == "slab" and a.impl == "gpu":
+        return slab_bench(a)
 
     if a.impl == "reference":
         if rank != 0:

@@ -379,6 +379,21 @@ class SlabSimulation:
         i = self.slab.info
         return float(np.sqrt(t.item() / (i.dim[0] * i.dim[1])))
 
+    def state(self) -> np.ndarray:
+        """This slab's ghosted state (reference layout, host copy)."""
+        i = self.slab.info
+        u = np.empty((i.dim[0] + 2 * i.ghosts) * (i.slab_rows + 2 * i.ghosts) * i.nvars)
+        _check(self.slab.L.piafs_gpu_get_state(self.slab.sim, _hp(u)))
+        return u
+
+    def set_state(self, u: np.ndarray, t: float):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        _check(self.slab.L.piafs_gpu_set_state(self.slab.sim, _hp(u), float(t)))
+
+    @property
+    def stream(self) -> int:
+        return self.slab.stream
+
     def cfl(self) -> float:
         import torch
         t = torch.tensor([self.slab.cfl()], dtype=torch.float64, device="cuda")
