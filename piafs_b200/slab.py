@@ -308,14 +308,20 @@ def local_exchange(sync=lambda: None):
     return ex
 
 
-def dist_exchange(group=None):
+def dist_exchange(group=None, host_staging=False):
     """The exchange of one slab per rank of a torch.distributed group: one
-    all_to_all_single per exchange point."""
+    all_to_all_single per exchange point, on device buffers (NCCL), or
+    through host copies for a backend without device collectives (gloo)."""
     import torch.distributed as dist
 
     def ex(kind, sends, recvs, ss, rs):
-        dist.all_to_all_single(recvs[0], sends[0], output_split_sizes=rs[0] if rs else None,
-                               input_split_sizes=ss[0] if ss else None, group=group)
+        osz, isz = (rs[0] if rs else None), (ss[0] if ss else None)
+        if host_staging:
+            r = recvs[0].new_empty(recvs[0].shape, device="cpu")
+            dist.all_to_all_single(r, sends[0].cpu(), output_split_sizes=osz, input_split_sizes=isz, group=group)
+            recvs[0].copy_(r)
+        else:
+            dist.all_to_all_single(recvs[0], sends[0], output_split_sizes=osz, input_split_sizes=isz, group=group)
     return ex
 
 
@@ -357,6 +363,8 @@ class SlabSimulation:
     def __init__(self, deck_dir: str, precision: str = "fp64", group=None):
         import torch.distributed as dist
         self.dist, self.group = dist, group
+        # a backend without device collectives exchanges through host copies
+        self.host_staging = dist.get_backend(group) != "nccl"
         rank, world = dist.get_rank(group), dist.get_world_size(group)
         self.slab = _Slab(deck_dir, precision, rank, world)
 
@@ -370,14 +378,17 @@ class SlabSimulation:
         stream = torch.cuda.ExternalStream(self.slab.stream)
         with torch.cuda.stream(stream):
             for k in range(nsteps):
-                run_step([self.slab], dist_exchange(self.group), norm and k == nsteps - 1)
+                run_step([self.slab], dist_exchange(self.group, self.host_staging), norm and k == nsteps - 1)
         self.slab.synchronize()
         if not norm:
             return None
-        t = torch.tensor([self.slab.norm_sum()], dtype=torch.float64, device="cuda")
+        t = torch.tensor([self.slab.norm_sum()], dtype=torch.float64, device=self._coll_device())
         self.dist.all_reduce(t, group=self.group)
         i = self.slab.info
         return float(np.sqrt(t.item() / (i.dim[0] * i.dim[1])))
+
+    def _coll_device(self):
+        return "cpu" if self.host_staging else "cuda"
 
     def state(self) -> np.ndarray:
         """This slab's ghosted state (reference layout, host copy)."""
@@ -396,7 +407,7 @@ class SlabSimulation:
 
     def cfl(self) -> float:
         import torch
-        t = torch.tensor([self.slab.cfl()], dtype=torch.float64, device="cuda")
+        t = torch.tensor([self.slab.cfl()], dtype=torch.float64, device=self._coll_device())
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX, group=self.group)
         return t.item()
 

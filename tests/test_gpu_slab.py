@@ -83,3 +83,55 @@ def test_slabs_refuse_what_they_do_not_cover(tmp_path, name, nranks, what):
     d = copy_deck(name, str(tmp_path / name))
     with pytest.raises(PiafsError, match=what):
         LocalSlabs(d, nranks, precision="mixed" if what == "mixed precision" else "fp64")
+
+
+def _slab_rank(rank, world, port, d, out):
+    """One rank of a decomposed run as its own process (gloo, so the
+    exchanges go through host copies; both ranks share the one GPU, and no
+    kernel of one waits on the other's)."""
+    import torch
+    import torch.distributed as dist
+    from piafs_b200.slab import SlabSimulation
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        torch.cuda.set_device(0)
+        sim = SlabSimulation(d)
+        u0 = sim.state()
+        sim.step(2)
+        sim.set_state(u0, 0.0)                 # back to the start: the same run again
+        sim.step(NSTEPS - 1)
+        norm = sim.step(1, norm=True)
+        cfl = sim.cfl()
+        sol = sim.gather_solution()
+        sim.close()
+        if rank == 0:
+            np.save(out, sol)
+            np.save(out + ".diag.npy", np.array([norm, cfl]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slabs_as_processes_over_gloo(tmp_path):
+    import socket
+    import torch.multiprocessing as mp
+    d = copy_deck("ns2d_chem_crweno5_llf_64x48", str(tmp_path / "d"))
+    with Simulation(d) as sim:
+        sim.time_rk(NSTEPS - 1)
+        norm_ref = sim.time_rk_norm(1)
+        cfl_ref = sim.cfl()
+        ref = sim.solution()
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    out = str(tmp_path / "sol.npy")
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_slab_rank, args=(r, 2, port, d, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    assert np.array_equal(np.load(out), ref)
+    norm, cfl = np.load(out + ".diag.npy")
+    assert abs(norm - norm_ref) <= 1e-12 * norm_ref and abs(cfl - cfl_ref) <= 1e-14 * cfl_ref
