@@ -434,10 +434,7 @@ int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL
   const int N = dir == 0 ? P.N0 : P.N1;
   if (P.mixed && dir != 0) return -1;
   if (crweno_line_fits(N)) return launch_crweno_line(P, U, F, uL, uR, fL, fR, dir, err, s);
-  if (crweno_cluster_size(N) > 1) {
-    crweno_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s);
-    return 0;
-  }
+  if (crweno_cluster_size(N) > 1) return launch_crweno_seg(P, U, F, uL, uR, fL, fR, dir, err, s);
   switch (crweno_rows_per_thread(N)) {
     case 2: crweno_launch_m<2>(P, U, F, uL, uR, fL, fR, dir, err, s); break;
     case 4: crweno_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s); break;

@@ -33,10 +33,13 @@
 // rows use: they are formed at 30x (3x for the compact scheme's thirds, 10x
 // for the optimal weights 0.2, 0.5, 0.3) from unnormalised weights, and the
 // smoothness indicators at 4x with eps at 4x.  Quotients use rcp_nr.
+#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "crweno_solve.cuh"
 #include "kernels.h"
+
+namespace cg = cooperative_groups;
 
 namespace piafs {
 
@@ -85,6 +88,245 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
 }
 
 
+// Lines longer than one CTA serves (more than 4097 interfaces): a cluster
+// of ncta CTAs per line, CTA r owning the separators [r Pt, (r+1) Pt) and
+// their chunks of M rows.  Each CTA builds and reduces its chunks as above,
+// then solves its own part of the separator system by PCR with the two
+// unknowns outside it -- the previous CTA's last separator L and the next
+// CTA's first separator R -- carried as two extra columns (e, f) of every
+// row, so that after the local PCR every separator reads
+// X_k = d_k - e_k L - f_k R.  The first and last separators of every CTA
+// then form a system of 2 ncta unknowns, gathered from the cluster's shared
+// memory and solved by one thread of each CTA; L and R give every X_k.  Two
+// cluster barriers (the neighbour's last chunk row for the first separator
+// equation; the boundary rows) and a third before exit, instead of one per
+// PCR level across the cluster.
+template <int M, int DIR, int WT, bool MX>
+__global__ void __launch_bounds__(line_threads_max(), 1)
+    k_crw_seg(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
+              void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
+  typedef typename std::conditional<MX, float, double>::type R;   // weights' arithmetic
+  typedef typename std::conditional<MX, float, double>::type O;   // interface storage
+  extern __shared__ double2 sm2[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank(), ncta = (int)cl.num_blocks();
+  const int Pt = blockDim.x, k = threadIdx.x, lane = k & 31;
+  double2* pcA = sm2;              // PCR rows (a, c, d, e, f), both biases: [2 buffers][5][Pt]
+  double2* tp = sm2 + 10 * Pt;     // last-row coefficients (al, cg, rh) of each chunk: [3][Pt]
+  double2* sy = sm2 + 13 * Pt;     // separator values [Pt]
+  double2* bnd = sm2 + 14 * Pt;    // (d, e, f) of the first and the last separator; L, R
+  double* cs = (double*)(sm2 + 14 * Pt + 8);   // staged cells; later the output staging
+  O* so = (O*)cs;
+
+  const int line = (int)blockIdx.x / ncta, v = blockIdx.y;
+  const bool isF = blockIdx.z != 0;
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const long long st = DIR == 0 ? 1 : P.W0;
+  const long long ist = DIR == 0 ? 1 : P.N0;
+  const long long base = DIR == 0 ? pidx(P, 0, line) : pidx(P, line, 0);
+  const double* src = (isF ? F : U) + (long long)v * P.ps + base;
+  const long long ibase = DIR == 0 ? (long long)(P.N0 + 1) * line : line;
+  O* oL = (O*)(isF ? fL : uL) + (long long)v * P.pis + ibase;
+  O* oR = (O*)(isF ? fR : uR) + (long long)v * P.pis + ibase;
+  const double ref = MX ? src[0] : 0.0;
+  const int K = rank * Pt + k;               // separator of this thread in the line
+  const int rb = rank * Pt * M;              // rows before the segment
+  const int s = 1 + K * M;
+  const int kN = (N - 2) / M;                // separator owning row N-1
+  const R eps = R(4) * (R)P.eps;
+  int bad = 0;
+  // cells rb-3 .. rb+Pt M+2 at staged index j = cell - rb + 3, zero past N+2
+  {
+    const int ncell = Pt * M + 6;
+    double cv[M + 1];
+#pragma unroll
+    for (int it = 0; it <= M; it++) {
+      const int j = k + it * Pt;
+      cv[it] = (j < ncell && rb + j < N + 6) ? src[(rb + j - 3) * st] - ref : 0.0;
+    }
+#pragma unroll
+    for (int it = 0; it <= M; it++) {
+      const int j = k + it * Pt;
+      if (j < ncell) cs[cpad(j)] = cv[it];
+    }
+  }
+  double x0[2] = {0.0, 0.0}, xN[2] = {0.0, 0.0};
+  if (MX) {
+    if (K == 0) { x0[0] = crw_edge_f(P, src, st, 0, 1, ref); x0[1] = crw_edge_f(P, src, st, 0, -1, ref); }
+    if (K == kN) { xN[0] = crw_edge_f(P, src, st, N, 1, ref); xN[1] = crw_edge_f(P, src, st, N, -1, ref); }
+  } else {
+    if (K == 0) { x0[0] = crw_edge(P, src, st, 0, 1); x0[1] = crw_edge(P, src, st, 0, -1); }
+    if (K == kN) { xN[0] = crw_edge(P, src, st, N, 1); xN[1] = crw_edge(P, src, st, N, -1); }
+  }
+  __syncthreads();
+
+  double As[2], Bs[2], Cs[2], Rs[2];
+  double al[2][M], cg_[2][M], rh[2][M];
+  const int Kw = K - lane;                   // first separator of this warp
+  if (Kw >= 1 && (Kw + 32) * M <= N - 2)
+    crw_chunk<M, WT, true, R>(cs, k, s, N, x0, xN, eps, As, Bs, Cs, Rs, al, cg_, rh, bad);
+  else
+    crw_chunk<M, WT, false, R>(cs, k, s, N, x0, xN, eps, As, Bs, Cs, Rs, al, cg_, rh, bad);
+  tp[k] = make_double2(al[0][M - 1], al[1][M - 1]);
+  tp[Pt + k] = make_double2(cg_[0][M - 1], cg_[1][M - 1]);
+  tp[2 * Pt + k] = make_double2(rh[0][M - 1], rh[1][M - 1]);
+  cl.sync();   // the previous CTA's last chunk row is read below
+
+  // separator equations, scaled to a unit diagonal; the first separator of
+  // CTA r > 0 couples to the previous CTA's last one (L, column e) and the
+  // last of CTA r < ncta-1 to the next CTA's first (R, column f)
+  double a[2], cq[2], d[2], e[2], f[2];
+  {
+    double2 alp = make_double2(0.0, 0.0), gap = alp, rhp = alp;
+    if (k > 0) {
+      alp = tp[k - 1]; gap = tp[Pt + k - 1]; rhp = tp[2 * Pt + k - 1];
+    } else if (rank > 0) {
+      const double2* rt = cl.map_shared_rank(tp, rank - 1);
+      alp = rt[Pt - 1]; gap = rt[2 * Pt - 1]; rhp = rt[3 * Pt - 1];
+    }
+    const double alq[2] = {alp.x, alp.y}, gaq[2] = {gap.x, gap.y}, rhq[2] = {rhp.x, rhp.y};
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const double b = Bs[q] - As[q] * gaq[q] - Cs[q] * al[q][1];
+      bad |= (b == 0.0);
+      const double rbq = rcp_nr(b);
+      a[q] = -(As[q] * alq[q]) * rbq;
+      cq[q] = -(Cs[q] * cg_[q][1]) * rbq;
+      d[q] = (Rs[q] - As[q] * rhq[q] - Cs[q] * rh[q][1]) * rbq;
+      e[q] = 0.0;
+      f[q] = 0.0;
+      if (k == 0) { e[q] = a[q]; a[q] = 0.0; }
+      if (k == Pt - 1) { f[q] = cq[q]; cq[q] = 0.0; }
+    }
+  }
+  auto put = [&](double2* row) {
+    row[k] = make_double2(a[0], a[1]);
+    row[Pt + k] = make_double2(cq[0], cq[1]);
+    row[2 * Pt + k] = make_double2(d[0], d[1]);
+    row[3 * Pt + k] = make_double2(e[0], e[1]);
+    row[4 * Pt + k] = make_double2(f[0], f[1]);
+  };
+  put(pcA);
+  __syncthreads();
+  // PCR within the CTA (rows outside it: zero couplings, clamped as in
+  // line_pair_solve), the external unknowns' columns updated alongside
+  int buf = 0;
+  for (int dl = 1; dl < Pt; dl <<= 1) {
+    const double2* cur = pcA + buf * 5 * Pt;
+    const int km = k >= dl ? k - dl : k, kp = k + dl < Pt ? k + dl : k;
+    const double2 am = cur[km], cm = cur[Pt + km], dm = cur[2 * Pt + km], em = cur[3 * Pt + km],
+                  fm = cur[4 * Pt + km];
+    const double2 ap = cur[kp], cp = cur[Pt + kp], dp = cur[2 * Pt + kp], ep = cur[3 * Pt + kp],
+                  fp = cur[4 * Pt + kp];
+    const double amq[2] = {am.x, am.y}, cmq[2] = {cm.x, cm.y}, dmq[2] = {dm.x, dm.y}, emq[2] = {em.x, em.y},
+                 fmq[2] = {fm.x, fm.y};
+    const double apq[2] = {ap.x, ap.y}, cpq[2] = {cp.x, cp.y}, dpq[2] = {dp.x, dp.y}, epq[2] = {ep.x, ep.y},
+                 fpq[2] = {fp.x, fp.y};
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const double bn = 1.0 - a[q] * cmq[q] - cq[q] * apq[q];
+      const double rbq = rcp_nr(bn);
+      const double an = -(a[q] * amq[q]) * rbq, cn = -(cq[q] * cpq[q]) * rbq;
+      d[q] = (d[q] - a[q] * dmq[q] - cq[q] * dpq[q]) * rbq;
+      e[q] = (e[q] - a[q] * emq[q] - cq[q] * epq[q]) * rbq;
+      f[q] = (f[q] - a[q] * fmq[q] - cq[q] * fpq[q]) * rbq;
+      a[q] = an; cq[q] = cn;
+    }
+    put(pcA + (buf ^ 1) * 5 * Pt);
+    buf ^= 1;
+    __syncthreads();
+  }
+  // X_k = d_k - e_k L - f_k R; the first and last rows to the cluster
+  if (k == 0) { bnd[0] = make_double2(d[0], d[1]); bnd[1] = make_double2(e[0], e[1]); bnd[2] = make_double2(f[0], f[1]); }
+  if (k == Pt - 1) { bnd[3] = make_double2(d[0], d[1]); bnd[4] = make_double2(e[0], e[1]); bnd[5] = make_double2(f[0], f[1]); }
+  cl.sync();
+  if (k == 0) {
+    // unknowns F_c (first separator of CTA c) = z[2c], G_c (last) = z[2c+1]:
+    //   F_c + e0_c G_{c-1} + f0_c F_{c+1} = d0_c,  G_c + el_c G_{c-1} + fl_c F_{c+1} = dl_c
+    // (no G_{-1}, no F_{ncta}: those columns are zero), banded elimination
+    // without pivoting (the off-diagonal columns are what the local PCR left
+    // of single couplings, below one in magnitude)
+    constexpr int MAXC = 8;
+    double A[2][2 * MAXC][2 * MAXC], z[2][2 * MAXC];
+    const int n = 2 * ncta;
+    for (int c = 0; c < ncta; c++) {
+      const double2* rb2 = cl.map_shared_rank(bnd, c);
+      const double2 d0 = rb2[0], e0 = rb2[1], f0 = rb2[2], dl2 = rb2[3], el = rb2[4], fl = rb2[5];
+      const double d0q[2] = {d0.x, d0.y}, e0q[2] = {e0.x, e0.y}, f0q[2] = {f0.x, f0.y};
+      const double dlq[2] = {dl2.x, dl2.y}, elq[2] = {el.x, el.y}, flq[2] = {fl.x, fl.y};
+      for (int q = 0; q < 2; q++) {
+        for (int j = 0; j < n; j++) { A[q][2 * c][j] = 0.0; A[q][2 * c + 1][j] = 0.0; }
+        A[q][2 * c][2 * c] = 1.0;
+        A[q][2 * c + 1][2 * c + 1] = 1.0;
+        if (c > 0) { A[q][2 * c][2 * c - 1] = e0q[q]; A[q][2 * c + 1][2 * c - 1] = elq[q]; }
+        if (c + 1 < ncta) { A[q][2 * c][2 * c + 2] = f0q[q]; A[q][2 * c + 1][2 * c + 2] = flq[q]; }
+        z[q][2 * c] = d0q[q];
+        z[q][2 * c + 1] = dlq[q];
+      }
+    }
+    for (int q = 0; q < 2; q++) {
+      for (int i = 0; i < n; i++) {
+        const double piv = A[q][i][i];
+        bad |= (piv == 0.0);
+        const double ip = 1.0 / piv;
+        for (int r = i + 1; r < n && r <= i + 3; r++) {
+          const double m = A[q][r][i] * ip;
+          if (m == 0.0) continue;
+          for (int j = i; j < n && j <= i + 3; j++) A[q][r][j] -= m * A[q][i][j];
+          z[q][r] -= m * z[q][i];
+        }
+      }
+      for (int i = n - 1; i >= 0; i--) {
+        double t = z[q][i];
+        for (int j = i + 1; j < n && j <= i + 3; j++) t -= A[q][i][j] * z[q][j];
+        z[q][i] = t / A[q][i][i];
+      }
+    }
+    const double L0 = rank > 0 ? z[0][2 * rank - 1] : 0.0, L1 = rank > 0 ? z[1][2 * rank - 1] : 0.0;
+    const double R0 = rank + 1 < ncta ? z[0][2 * rank + 2] : 0.0, R1 = rank + 1 < ncta ? z[1][2 * rank + 2] : 0.0;
+    bnd[6] = make_double2(L0, L1);
+    bnd[7] = make_double2(R0, R1);
+  }
+  cl.sync();   // every CTA's reads of the others' shared memory are done
+  const double2 Lv = bnd[6], Rv = bnd[7];
+  const double Lq[2] = {Lv.x, Lv.y}, Rq[2] = {Rv.x, Rv.y};
+#pragma unroll
+  for (int q = 0; q < 2; q++) d[q] = d[q] - e[q] * Lq[q] - f[q] * Rq[q];
+  sy[k] = make_double2(d[0], d[1]);
+  __syncthreads();
+
+  // recover the segment's rows into the output staging (index row - rb)
+  const double2 xn = k + 1 < Pt ? sy[k + 1] : Rv;
+  {
+    const double2 l0 = tp[k], l1 = tp[Pt + k], l2 = tp[2 * Pt + k];
+    al[0][M - 1] = l0.x; al[1][M - 1] = l0.y;
+    cg_[0][M - 1] = l1.x; cg_[1][M - 1] = l1.y;
+    rh[0][M - 1] = l2.x; rh[1][M - 1] = l2.y;
+  }
+  const int ostride = opad(Pt * M + 1) + 1;
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const double Xk = d[q], Xn = q == 0 ? xn.x : xn.y;
+    O* o = so + q * ostride;
+    if (s <= N - 1) o[opad(s - rb)] = (O)Xk;
+#pragma unroll
+    for (int r = 1; r < M; r++) {
+      const int i = s + r;
+      if (i <= N - 1) o[opad(i - rb)] = (O)(rh[q][r] - al[q][r] * Xk - cg_[q][r] * Xn);
+    }
+    if (K == 0) o[0] = (O)x0[q];
+    if (K == kN) o[opad(N - rb)] = (O)xN[q];
+  }
+  if (bad) atomicOr(err, 1);
+  __syncthreads();
+  const int lo = rank == 0 ? 0 : rb + 1;
+  const int hi = kN / Pt == rank ? N : min(N - 1, rb + Pt * M);
+  for (int i = lo + k; i <= hi; i += Pt) {
+    oL[i * ist] = so[opad(i - rb)];
+    oR[i * ist] = so[ostride + opad(i - rb)];
+  }
+}
+
 // shared memory of a launch: PCR rows, last-row coefficients, separators,
 // and the larger of the staged cells and the output staging
 template <int M, bool MX>
@@ -93,6 +335,51 @@ size_t line_smem(int N, int Pt) {
   const size_t cells = (size_t)(Pt * M + 6 + (Pt * M + 6) / 8 + 1) * sizeof(double);
   const size_t outs = (size_t)2 * (N + N / 16 + 1) * osz;
   return (size_t)10 * Pt * sizeof(double2) + (cells > outs ? cells : outs);
+}
+
+template <bool MX>
+size_t seg_smem(int Pt) {
+  const size_t osz = MX ? sizeof(float) : sizeof(double);
+  const int M = 8;
+  const size_t cells = (size_t)(Pt * M + 6 + (Pt * M + 6) / 8 + 1) * sizeof(double);
+  const size_t outs = (size_t)2 * (opad(Pt * M + 1) + 1) * osz;
+  return (size_t)(14 * Pt + 8) * sizeof(double2) + (cells > outs ? cells : outs);
+}
+
+template <int DIR, int WT, bool MX>
+void seg_launch(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                int* err, int ncta, cudaStream_t s) {
+  constexpr int M = 8;
+  const int N = DIR == 0 ? P.N0 : P.N1;
+  const int nlines = DIR == 0 ? P.N1 : P.N0;
+  const int chunks = (N - 1 + M - 1) / M;
+  const int Pt = ((chunks + ncta - 1) / ncta + 31) / 32 * 32;
+  raise_smem_limit<k_crw_seg<M, DIR, WT, MX>>((int)seg_smem<MX>(line_threads_max()));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nlines * ncta), (unsigned)P.nvars, 2);
+  cfg.blockDim = dim3((unsigned)Pt, 1, 1);
+  cfg.dynamicSmemBytes = seg_smem<MX>(Pt);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)ncta;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_crw_seg<M, DIR, WT, MX>, P, U, F, uL, uR, fL, fR, err);
+}
+
+template <int DIR, bool MX>
+void seg_launch_wt(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                   int* err, int ncta, cudaStream_t s) {
+  if (P.no_limiting) return seg_launch<DIR, WT_NOLIM, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+  switch (P.weno_type) {
+    case W_MAPPED: return seg_launch<DIR, W_MAPPED, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+    case W_BORGES: return seg_launch<DIR, W_BORGES, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+    case W_YC: return seg_launch<DIR, W_YC, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+    default: return seg_launch<DIR, W_JS, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+  }
 }
 
 template <int M, int DIR, int WT, bool MX>
@@ -131,6 +418,18 @@ void line_launch_m(const DevParams& P, const double* U, const double* F, void* u
 // lines of 3 .. 4097 interfaces: 8 rows per thread from 128 interfaces up
 // (up to 512 threads), 4 below
 bool crweno_line_fits(int N) { return N >= 3 && line_threads_m<8>(N) <= line_threads_max(); }
+
+// lines of 4098 .. 32769 interfaces: clusters of up to 8 CTAs
+int launch_crweno_seg(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
+                      int dir, int* err, cudaStream_t s) {
+  const int N = dir == 0 ? P.N0 : P.N1;
+  const int ncta = crweno_cluster_size(N);
+  if (ncta < 2 || (P.mixed && dir != 0)) return -1;
+  if (P.mixed) seg_launch_wt<0, true>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+  else if (dir == 0) seg_launch_wt<0, false>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+  else seg_launch_wt<1, false>(P, U, F, uL, uR, fL, fR, err, ncta, s);
+  return 0;
+}
 
 int launch_crweno_line(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
                        void* fR, int dir, int* err, cudaStream_t s) {

@@ -170,6 +170,11 @@ int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL
 bool crweno_line_fits(int N);
 int launch_crweno_line(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
                        void* fR, int dir, int* err, cudaStream_t s);
+// longer lines (up to 32769 interfaces) by clusters of CTAs that solve their
+// segments' separator systems locally and couple them through one small
+// system (crweno_line.cu); -1 if the line is not one of those
+int launch_crweno_seg(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
+                      void* fR, int dir, int* err, cudaStream_t s);
 // CRWENO5 on characteristic variables (crweno_char.cu; 1D Euler and 2D
 // Navier-Stokes without chemistry, FP64): all four interface arrays of
 // direction dir; scratch holds crweno_char_scratch(P) doubles; *err is set on

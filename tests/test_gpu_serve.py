@@ -3,7 +3,9 @@
 A request's deck is written in memory and its fields generated on the
 device; it must reproduce the same solve set up from the case generator's
 deck files (the fields agree up to the last bit of sin / exp), and it must
-give the same result, bit for bit, alone and in the served mix.
+give the same result, bit for bit, alone and in the served mix (checksums
+through the serving loop, whole solutions through the same continuous
+batching driven step by step; FP64 and mixed precision).
 """
 import os
 
@@ -22,8 +24,8 @@ def rel_l2(got, ref):
     return np.where(den > 1e-15, num / np.maximum(den, 1e-300), num).max()
 
 
-def one(req):
-    with Batch() as b:
+def one(req, precision="fp64"):
+    with Batch(precision=precision) as b:
         i = b.add_request(req)
         b.step(req.nsteps)
         return b.solution(i), b.checksum(i)
@@ -69,6 +71,41 @@ def test_served_results_equal_alone_results():
         assert r["steps"] == q.nsteps
         _, cs = one(q)
         assert r["checksum"] == cs
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_served_checksums_equal_alone_checksums(precision):
+    reqs, arr = small_trace(24)
+    res = serve_trace(reqs, arr, precision=precision, steps_per_round=3)
+    for q, r in zip(reqs, res):
+        _, cs = one(q, precision)
+        assert r["checksum"] == cs
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_continuous_batching_full_solutions_equal_alone(precision):
+    """The serving loop's pattern -- requests joining a batch whose other
+    members are part-way through their steps, finished members polled out
+    and removed while the rest go on -- leaves every member's whole solution
+    bit for bit as it is alone."""
+    reqs, _ = small_trace(16)
+    alone = [one(q, precision)[0] for q in reqs]
+    got = {}
+    with Batch(precision=precision) as b:
+        ids = {}
+        pending = list(range(len(reqs)))
+        while pending or ids:
+            for _ in range(min(3, len(pending))):       # a few arrivals per round
+                k = pending.pop(0)
+                ids[b.add_request(reqs[k])] = k
+            b.step(2)
+            for i in b.poll():
+                got[ids[i]] = b.solution(i)
+                b.remove(i)
+                del ids[i]
+    assert sorted(got) == list(range(len(reqs)))
+    for k, ref in enumerate(alone):
+        assert np.array_equal(got[k], ref), (k, precision)
 
 
 def test_serving_under_a_small_budget():
