@@ -22,26 +22,18 @@
 //   * every row is recovered from its two separators and the results are
 //     staged in shared memory so that the x-direction stores are coalesced.
 //
-// Lines longer than one CTA serves (T M + 1 interfaces, 4097 at M = 8) run as
-// a thread-block cluster of up to 8 CTAs per line (CL): each CTA reduces a
-// segment of consecutive chunks, the separator system of the whole line is
-// solved by the same parallel cyclic reduction across the cluster, each step
-// reading the neighbours' rows from the other CTAs' shared memory
-// (distributed shared memory) between cluster barriers, and every CTA
-// recovers and stores its own segment.
+// The lines of a grid run through k_crw_line and k_crw_seg (crweno_line.cu):
+// this kernel serves the lines those do not (fewer than three interfaces).
 //
 // Rows 0 and N are the WENO5 rows with the WENO5 optimal weights (physical
 // boundaries, also on periodic domains, Interp1PrimFifthOrderCRWENO.c:164-175);
 // they are computed directly and folded into rows 1 and N-1.  Rows past N-1
 // are identity rows.  Divisions are reciprocals by Newton-Raphson refinement
 // (rcp_nr), so results agree with the reference to rounding, not bit for bit.
-#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "crweno_common.cuh"
 #include "kernels.h"
-
-namespace cg = cooperative_groups;
 
 namespace piafs {
 
@@ -65,9 +57,7 @@ __device__ __forceinline__ int stg(int i) { return i + (i >> 4); }
 // otherwise
 __host__ __device__ constexpr int crweno_max_threads(int M) { return M == 8 ? 512 : 256; }
 
-// CL: the line is shared by the CTAs of a cluster (blockIdx.x = line x
-// cluster size + rank), the separator index of a thread is rank x Pt + k.
-template <int M, int DIR, int WT, bool MX, bool CL = false>
+template <int M, int DIR, int WT, bool MX>
 __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     k_crweno_pair(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
                   void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
@@ -80,30 +70,10 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
   double* tp = sm + 12 * Pt;     // last-row coefficients per chunk, [2][3][Pt]
   double* sy = sm + 18 * Pt;     // separator values, [2][Pt]
   double* so = sm + 20 * Pt;     // output staging, [2][stg(rows of the segment) + 1]
-  // cluster: rank of this CTA, separators of the line, first row of the segment
-  int rank = 0, ncta = 1;
-  if constexpr (CL) {
-    rank = (int)cg::this_cluster().block_rank();
-    ncta = (int)cg::this_cluster().num_blocks();
-  }
-  const int K = rank * Pt + k, Ptot = ncta * Pt;
-  const int rowbase = rank * Pt * M;
-  auto sync = [&]() {
-    if constexpr (CL) cg::this_cluster().sync();
-    else __syncthreads();
-  };
-  // a shared-memory value of separator index j of the line (this CTA or,
-  // in a cluster, the CTA that owns it)
-  auto at = [&](double* arr, int j) -> double {
-    if constexpr (CL) {
-      const int r = j / Pt;
-      if (r != rank) return *cg::this_cluster().map_shared_rank(arr + (j - r * Pt), r);
-      return arr[j - r * Pt];
-    } else {
-      return arr[j];
-    }
-  };
-  const int line = CL ? (int)blockIdx.x / ncta : (int)blockIdx.x, v = blockIdx.y;
+  const int K = k, Ptot = Pt;
+  auto sync = [&]() { __syncthreads(); };
+  auto at = [&](double* arr, int j) -> double { return arr[j]; };
+  const int line = (int)blockIdx.x, v = blockIdx.y;
   const bool isF = blockIdx.z != 0;
   const int N = DIR == 0 ? P.N0 : P.N1;
   const long long st = DIR == 0 ? 1 : P.W0;
@@ -277,7 +247,7 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
   sync();
 
   // ---- recover every row
-  if constexpr (!CL) {
+  {
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       const double Xk = d[q];
@@ -296,36 +266,6 @@ __global__ void __launch_bounds__(crweno_max_threads(M), (M <= 4 ? 2 : 1))
     for (int i = k; i <= N; i += Pt) {
       oL[i * ist] = (O)so[stg(i)];
       oR[i * ist] = (O)so[stg(N) + 1 + stg(i)];
-    }
-  } else {
-    // staged at the row's index in this CTA's segment
-    const int nst = min(N, rowbase + Pt * M + 1) - rowbase;   // last staged row of the segment
-    double Xn2[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) Xn2[q] = K + 1 < Ptot ? at(sy + q * Pt, K + 1) : 0.0;
-    sync();     // the last reads of other CTAs' shared memory are done
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      const double Xk = d[q];
-      const double Xn = Xn2[q];
-      double* o = so + q * (stg(nst) + 1);
-      if (s <= N - 1) o[stg(s - rowbase)] = Xk;
-#pragma unroll
-      for (int r = 1; r < M; r++) {
-        const int i = s + r;
-        if (i <= N - 1) o[stg(i - rowbase)] = rh[q][r] - al[q][r] * Xk - cg[q][r] * Xn;
-      }
-      if (K == 0) o[0] = x0[q];
-      if (K == kN) o[stg(N - rowbase)] = xN[q];
-    }
-    __syncthreads();
-    // rows of this segment: [rowbase + 1, rowbase + Pt M] within [1, N - 1],
-    // with row 0 in the first segment and row N in the segment holding N - 1
-    const int lo = rank == 0 ? 0 : rowbase + 1;
-    const int hi = (kN / Pt == rank) ? N : min(N - 1, rowbase + Pt * M);
-    for (int i = lo + k; i <= hi; i += Pt) {
-      oL[i * ist] = (O)so[stg(i - rowbase)];
-      oR[i * ist] = (O)so[stg(nst) + 1 + stg(i - rowbase)];
     }
   }
 }
@@ -354,46 +294,11 @@ int crweno_cluster_size(int N) {
 
 namespace {
 
-// a line shared by a cluster of CTAs (M = 8): the separators split evenly,
-// each CTA staging its segment
-template <int DIR, int WT, bool MX>
-void crweno_launch_cluster(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
-                           void* fR, int* err, int ncta, cudaStream_t s) {
-  constexpr int M = 8;
-  const int N = DIR == 0 ? P.N0 : P.N1;
-  const int nlines = DIR == 0 ? P.N1 : P.N0;
-  const int chunks = (N - 1 + M - 1) / M;
-  int Pt = (chunks + ncta - 1) / ncta;
-  Pt = ((Pt + 31) / 32) * 32;
-  const int seg = Pt * M + 1;
-  const size_t smem = (size_t)(20 * Pt + 2 * (seg + (seg >> 4) + 1)) * sizeof(double);
-  constexpr int T = crweno_max_threads(M);
-  raise_smem_limit<k_crweno_pair<M, DIR, WT, MX, true>>(
-      (20 * T + 2 * (T * M + 1 + ((T * M + 1) >> 4) + 1)) * (int)sizeof(double));
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(nlines * ncta), (unsigned)P.nvars, 2);
-  cfg.blockDim = dim3((unsigned)Pt, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)ncta;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_crweno_pair<M, DIR, WT, MX, true>, P, U, F, uL, uR, fL, fR, err);
-}
-
 template <int M, int DIR, int WT, bool MX>
 void crweno_launch(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
                    int* err, cudaStream_t s) {
   const int N = DIR == 0 ? P.N0 : P.N1;
   const int nlines = DIR == 0 ? P.N1 : P.N0;
-  if constexpr (M == 8) {
-    const int ncta = crweno_cluster_size(N);
-    if (ncta > 1) return crweno_launch_cluster<DIR, WT, MX>(P, U, F, uL, uR, fL, fR, err, ncta, s);
-  }
   int Pt = (N - 1 + M - 1) / M;
   Pt = ((Pt + 31) / 32) * 32;
   const size_t smem = (size_t)(20 * Pt + 2 * (N + (N >> 4) + 1)) * sizeof(double);
