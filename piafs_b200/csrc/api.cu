@@ -82,24 +82,6 @@ void piafs::enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* cons
     mark();
     return;
   }
-  if (s->fuse_species) {
-    // flow variables' interface values, the passive variables' upwinding
-    // speed from them, then the passive variables reconstructed, upwinded
-    // and differenced into the uL arrays of those variables; the speed in
-    // the uR array of the first of them
-    const DevParams& Q = d == 0 ? P : s->PT;
-    const double* cells = d == 0 ? U : s->ut;
-    if (d == 1) launch_transpose(P, U, s->ut, s->stream);
-    launch_flux(P, cells, s->fC, d, s->stream);
-    mark();
-    void* speed = P.mixed ? (void*)((float*)I[1] + (long long)P.nflow * P.pis)
-                          : (void*)(I[1] + (long long)P.nflow * P.pis);
-    launch_crweno_line(Q, cells, s->fC, I[0], I[1], I[2], I[3], 0, s->err, s->stream, 0, P.nflow);
-    launch_species_speed(Q, cells, I[0], I[1], speed, d, s->stream);
-    launch_crweno_species(Q, cells, s->fC, speed, I[0], s->err, s->stream);
-    mark();
-    return;
-  }
   if (d == 1 && s->ut) {
     launch_transpose(P, U, s->ut, s->stream);
     launch_flux(P, s->ut, s->fC, 1, s->stream);
@@ -131,11 +113,7 @@ static void enqueue_hyp(piafs_gpu_sim* s, const double* U, double* out, bool neg
     enqueue_recon(s, U, 1, s->iface_y, ev, k);
     const void* xi[4] = {s->iface[0], s->iface[1], s->iface[2], s->iface[3]};
     const void* yi[4] = {s->iface_y[0], s->iface_y[1], s->iface_y[2], s->iface_y[3]};
-    if (s->fuse_species)
-      launch_upwind_div2d_sp(P, U, s->ut, xi, yi, s->iface[0], s->iface_y[0], s->dxinv, out, neg ? 1 : 0,
-                             s->stream);
-    else
-      launch_upwind_div2d(P, U, s->ut, xi, yi, s->dxinv, out, neg ? 1 : 0, s->stream);
+    launch_upwind_div2d(P, U, s->ut, xi, yi, s->dxinv, out, neg ? 1 : 0, s->stream);
   }
   if (ev) cudaEventRecord(ev[++*k], s->stream);
 }
@@ -289,11 +267,6 @@ int piafs::create_sim(Deck&& deck, int precision, piafs_gpu_sim** out) {
     e = alloc(&s->ut, planes);
     s->PT = transposed_params(P);
   }
-  // PIAFS_GPU_NO_FUSED_SPECIES=1 keeps the passive variables in the separate
-  // upwind kernel (the same values; for checking the fused path against it)
-  const char* nfs = std::getenv("PIAFS_GPU_NO_FUSED_SPECIES");
-  s->fuse_species = s->ut && P.model == NS2D && P.nvars > P.nflow && crweno_line_fits(P.N0) &&
-                    crweno_line_fits(P.N1) && !(nfs && nfs[0] == '1');
   if (e == cudaSuccess) e = alloc(&s->dxinv, d.dxinv.size());
   if (e == cudaSuccess) e = alloc(&s->imap, d.imap.size());
   if (e == cudaSuccess) e = alloc(&s->tdev, 1);
@@ -385,8 +358,7 @@ int piafs_gpu_get_info(piafs_gpu_sim* s, piafs_gpu_info* info) {
   const int nz = (int)d.zones.size();
   const int vs = ((s->P.ndims == 2 && s->P.viscous) || s->P.chem) ? 1 : 0;
   const int tr = s->ut ? 1 : 0;
-  const int fs = s->fuse_species ? 4 : 0;   // speed and species kernels of both directions
-  info->launches_per_step = nz + d.nstages * (2 * s->P.ndims + 1 + tr + vs + fs) + (d.nstages - 1) * (1 + nz) + 2;
+  info->launches_per_step = nz + d.nstages * (2 * s->P.ndims + 1 + tr + vs) + (d.nstages - 1) * (1 + nz) + 2;
   return PIAFS_OK;
 }
 

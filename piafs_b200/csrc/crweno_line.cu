@@ -38,7 +38,6 @@
 
 #include "crweno_solve.cuh"
 #include "kernels.h"
-#include "physics.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -51,7 +50,7 @@ namespace {
 template <int M, int DIR, int WT, bool MX>
 __global__ void __launch_bounds__(line_threads_max(), 1)
     k_crw_line(DevParams P, const double* __restrict__ U, const double* __restrict__ F, void* __restrict__ uL,
-               void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err, int v0) {
+               void* __restrict__ uR, void* __restrict__ fL, void* __restrict__ fR, int* __restrict__ err) {
   typedef typename std::conditional<MX, float, double>::type R;   // weights' arithmetic
   typedef typename std::conditional<MX, float, double>::type O;   // interface storage
   extern __shared__ double2 sm2[];
@@ -62,7 +61,7 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
   double* cs = (double*)(sm2 + 10 * Pt);   // staged cells; later the output staging
   O* so = (O*)(sm2 + 10 * Pt);
 
-  const int line = blockIdx.x, v = v0 + (int)blockIdx.y;
+  const int line = blockIdx.x, v = blockIdx.y;
   const bool isF = blockIdx.z != 0;
   const int N = DIR == 0 ? P.N0 : P.N1;
   const long long st = DIR == 0 ? 1 : P.W0;            // cell stride along the line
@@ -88,59 +87,6 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
   }
 }
 
-
-// The passive variables of 2D Navier-Stokes (variables nflow .. nvars-1)
-// with their upwinding and flux difference in the epilogue: one CTA per line
-// and variable solves the u and the f systems (both biases) one after the
-// other, keeps all four interface values in shared memory, forms the upwind
-// flux of every interface from the flow's speed at that interface
-// (upwind_species: the scalar eigenvalue treatment of
-// NavierStokes2DUpwind.c), and writes only fI[i+1] - fI[i] of every cell
-// (dterm[v][i + N line]) -- one plane instead of four interface planes, and
-// nothing for the upwind kernel to re-read.  The values are those the
-// separate upwind kernel forms.  SPM: the species mode, 0 (Roe, Rusanov) or
-// 1 (LLF) for every interface, 2 (RF) encoded in the speed plane (the speed
-// itself for mode 1, -1 for mode 2 (fL), -2 for mode 3 (fR)).  x lines and
-// the y lines of a transposed state (unit stride).
-template <int M, int WT, bool MX, int SPM>
-__global__ void __launch_bounds__(line_threads_max(), 1)
-    k_crw_species(DevParams P, const double* __restrict__ U, const double* __restrict__ F,
-                  const void* __restrict__ speed, void* __restrict__ dterm, int* __restrict__ err) {
-  typedef typename std::conditional<MX, float, double>::type R;
-  typedef typename std::conditional<MX, float, double>::type O;
-  extern __shared__ double2 sm2[];
-  const int Pt = blockDim.x, k = threadIdx.x;
-  const int N = P.N0;
-  const int ostride = opad(N) + 1;
-  double2* pcA = sm2;
-  double2* tp = sm2 + 6 * Pt;
-  double2* sy = sm2 + 9 * Pt;
-  O* su = (O*)(sm2 + 10 * Pt);                                   // u interface values, both biases
-  double* cs = (double*)(sm2 + 10 * Pt + (2 * ostride * (int)sizeof(O) + 15) / 16);
-  O* sf = (O*)cs;                                                // f interface values
-  const int line = blockIdx.x, v = P.nflow + (int)blockIdx.y;
-  const long long base = pidx(P, 0, line);
-  const double* srcU = U + (long long)v * P.ps + base;
-  const double* srcF = F + (long long)v * P.ps + base;
-  int bad = 0;
-  line_pair_solve<M, WT, R, O>(P, srcU, 1, MX ? srcU[0] : 0.0, N, cs, pcA, tp, sy, su, bad);
-  line_pair_solve<M, WT, R, O>(P, srcF, 1, MX ? srcF[0] : 0.0, N, cs, pcA, tp, sy, sf, bad);
-  if (bad) atomicOr(err, 1);
-  O* fi = (O*)pcA;                                               // N + 1 interface fluxes
-  const O* spd = (const O*)speed + (long long)(N + 1) * line;
-  for (int i = k; i <= N; i += Pt) {
-    const O a = spd[i];
-    int mode;
-    O alpha = a;
-    if (SPM == 0) mode = 0;
-    else if (SPM == 1) mode = 1;
-    else { mode = a >= O(0) ? 1 : (a == O(-1) ? 2 : 3); alpha = a >= O(0) ? a : O(0); }
-    fi[i] = upwind_species(mode, alpha, su[opad(i)], su[ostride + opad(i)], sf[opad(i)], sf[ostride + opad(i)]);
-  }
-  __syncthreads();
-  O* out = (O*)dterm + (long long)v * P.pis + (long long)N * line;
-  for (int i = k; i < N; i += Pt) out[i] = fi[i + 1] - fi[i];
-}
 
 // Lines longer than one CTA serves (more than 4097 interfaces): a cluster
 // of ncta CTAs per line, CTA r owning the separators [r Pt, (r+1) Pt) and
@@ -438,71 +384,33 @@ void seg_launch_wt(const DevParams& P, const double* U, const double* F, void* u
 
 template <int M, int DIR, int WT, bool MX>
 void line_launch(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
-                 int* err, cudaStream_t s, int v0, int nv) {
+                 int* err, cudaStream_t s, int nv) {
   const int N = DIR == 0 ? P.N0 : P.N1;
   const int Pt = line_threads_m<M>(N);
   constexpr int T = line_threads_max();
   raise_smem_limit<k_crw_line<M, DIR, WT, MX>>((int)line_smem<M, MX>(T * M + 1, T));
   dim3 grid(DIR == 0 ? P.N1 : P.N0, nv, 2);
-  k_crw_line<M, DIR, WT, MX><<<grid, Pt, line_smem<M, MX>(N, Pt), s>>>(P, U, F, uL, uR, fL, fR, err, v0);
-}
-
-// shared memory of a species launch: the line solve's, with the u interface
-// values kept beside the cells / f values
-template <int M, bool MX>
-size_t species_smem(int N, int Pt) {
-  const size_t osz = MX ? sizeof(float) : sizeof(double);
-  const size_t su = ((size_t)2 * (opad(N) + 1) * osz + 15) / 16 * 16;
-  return line_smem<M, MX>(N, Pt) + su;
-}
-
-template <int M, int WT, bool MX, int SPM>
-void species_launch(const DevParams& P, const double* U, const double* F, const void* speed, void* dterm, int* err,
-                    cudaStream_t s) {
-  const int N = P.N0;
-  const int Pt = line_threads_m<M>(N);
-  constexpr int T = line_threads_max();
-  raise_smem_limit<k_crw_species<M, WT, MX, SPM>>((int)species_smem<M, MX>(T * M + 1, T));
-  dim3 grid(P.N1, P.nvars - P.nflow);
-  k_crw_species<M, WT, MX, SPM><<<grid, Pt, species_smem<M, MX>(N, Pt), s>>>(P, U, F, speed, dterm, err);
-}
-template <int M, int WT, bool MX>
-void species_launch_spm(const DevParams& P, const double* U, const double* F, const void* speed, void* dterm,
-                        int* err, cudaStream_t s) {
-  if (P.upwind == UPW_LLF) species_launch<M, WT, MX, 1>(P, U, F, speed, dterm, err, s);
-  else if (P.upwind == UPW_RF) species_launch<M, WT, MX, 2>(P, U, F, speed, dterm, err, s);
-  else species_launch<M, WT, MX, 0>(P, U, F, speed, dterm, err, s);
-}
-template <int M, bool MX>
-void species_launch_wt(const DevParams& P, const double* U, const double* F, const void* speed, void* dterm,
-                       int* err, cudaStream_t s) {
-  if (P.no_limiting) return species_launch_spm<M, WT_NOLIM, MX>(P, U, F, speed, dterm, err, s);
-  switch (P.weno_type) {
-    case W_MAPPED: return species_launch_spm<M, W_MAPPED, MX>(P, U, F, speed, dterm, err, s);
-    case W_BORGES: return species_launch_spm<M, W_BORGES, MX>(P, U, F, speed, dterm, err, s);
-    case W_YC: return species_launch_spm<M, W_YC, MX>(P, U, F, speed, dterm, err, s);
-    default: return species_launch_spm<M, W_JS, MX>(P, U, F, speed, dterm, err, s);
-  }
+  k_crw_line<M, DIR, WT, MX><<<grid, Pt, line_smem<M, MX>(N, Pt), s>>>(P, U, F, uL, uR, fL, fR, err);
 }
 
 template <int M, int DIR, bool MX>
 void line_launch_wt(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
-                    int* err, cudaStream_t s, int v0, int nv) {
-  if (P.no_limiting) return line_launch<M, DIR, WT_NOLIM, MX>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
+                    int* err, cudaStream_t s, int nv) {
+  if (P.no_limiting) return line_launch<M, DIR, WT_NOLIM, MX>(P, U, F, uL, uR, fL, fR, err, s, nv);
   switch (P.weno_type) {
-    case W_MAPPED: return line_launch<M, DIR, W_MAPPED, MX>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
-    case W_BORGES: return line_launch<M, DIR, W_BORGES, MX>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
-    case W_YC: return line_launch<M, DIR, W_YC, MX>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
-    default: return line_launch<M, DIR, W_JS, MX>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
+    case W_MAPPED: return line_launch<M, DIR, W_MAPPED, MX>(P, U, F, uL, uR, fL, fR, err, s, nv);
+    case W_BORGES: return line_launch<M, DIR, W_BORGES, MX>(P, U, F, uL, uR, fL, fR, err, s, nv);
+    case W_YC: return line_launch<M, DIR, W_YC, MX>(P, U, F, uL, uR, fL, fR, err, s, nv);
+    default: return line_launch<M, DIR, W_JS, MX>(P, U, F, uL, uR, fL, fR, err, s, nv);
   }
 }
 
 template <int M>
 void line_launch_m(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL, void* fR,
-                   int dir, int* err, cudaStream_t s, int v0, int nv) {
-  if (P.mixed) line_launch_wt<M, 0, true>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
-  else if (dir == 0) line_launch_wt<M, 0, false>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
-  else line_launch_wt<M, 1, false>(P, U, F, uL, uR, fL, fR, err, s, v0, nv);
+                   int dir, int* err, cudaStream_t s, int nv) {
+  if (P.mixed) line_launch_wt<M, 0, true>(P, U, F, uL, uR, fL, fR, err, s, nv);
+  else if (dir == 0) line_launch_wt<M, 0, false>(P, U, F, uL, uR, fL, fR, err, s, nv);
+  else line_launch_wt<M, 1, false>(P, U, F, uL, uR, fL, fR, err, s, nv);
 }
 
 }  // namespace
@@ -524,25 +432,11 @@ int launch_crweno_seg(const DevParams& P, const double* U, const double* F, void
 }
 
 int launch_crweno_line(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
-                       void* fR, int dir, int* err, cudaStream_t s, int v0, int nv) {
+                       void* fR, int dir, int* err, cudaStream_t s) {
   const int N = dir == 0 ? P.N0 : P.N1;
   if (!crweno_line_fits(N) || (P.mixed && dir != 0)) return -1;
-  if (nv < 0) nv = P.nvars - v0;
-  if (N >= 128) line_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s, v0, nv);
-  else line_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s, v0, nv);
-  return 0;
-}
-
-int launch_crweno_species(const DevParams& P, const double* U, const double* F, const void* speed, void* dterm,
-                          int* err, cudaStream_t s) {
-  if (!crweno_line_fits(P.N0) || P.nvars <= P.nflow) return -1;
-  if (P.N0 >= 128) {
-    if (P.mixed) species_launch_wt<8, true>(P, U, F, speed, dterm, err, s);
-    else species_launch_wt<8, false>(P, U, F, speed, dterm, err, s);
-  } else {
-    if (P.mixed) species_launch_wt<4, true>(P, U, F, speed, dterm, err, s);
-    else species_launch_wt<4, false>(P, U, F, speed, dterm, err, s);
-  }
+  if (N >= 128) line_launch_m<8>(P, U, F, uL, uR, fL, fR, dir, err, s, P.nvars);
+  else line_launch_m<4>(P, U, F, uL, uR, fL, fR, dir, err, s, P.nvars);
   return 0;
 }
 

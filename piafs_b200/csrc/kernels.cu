@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) k_upwind_div(DevParams P, const double* _
 // floats relative to the line's reference values, uref (absolute, FP64) are
 // those references for the flow variables, the flux is computed in FP32 in
 // deviation form and stored relative to the line's flux reference.
-template <int UPW, int DIR, bool MX, bool FLOWONLY = false>
+template <int UPW, int DIR, bool MX>
 __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __restrict__ uLv,
                                              const void* __restrict__ uRv, const void* __restrict__ fLv,
                                              const void* __restrict__ fRv, long long q,
@@ -435,7 +435,6 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __r
   }
 #pragma unroll
   for (int m = 0; m < NF; m++) so[m * sm_stride] = fi[m];
-  if (FLOWONLY) return;
   // passive variables four at a time, their sixteen loads in flight together
   int m = NF;
   for (; m + 4 <= P.nvars; m += 4) {
@@ -464,7 +463,7 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __r
 // standard one (q = i + N0 j, cell values from U).  MX: mixed precision (FP32
 // interface values relative to their line's reference, FP32 fluxes and
 // differences, FP64 result).
-template <int UPW, bool YT, bool MX, bool HYIN, bool SP = false>
+template <int UPW, bool YT, bool MX, bool HYIN>
 __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const double* __restrict__ U,
                                                       const double* __restrict__ UT,
                                                       const void* __restrict__ xuL, const void* __restrict__ xuR,
@@ -472,9 +471,7 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
                                                       const void* __restrict__ yuL, const void* __restrict__ yuR,
                                                       const void* __restrict__ yfL, const void* __restrict__ yfR,
                                                       const double* __restrict__ dxinv, double* __restrict__ rhs,
-                                                      int neg, const void* __restrict__ hyin, int n0,
-                                                      const void* __restrict__ dX = nullptr,
-                                                      const void* __restrict__ dY = nullptr) {
+                                                      int neg, const void* __restrict__ hyin, int n0) {
   typedef typename std::conditional<MX, float, double>::type T;
   extern __shared__ double sfd[];
   T* sf = (T*)sfd;
@@ -483,11 +480,8 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
   const int nvars = P.nvars, N0 = P.N0, N1 = P.N1, g = P.ghosts;
   const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
   const int tid = threadIdx.x;
-  // SP: the passive variables' differences come precomputed (dX, dY:
-  // k_crw_species) and only the flow variables' fluxes are formed here
-  const int nsm = SP ? P.nflow : nvars;
   T* sx = sf;               // x-interface fluxes [m][row jj][ii = 0..TI]
-  T* sy = sf + nsm * NX;    // y-interface fluxes [m][column ii][jj = 0..TJ]
+  T* sy = sf + nvars * NX;  // y-interface fluxes [m][column ii][jj = 0..TJ]
   double uref[4];
   if (tid < NX) {                // (TI + 1) x TJ x-interfaces
     const int ii = tid % LX, jj = tid / LX;
@@ -499,8 +493,8 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
 #pragma unroll
         for (int m = 0; m < 4; m++) uref[m] = U[m * P.ps + p0];
       }
-      iface_upwind<UPW, 0, MX, SP>(P, xuL, xuR, xfL, xfR, i + (long long)(N0 + 1) * j, U, pR - 1, pR, uref,
-                                   sx + jj * LX + ii, NX);
+      iface_upwind<UPW, 0, MX>(P, xuL, xuR, xfL, xfR, i + (long long)(N0 + 1) * j, U, pR - 1, pR, uref,
+                               sx + jj * LX + ii, NX);
     }
   }
   if (!HYIN) {                   // TI x (TJ + 1) y-interfaces
@@ -516,8 +510,8 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
       }
       if (YT) {
         const long long pR = (long long)(j + g) + (long long)P.W1 * (i + g);
-        iface_upwind<UPW, 1, MX, SP>(P, yuL, yuR, yfL, yfR, j + (long long)(N1 + 1) * i, UT, pR - 1, pR, uref,
-                                     sy + ii * LY + jj, NY);
+        iface_upwind<UPW, 1, MX>(P, yuL, yuR, yfL, yfR, j + (long long)(N1 + 1) * i, UT, pR - 1, pR, uref,
+                                 sy + ii * LY + jj, NY);
       } else {
         const long long pR = pidx(P, i, j);
         iface_upwind<UPW, 1, MX>(P, yuL, yuR, yfL, yfR, i + (long long)N0 * j, U, pR - P.W0, pR, uref,
@@ -536,7 +530,7 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
   // hyin[((i / n0) nvars + m) N1 + j) n0 + i % n0] (k_slab_upwind_y)
   const T* hyv = (const T*)hyin;
   const long long hbase = HYIN ? (long long)(i / n0) * nvars * N1 * n0 + (long long)j * n0 + i % n0 : 0;
-  for (int m = 0; m < nsm; m++) {
+  for (int m = 0; m < nvars; m++) {
     // hyp = dxinv_x dfx + dxinv_y dfy as dxinv_x dfx fused onto the rounded y
     // term, on both paths
     const T dfx = sx[m * NX + jj * LX + ii + 1] - sx[m * NX + jj * LX + ii];
@@ -545,60 +539,6 @@ __global__ void __launch_bounds__(256, 3) k_upwind_div2d(DevParams P, const doub
     const double h = (double)fma_rn(dxi, dfx, hy);
     rhs[(long long)m * P.ps + p] = neg ? -h : h;
   }
-  if (SP) {
-    // dX in the cell layout of x lines (i + N0 j), dY in that of the
-    // transposed y lines (j + N1 i)
-    const T* dxv = (const T*)dX;
-    const T* dyv = (const T*)dY;
-    for (int m = nsm; m < nvars; m++) {
-      const T dfx = dxv[(long long)m * P.pis + i + (long long)N0 * j];
-      const T hy = mul_rn(dyi, dyv[(long long)m * P.pis + j + (long long)N1 * i]);
-      const double h = (double)fma_rn(dxi, dfx, hy);
-      rhs[(long long)m * P.ps + p] = neg ? -h : h;
-    }
-  }
-}
-
-// The passive variables' upwinding speed at every interface of unit-stride
-// lines (P: N0 points along a line, N1 lines; x lines, or the y lines of a
-// transposed state with PD = 1), as upwind_flow forms it (sp_alpha, sp_mode)
-// from the flow variables' interface values and the cells either side; the
-// flow fluxes themselves are not needed here (zero fL, fR).  RF stores its
-// mode in the value: the speed for mode 1, -1 for mode 2, -2 for mode 3.
-template <int UPW, int PD, bool MX>
-__global__ void __launch_bounds__(256) k_species_speed(DevParams P, const double* __restrict__ cells,
-                                                       const void* __restrict__ uLv, const void* __restrict__ uRv,
-                                                       void* __restrict__ speed) {
-  typedef typename std::conditional<MX, float, double>::type T;
-  const long long nq = (long long)(P.N0 + 1) * P.N1;
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nq) return;
-  const int i = (int)(q % (P.N0 + 1)), line = (int)(q / (P.N0 + 1));
-  const long long pR = pidx(P, i, line), pL = pR - 1;
-  const T* uL = (const T*)uLv;
-  const T* uR = (const T*)uRv;
-  T a[4], b[4], ucl[4], ucr[4], zero[4] = {T(0), T(0), T(0), T(0)}, fi[4], spa;
-  int spm;
-#pragma unroll
-  for (int m = 0; m < 4; m++) {
-    a[m] = uL[m * P.pis + q]; b[m] = uR[m * P.pis + q];
-    if (UPW != UPW_LLF) { ucl[m] = (T)cells[m * P.ps + pL]; ucr[m] = (T)cells[m * P.ps + pR]; }
-  }
-  if (MX) {
-    T aL[4], aR[4];
-    if (UPW == UPW_LLF || UPW == UPW_RF) {
-      const long long p0 = pidx(P, 0, line);
-#pragma unroll
-      for (int m = 0; m < 4; m++) {
-        const T r = (T)cells[m * P.ps + p0];
-        aL[m] = r + a[m]; aR[m] = r + b[m];
-      }
-    }
-    upwind_flow_dev<NS2D, UPW, T>(a, b, zero, zero, aL, aR, ucl, ucr, (T)P.gamma, PD, fi, &spa, &spm);
-  } else {
-    upwind_flow<NS2D, UPW, T>(a, b, zero, zero, ucl, ucr, (T)P.gamma, PD, fi, &spa, &spm);
-  }
-  ((T*)speed)[q] = UPW == UPW_RF ? (spm == 2 ? T(-1) : spm == 3 ? T(-2) : spa) : spa;
 }
 
 // The y term of the 2D hyperbolic divergence on a column slab of a grid
@@ -1137,60 +1077,6 @@ static void upwind_div2d_u(const DevParams& P, const double* U, const double* UT
                                                              HYIN ? none : yi[0], HYIN ? none : yi[1],
                                                              HYIN ? none : yi[2], HYIN ? none : yi[3], dxinv, rhs,
                                                              neg, hyin, n0);
-}
-template <int UPW, bool MX>
-static void upwind_div2d_sp_u(const DevParams& P, const double* U, const double* UT, const void* const* xi,
-                              const void* const* yi, const void* dX, const void* dY, const double* dxinv,
-                              double* rhs, int neg, cudaStream_t s) {
-  raise_smem_limit<k_upwind_div2d<UPW, true, MX, false, true>>(200 * 1024);
-  dim3 grid(nblk(P.N0, 16), nblk(P.N1, 15));
-  size_t smem = (size_t)P.nflow * (17 * 15 + 16 * 17) * (MX ? sizeof(float) : sizeof(double));
-  k_upwind_div2d<UPW, true, MX, false, true><<<grid, 256, smem, s>>>(P, U, UT, xi[0], xi[1], xi[2], xi[3], yi[0],
-                                                                      yi[1], yi[2], yi[3], dxinv, rhs, neg,
-                                                                      nullptr, 0, dX, dY);
-}
-template <bool MX>
-static void upwind_div2d_sp_m(const DevParams& P, const double* U, const double* UT, const void* const* xi,
-                              const void* const* yi, const void* dX, const void* dY, const double* dxinv,
-                              double* rhs, int neg, cudaStream_t s) {
-  switch (P.upwind) {
-    case UPW_ROE: upwind_div2d_sp_u<UPW_ROE, MX>(P, U, UT, xi, yi, dX, dY, dxinv, rhs, neg, s); break;
-    case UPW_RF: upwind_div2d_sp_u<UPW_RF, MX>(P, U, UT, xi, yi, dX, dY, dxinv, rhs, neg, s); break;
-    case UPW_RUSANOV: upwind_div2d_sp_u<UPW_RUSANOV, MX>(P, U, UT, xi, yi, dX, dY, dxinv, rhs, neg, s); break;
-    default: upwind_div2d_sp_u<UPW_LLF, MX>(P, U, UT, xi, yi, dX, dY, dxinv, rhs, neg, s); break;
-  }
-}
-void launch_upwind_div2d_sp(const DevParams& P, const double* U, const double* UT, const void* const* xi,
-                            const void* const* yi, const void* dX, const void* dY, const double* dxinv, double* rhs,
-                            int neg, cudaStream_t s) {
-  if (P.mixed) upwind_div2d_sp_m<true>(P, U, UT, xi, yi, dX, dY, dxinv, rhs, neg, s);
-  else upwind_div2d_sp_m<false>(P, U, UT, xi, yi, dX, dY, dxinv, rhs, neg, s);
-}
-template <int UPW, int PD, bool MX>
-static void species_speed_u(const DevParams& P, const double* cells, const void* uL, const void* uR, void* speed,
-                            cudaStream_t s) {
-  const long long nq = (long long)(P.N0 + 1) * P.N1;
-  k_species_speed<UPW, PD, MX><<<nblk(nq, 256), 256, 0, s>>>(P, cells, uL, uR, speed);
-}
-template <int PD, bool MX>
-static void species_speed_m(const DevParams& P, const double* cells, const void* uL, const void* uR, void* speed,
-                            cudaStream_t s) {
-  switch (P.upwind) {
-    case UPW_ROE: species_speed_u<UPW_ROE, PD, MX>(P, cells, uL, uR, speed, s); break;
-    case UPW_RF: species_speed_u<UPW_RF, PD, MX>(P, cells, uL, uR, speed, s); break;
-    case UPW_RUSANOV: species_speed_u<UPW_RUSANOV, PD, MX>(P, cells, uL, uR, speed, s); break;
-    default: species_speed_u<UPW_LLF, PD, MX>(P, cells, uL, uR, speed, s); break;
-  }
-}
-void launch_species_speed(const DevParams& P, const double* cells, const void* uL, const void* uR, void* speed,
-                          int pdir, cudaStream_t s) {
-  if (P.mixed) {
-    if (pdir == 0) species_speed_m<0, true>(P, cells, uL, uR, speed, s);
-    else species_speed_m<1, true>(P, cells, uL, uR, speed, s);
-  } else {
-    if (pdir == 0) species_speed_m<0, false>(P, cells, uL, uR, speed, s);
-    else species_speed_m<1, false>(P, cells, uL, uR, speed, s);
-  }
 }
 template <bool YT, bool MX, bool HYIN>
 static void upwind_div2d_yt(const DevParams& P, const double* U, const double* UT, const void* const* xi,

@@ -169,20 +169,7 @@ int launch_crweno(const DevParams& P, const double* U, const double* F, void* uL
 // launcher otherwise
 bool crweno_line_fits(int N);
 int launch_crweno_line(const DevParams& P, const double* U, const double* F, void* uL, void* uR, void* fL,
-                       void* fR, int dir, int* err, cudaStream_t s, int v0 = 0, int nv = -1);
-// the passive variables (nflow .. nvars-1) of 2D Navier-Stokes along unit-
-// stride lines (x lines, or y lines of a transposed state), reconstructed,
-// upwinded with the flow's speed at each interface (launch_species_speed)
-// and differenced: dterm[v][i + N0 line] = fI[i+1] - fI[i]; -1 if the lines
-// do not fit one CTA
-int launch_crweno_species(const DevParams& P, const double* U, const double* F, const void* speed, void* dterm,
-                          int* err, cudaStream_t s);
-// the passive variables' upwinding speed (and for RF the mode) at every
-// interface of unit-stride lines from the flow variables' interface values
-// and the cells (physical direction pdir: 0 for x lines, 1 for the y lines
-// of a transposed state); speed in the interface layout of those lines
-void launch_species_speed(const DevParams& P, const double* cells, const void* uL, const void* uR, void* speed,
-                          int pdir, cudaStream_t s);
+                       void* fR, int dir, int* err, cudaStream_t s);
 // longer lines (up to 32769 interfaces) by clusters of CTAs that solve their
 // segments' separator systems locally and couple them through one small
 // system (crweno_line.cu); -1 if the line is not one of those
@@ -205,12 +192,6 @@ void launch_upwind_div(const DevParams& P, const double* U, const void* uL, cons
 // with cell values from UT when UT is given.  rhs = -hyp (neg) or hyp.
 void launch_upwind_div2d(const DevParams& P, const double* U, const double* UT, const void* const* xi,
                          const void* const* yi, const double* dxinv, double* rhs, int neg, cudaStream_t s);
-// the same with the passive variables' differences given (the fused species
-// path: dX in the cell layout of x lines, dY in that of the transposed y
-// lines, from launch_crweno_species); y interface arrays transposed
-void launch_upwind_div2d_sp(const DevParams& P, const double* U, const double* UT, const void* const* xi,
-                            const void* const* yi, const void* dX, const void* dY, const double* dxinv, double* rhs,
-                            int neg, cudaStream_t s);
 // the same with the y term given: hy from the column slabs of a grid
 // decomposed along y (launch_slab_upwind_y's layout, n0 columns per slab)
 void launch_upwind_div2d_hy(const DevParams& P, const double* U, const void* const* xi, const double* dxinv,

@@ -52,10 +52,6 @@ struct piafs_gpu_sim {
   // CUDA graphs of one step: [0] plain, [1] with residual norm
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool use_graph = true;
-  // 2D Navier-Stokes CRWENO5 with passive variables: their reconstruction,
-  // upwinding and flux differences in one kernel per direction
-  // (launch_crweno_species), the upwind kernel forming the flow's only
-  bool fuse_species = false;
 };
 
 namespace piafs {

@@ -110,12 +110,9 @@ int piafs_gpu_slab_create(const char* deck_dir, int precision, int rank, int nra
     return r;
   }
   piafs_gpu_sim* s = sl->row;
-  // the row slab never runs a y pass of its own; its x pass keeps the
-  // passive variables' interface arrays, which the upwind kernel with the
-  // received y term reads
+  // the row slab never runs a y pass of its own
   cudaFree(s->ut);
   s->ut = nullptr;
-  s->fuse_species = false;
   for (auto& p : s->iface_y) { cudaFree(p); p = nullptr; }
   // the column slab: columns [rank n0, (rank + 1) n0), every row
   DevParams& C = sl->Pc;
