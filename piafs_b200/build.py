@@ -93,8 +93,10 @@ def build_hypar(force: bool = False, verbose: bool = False):
     reference's headers in their single-rank (-Dserial) layout."""
     inc = reference_include()
     src = os.path.join(CSRC, "hypar_attach.cpp")
-    deps = [src, LIB, os.path.join(HERE, "..", "include", "piafs_hypar.h"), os.path.join(CSRC, "deck.h"),
-            os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "kernels.h")]
+    # it links libpiafs_gpu.so dynamically: only the structures it shares
+    # with the library (these headers) make it stale
+    deps = [src, os.path.join(HERE, "..", "include", "piafs_hypar.h"), os.path.join(HERE, "..", "include", "piafs_gpu.h"),
+            os.path.join(CSRC, "deck.h"), os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "kernels.h")]
     if inc is None:
         # without the reference's headers it cannot be rebuilt; one built
         # against older library structures must not be loaded
