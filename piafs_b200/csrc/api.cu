@@ -83,8 +83,12 @@ void piafs::enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* cons
     return;
   }
   if (d == 1 && s->ut) {
-    launch_transpose(P, U, s->ut, s->stream);
-    launch_flux(P, s->ut, s->fC, 1, s->stream);
+    if (P.model == NS2D) {
+      launch_transpose_flux_y(P, U, s->ut, s->fC, s->stream);
+    } else {
+      launch_transpose(P, U, s->ut, s->stream);
+      launch_flux(P, s->ut, s->fC, 1, s->stream);
+    }
     mark();
     launch_crweno(s->PT, s->ut, s->fC, I[0], I[1], I[2], I[3], 0, s->err, s->stream);
     mark();
@@ -357,7 +361,7 @@ int piafs_gpu_get_info(piafs_gpu_sim* s, piafs_gpu_info* info) {
   // pass, one upwind/divergence kernel, viscous/source), update, clock
   const int nz = (int)d.zones.size();
   const int vs = ((s->P.ndims == 2 && s->P.viscous) || s->P.chem) ? 1 : 0;
-  const int tr = s->ut ? 1 : 0;
+  const int tr = (s->ut && s->P.model != NS2D) ? 1 : 0;   // NS2D: the transpose also forms the y flux
   info->launches_per_step = nz + d.nstages * (2 * s->P.ndims + 1 + tr + vs) + (d.nstages - 1) * (1 + nz) + 2;
   return PIAFS_OK;
 }

@@ -93,6 +93,66 @@ __global__ void k_transpose_planes(const double* __restrict__ in, double* __rest
   }
 }
 
+// The y pass's transposed state and its y flux in one pass (2D
+// Navier-Stokes): a 32 x 32 tile of points with all variables, the flow
+// variables kept in shared memory for the flux, every variable written
+// transposed to UT and its y flux (ns2d_flux; vn U_m for the passive ones,
+// as k_flux forms them) to FT -- one read of U where the transpose and
+// k_flux read it twice.
+__global__ void __launch_bounds__(256) k_transpose_flux_y(DevParams P, const double* __restrict__ U,
+                                                          double* __restrict__ UT, double* __restrict__ FT) {
+  __shared__ double flow[4][32][33];
+  __shared__ double tile[32][33];
+  const int W0 = P.W0, W1 = P.W1;
+  const long long ps = P.ps;
+  const int i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+  for (int m = 0; m < 4; m++)
+    for (int r = ty; r < 32; r += 8) {
+      const int i = i0 + tx, j = j0 + r;
+      if (i < W0 && j < W1) flow[m][r][tx] = U[m * ps + (long long)j * W0 + i];
+    }
+  __syncthreads();
+  // point (i = i0 + r, j = j0 + tx): writes along j are coalesced
+  double vn[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int r = ty + 8 * k;
+    const int j = j0 + tx, i = i0 + r;
+    vn[k] = 0.0;
+    if (i < W0 && j < W1) {
+      double f[4];
+      ns2d_flux(flow[0][tx][r], flow[1][tx][r], flow[2][tx][r], flow[3][tx][r], P.gamma, 1, f, vn[k]);
+      const long long q = (long long)i * W1 + j;
+#pragma unroll
+      for (int m = 0; m < 4; m++) {
+        UT[m * ps + q] = flow[m][tx][r];
+        FT[m * ps + q] = f[m];
+      }
+    }
+  }
+  for (int m = 4; m < P.nvars; m++) {
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+      const int i = i0 + tx, j = j0 + r;
+      if (i < W0 && j < W1) tile[r][tx] = U[m * ps + (long long)j * W0 + i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int r = ty + 8 * k;
+      const int j = j0 + tx, i = i0 + r;
+      if (i < W0 && j < W1) {
+        const long long q = (long long)i * W1 + j;
+        const double x = tile[tx][r];
+        UT[m * ps + q] = x;
+        FT[m * ps + q] = __dmul_rn(vn[k], x);
+      }
+    }
+  }
+}
+
 // ================================================================ boundaries
 // One zone of ApplyBoundaryConditions: BCPeriodicU (BCPeriodic.c:22-62),
 // BCExtrapolateU (BCExtrapolate.c:16-50), BCSlipWallU (BCSlipWall.c:24-136).
@@ -143,6 +203,54 @@ __global__ void k_update(DevParams P, double* __restrict__ u, const double* __re
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
     __shared__ double ws[32];
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ws[w] = sq;
+    __syncthreads();
+    if (w == 0) {
+      sq = lane < (blockDim.x >> 5) ? ws[lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+      if (lane == 0) atomicAdd(norm_acc, sq);
+    }
+  }
+}
+
+// k_update for ns stages, two consecutive values (one double2) per thread:
+// the same arithmetic per value, more bytes in flight per thread
+template <int NS>
+__global__ void k_update2(DevParams P, double* __restrict__ u, const double* __restrict__ d0, double b0,
+                          const double* __restrict__ d1, double b1, const double* __restrict__ d2, double b2,
+                          const double* __restrict__ d3, double b3, double* __restrict__ norm_acc) {
+  const long long n2 = (long long)P.nvars * P.ps / 2;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double sq = 0.0;
+  if (i < n2) {
+    const double2 old = reinterpret_cast<const double2*>(u)[i];
+    double2 x = old;
+    const double* dd[4] = {d0, d1, d2, d3};
+    const double bb[4] = {b0, b1, b2, b3};
+    double2 v[NS];
+#pragma unroll
+    for (int k = 0; k < NS; k++) v[k] = reinterpret_cast<const double2*>(dd[k])[i];
+#pragma unroll
+    for (int k = 0; k < NS; k++) { x.x += bb[k] * v[k].x; x.y += bb[k] * v[k].y; }
+    reinterpret_cast<double2*>(u)[i] = x;
+    if (norm_acc) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const long long p = (2 * i + h) % P.ps;
+        if (p < P.npg) {
+          const int ii = (int)(p % P.W0) - P.ghosts, jj = (int)(p / P.W0) - P.g1;
+          if (ii >= 0 && ii < P.N0 && jj >= 0 && jj < P.N1) {
+            const double d = h == 0 ? old.x - x.x : old.y - x.y;
+            sq += d * d;
+          }
+        }
+      }
+    }
+  }
+  if (norm_acc) {
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+    __shared__ double ws[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) ws[w] = sq;
     __syncthreads();
     if (w == 0) {
@@ -957,6 +1065,10 @@ void launch_iface_aos_to_soa(const double* aos, double* soa, long long ni, int n
 void launch_iface_soa_to_aos(const double* soa, double* aos, long long ni, int nv, long long pis, cudaStream_t s) {
   k_iface_soa_to_aos<<<nblk(ni * nv, 256), 256, 0, s>>>(soa, aos, ni, nv, pis);
 }
+void launch_transpose_flux_y(const DevParams& P, const double* U, double* UT, double* FT, cudaStream_t s) {
+  dim3 grid(nblk(P.W0, 32), nblk(P.W1, 32)), blk(32, 8);
+  k_transpose_flux_y<<<grid, blk, 0, s>>>(P, U, UT, FT);
+}
 void launch_transpose(const DevParams& P, const double* in, double* out, cudaStream_t s) {
   dim3 grid(nblk(P.W0, 32), nblk(P.W1, 32), P.nvars), blk(32, 8);
   k_transpose_planes<<<grid, blk, 0, s>>>(in, out, P.W0, P.W1, P.ps);
@@ -982,6 +1094,21 @@ void launch_stage(long long n, double* Us, const double* u, const double* const*
 void launch_update(const DevParams& P, double* u, const double* const* d, const double* b, int ns, double* norm_acc,
                    cudaStream_t s) {
   long long n = (long long)P.nvars * P.ps;
+  if (ns >= 1 && ns <= 4) {   // plane strides are multiples of 32: whole double2 pairs within a plane
+    const long long n2 = n / 2;
+    const double* dd[4] = {d[0], ns > 1 ? d[1] : nullptr, ns > 2 ? d[2] : nullptr, ns > 3 ? d[3] : nullptr};
+    const double bb[4] = {b[0], ns > 1 ? b[1] : 0.0, ns > 2 ? b[2] : 0.0, ns > 3 ? b[3] : 0.0};
+#define PIAFS_UPD(NS) k_update2<NS><<<nblk(n2, 256), 256, 0, s>>>(P, u, dd[0], bb[0], dd[1], bb[1], dd[2], bb[2], \
+                                                                 dd[3], bb[3], norm_acc)
+    switch (ns) {
+      case 1: PIAFS_UPD(1); break;
+      case 2: PIAFS_UPD(2); break;
+      case 3: PIAFS_UPD(3); break;
+      default: PIAFS_UPD(4); break;
+    }
+#undef PIAFS_UPD
+    return;
+  }
   k_update<<<nblk(n, 256), 256, 0, s>>>(P, u, d[0], b[0], ns > 1 ? d[1] : nullptr, ns > 1 ? b[1] : 0.0,
                                          ns > 2 ? d[2] : nullptr, ns > 2 ? b[2] : 0.0, ns > 3 ? d[3] : nullptr,
                                          ns > 3 ? b[3] : 0.0, ns, norm_acc);

@@ -141,6 +141,9 @@ void launch_bc(const DevParams& P, double* u, const Zone& z, cudaStream_t s);
 // 2D only: plane-wise transpose of a ghosted state (j fastest in `out`) and
 // the parameters that describe the transposed grid (dimensions swapped)
 void launch_transpose(const DevParams& P, const double* in, double* out, cudaStream_t s);
+// the transposed state of a 2D Navier-Stokes grid and its y flux, both in
+// the transposed layout, in one pass
+void launch_transpose_flux_y(const DevParams& P, const double* U, double* UT, double* FT, cudaStream_t s);
 DevParams transposed_params(const DevParams& P);
 void launch_stage(long long n, double* Us, const double* u, const double* const* d, const double* a, int nterms,
                   cudaStream_t s);
