@@ -132,12 +132,22 @@ __global__ void __launch_bounds__(256) k_transpose_flux_y(DevParams P, const dou
       }
     }
   }
+  // passive variables one tile at a time, the next tile's loads in flight
+  // while the current one is written
+  double nxt[4];
+  auto load = [&](int m) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int r = ty + 8 * k, i = i0 + tx, j = j0 + r;
+      nxt[k] = (m < P.nvars && i < W0 && j < W1) ? U[m * ps + (long long)j * W0 + i] : 0.0;
+    }
+  };
+  load(4);
   for (int m = 4; m < P.nvars; m++) {
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-      const int i = i0 + tx, j = j0 + r;
-      if (i < W0 && j < W1) tile[r][tx] = U[m * ps + (long long)j * W0 + i];
-    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) tile[ty + 8 * k][tx] = nxt[k];
+    load(m + 1);
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 4; k++) {
