@@ -733,9 +733,11 @@ __device__ __forceinline__ T d4(int i, int N, int g, Fn f) {
 // MX (mixed precision): velocities and temperature, their differences, the
 // viscous fluxes and the chemistry in FP32; the temperature is held relative
 // to the tile's first point (taken in FP64) so that its differences keep
-// FP32's relative precision; the result is added to the FP64 rhs.
+// FP32's relative precision; the result is added to the FP64 rhs.  Six
+// CTAs per SM (40 registers): the tile's two phases and its memory latency
+// overlap across more CTAs (0.33 vs 0.38 ms per launch at 2048^2).
 template <bool MX>
-__global__ void __launch_bounds__(256) k_visc_source(DevParams P, const double* __restrict__ U,
+__global__ void __launch_bounds__(256, 6) k_visc_source(DevParams P, const double* __restrict__ U,
                                                      const double* __restrict__ dxinv,
                                                      const double* __restrict__ imap,
                                                      const double* __restrict__ tdev, double cstage,
