@@ -238,6 +238,16 @@ int piafs::create_sim(Deck&& deck, int precision, piafs_gpu_sim** out) {
   if (r) { delete s; return fail(r, err); }
   s->precision = precision;
   s->P.mixed = precision == PIAFS_PRECISION_MIXED ? 1 : 0;
+  {
+    // PIAFS_GPU_NO_PACKED_SPECIES=1 keeps the passive variables' four
+    // interface arrays (the same values; for checking the packed form)
+    const DevParams& Q = s->P;
+    const char* npk = std::getenv("PIAFS_GPU_NO_PACKED_SPECIES");
+    s->P.pack_sp = (Q.model == NS2D && Q.ndims == 2 && Q.nvars > Q.nflow && Q.scheme == CRWENO5 &&
+                    !Q.char_interp && Q.upwind != UPW_RF && crweno_line_fits(Q.N0) && crweno_line_fits(Q.N1) &&
+                    !(npk && npk[0] == '1'))
+                       ? 1 : 0;
+  }
   if (s->P.mixed && s->P.char_interp) {
     delete s;
     return fail(PIAFS_ERR_UNSUPPORTED, "mixed precision runs hyp_interp_type components");
@@ -728,7 +738,8 @@ int piafs_gpu_InterpolateInterfacesHyp(piafs_gpu_sim* s, double* fI, const doubl
                                        int dir, int uflag) {
   if (!s || !fI || !fC || !u || dir < 0 || dir >= s->P.ndims) return fail(PIAFS_ERR_ARGUMENT, "bad argument");
   DevParams P = s->P;
-  P.mixed = 0;   // operator-level entry points are FP64
+  P.mixed = 0;     // operator-level entry points are FP64
+  P.pack_sp = 0;   // and return every interface array as the reference forms it
   to_soa(s, u, s->scratch);
   to_soa(s, fC, s->fC);
   if (P.scheme == CRWENO5 && P.char_interp)

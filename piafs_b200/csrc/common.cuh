@@ -52,6 +52,11 @@ struct DevParams {
   // rows [jg0, jg0 + N1) of a grid of N1g rows (a row slab of a decomposed
   // grid); 0 and N1 for a whole grid
   int jg0, N1g;
+  // 1: the CRWENO5 line solve stores the passive variables' interface values
+  // packed for their scalar upwinding -- uL - uR in the uL array, fL + fR in
+  // the fL array -- and the upwind kernels read them so (2D Navier-Stokes,
+  // upwinding other than RF)
+  int pack_sp;
 };
 
 __host__ __device__ inline long long pidx(const DevParams& P, int i, int j) {

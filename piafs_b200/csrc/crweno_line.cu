@@ -76,7 +76,19 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
   line_pair_solve<M, WT, R, O>(P, src, st, ref, N, cs, pcA, tp, sy, so, bad);
   if (bad) atomicOr(err, 1);
   const int ostride = opad(N) + 1;
-  // N + 1 interfaces over Pt threads: at most M + 1 each
+  // N + 1 interfaces over Pt threads: at most M + 1 each; the passive
+  // variables packed for their upwinding when P.pack_sp (uL - uR, fL + fR)
+  if (P.pack_sp && v >= P.nflow) {
+#pragma unroll
+    for (int it = 0; it <= M; it++) {
+      const int i = k + it * Pt;
+      if (i <= N) {
+        const O l = so[opad(i)], r = so[ostride + opad(i)];
+        oL[i * ist] = isF ? l + r : l - r;
+      }
+    }
+    return;
+  }
 #pragma unroll
   for (int it = 0; it <= M; it++) {
     const int i = k + it * Pt;

@@ -553,6 +553,23 @@ __device__ __forceinline__ void iface_upwind(const DevParams& P, const void* __r
   }
 #pragma unroll
   for (int m = 0; m < NF; m++) so[m * sm_stride] = fi[m];
+  if (P.pack_sp) {
+    // passive variables packed by the line solve: uL - uR, fL + fR
+    int m = NF;
+    for (; m + 4 <= P.nvars; m += 4) {
+      T du[4], sf[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const long long o = (long long)(m + k) * P.pis + q;
+        du[k] = uL[o]; sf[k] = fL[o];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) so[(m + k) * sm_stride] = upwind_species_packed(spm, spa, du[k], sf[k]);
+    }
+    for (; m < P.nvars; m++)
+      so[m * sm_stride] = upwind_species_packed(spm, spa, uL[m * P.pis + q], fL[m * P.pis + q]);
+    return;
+  }
   // passive variables four at a time, their sixteen loads in flight together
   int m = NF;
   for (; m + 4 <= P.nvars; m += 4) {

@@ -439,5 +439,12 @@ __device__ __forceinline__ T upwind_species(int mode, T alpha, T uL, T uR, T fL,
   if (mode == 1) return T(0.5) * (fL + fR + alpha * (uL - uR));
   return mode == 2 ? fL : fR;
 }
+// the same for modes 0 and 1 from the packed values du = uL - uR and
+// sf = fL + fR (uR - uL = -du exactly, so the values are the same)
+template <typename T>
+__device__ __forceinline__ T upwind_species_packed(int mode, T alpha, T du, T sf) {
+  if (mode == 0) return T(0.5) * sf - alpha * (T(0.5) * (-du));
+  return T(0.5) * (sf + alpha * du);
+}
 
 }  // namespace piafs

@@ -128,6 +128,9 @@ int piafs_gpu_slab_create(const char* deck_dir, int precision, int rank, int nra
   C.pis = round32(C.nint[0] > C.nint[1] ? C.nint[0] : C.nint[1]);
   C.jg0 = 0;
   C.N1g = C.N1;
+  // packed passive interface values need every line in one CTA, the column
+  // slab's whole-grid y lines included
+  if (!crweno_line_fits(sl->N1)) s->P.pack_sp = C.pack_sp = 0;
   sl->PTc = transposed_params(C);
   const size_t planes = (size_t)C.nvars * C.ps, iplanes = (size_t)C.nvars * C.pis;
   const size_t isz = s->P.mixed ? sizeof(float) : sizeof(double);
