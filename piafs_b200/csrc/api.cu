@@ -62,6 +62,10 @@ static void free_sim(piafs_gpu_sim* s) {
   cudaFree(s->sponge_buf);
   cudaFree(s->zone_buf);
   cudaFree(s->crwchar);
+  cudaFree(s->fCy);
+  if (s->yfork) cudaEventDestroy(s->yfork);
+  if (s->yjoin) cudaEventDestroy(s->yjoin);
+  if (s->ystream) cudaStreamDestroy(s->ystream);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -109,12 +113,23 @@ void piafs::enqueue_recon(piafs_gpu_sim* s, const double* U, int d, double* cons
 static void enqueue_hyp(piafs_gpu_sim* s, const double* U, double* out, bool neg, cudaEvent_t* ev = nullptr,
                         int* k = nullptr) {
   const DevParams& P = s->P;
+  if (s->concurrent_y && !ev && P.ndims == 2) cudaEventRecord(s->yfork, s->stream);
   enqueue_recon(s, U, 0, s->iface, ev, k);
   if (P.ndims == 1) {
     launch_upwind_div(P, U, s->iface[0], s->iface[1], s->iface[2], s->iface[3], s->dxinv, out, 0, neg ? 0 : 2,
                       s->stream);
   } else {
-    enqueue_recon(s, U, 1, s->iface_y, ev, k);
+    if (s->concurrent_y && !ev) {
+      // the y pass joins the x pass's stream before the upwind kernel
+      cudaStreamWaitEvent(s->ystream, s->yfork, 0);
+      double* const* Iy = s->iface_y;
+      launch_transpose_flux_y(P, U, s->ut, s->fCy, s->ystream);
+      launch_crweno(s->PT, s->ut, s->fCy, Iy[0], Iy[1], Iy[2], Iy[3], 0, s->err, s->ystream);
+      cudaEventRecord(s->yjoin, s->ystream);
+      cudaStreamWaitEvent(s->stream, s->yjoin, 0);
+    } else {
+      enqueue_recon(s, U, 1, s->iface_y, ev, k);
+    }
     const void* xi[4] = {s->iface[0], s->iface[1], s->iface[2], s->iface[3]};
     const void* yi[4] = {s->iface_y[0], s->iface_y[1], s->iface_y[2], s->iface_y[3]};
     launch_upwind_div2d(P, U, s->ut, xi, yi, s->dxinv, out, neg ? 1 : 0, s->stream);
@@ -280,6 +295,16 @@ int piafs::create_sim(Deck&& deck, int precision, piafs_gpu_sim** out) {
       (P.mixed || !(noyt && noyt[0] == '1'))) {
     e = alloc(&s->ut, planes);
     s->PT = transposed_params(P);
+    // PIAFS_GPU_NO_CONCURRENT_Y=1 runs the y pass after the x pass on one
+    // stream (the same values)
+    const char* ncy = std::getenv("PIAFS_GPU_NO_CONCURRENT_Y");
+    if (e == cudaSuccess && P.model == NS2D && !(ncy && ncy[0] == '1')) {
+      e = alloc(&s->fCy, planes);
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->ystream, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->yfork, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->yjoin, cudaEventDisableTiming);
+      s->concurrent_y = e == cudaSuccess;
+    }
   }
   if (e == cudaSuccess) e = alloc(&s->dxinv, d.dxinv.size());
   if (e == cudaSuccess) e = alloc(&s->imap, d.imap.size());

@@ -18,6 +18,13 @@ struct piafs_gpu_sim {
   int precision = 0;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // 2D Navier-Stokes with a transposed y pass: the y pass (transpose, y
+  // flux into fCy, y line solve) on ystream, concurrent with the x pass,
+  // forked from and joined to `stream` by the two events
+  bool concurrent_y = false;
+  cudaStream_t ystream = nullptr;
+  cudaEvent_t yfork = nullptr, yjoin = nullptr;
+  double* fCy = nullptr;
   // device state (structure of arrays)
   double* u = nullptr;
   double* U[MAX_STAGES] = {nullptr};       // U[0] aliases u

@@ -113,6 +113,9 @@ int piafs_gpu_slab_create(const char* deck_dir, int precision, int rank, int nra
   // the row slab never runs a y pass of its own
   cudaFree(s->ut);
   s->ut = nullptr;
+  s->concurrent_y = false;
+  cudaFree(s->fCy);
+  s->fCy = nullptr;
   for (auto& p : s->iface_y) { cudaFree(p); p = nullptr; }
   // the column slab: columns [rank n0, (rank + 1) n0), every row
   DevParams& C = sl->Pc;
