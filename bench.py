@@ -39,8 +39,9 @@ sys.path.insert(0, ROOT)
 
 BYTES_PER_UNIT = {11: 264, 4: 96, 3: 72}   # 3 * nvars * 8: read U_s, read u_n, write (FP64 state)
 # measured DRAM traffic of one CRWENO5 line-solve launch per interior point
-# (dram__bytes_read + dram__bytes_write, ncu at 1536^2, 11 variables)
-TRAFFIC_PER_POINT = {11: (417.0e6 + 776.5e6) / (1536 * 1536)}
+# (dram__bytes_read + dram__bytes_write, ncu at 1536^2, 11 variables, the
+# passive variables' interface values packed)
+TRAFFIC_PER_POINT = {11: (416.9e6 + 523.2e6) / (1536 * 1536)}
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
 CPU_SAMPLE_N = 512                          # sample grid of the CPU arms
 # Steps timed back to back from the initial condition before the state is
