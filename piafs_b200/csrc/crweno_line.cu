@@ -1,8 +1,10 @@
 // CRWENO5 interface reconstruction, one CTA per line, component and field,
 // lines of up to 4097 interfaces (sm_100a): x lines (unit stride, also the y
-// lines of a transposed state) and strided y lines.
+// lines of a transposed state) and strided y lines; longer lines by clusters
+// of CTAs (k_crw_seg, below).
 //
-// The method is that of k_crweno_pair (crweno.cu): Interp1PrimFifthOrderCRWENO
+// The method is that of k_crweno_pair (crweno.cu, which keeps the general
+// form for lines of fewer than three interfaces): Interp1PrimFifthOrderCRWENO
 // (Interp1PrimFifthOrderCRWENO.c:81-240) builds one tridiagonal system per
 // upwind bias, and the two systems of a (line, component, field) are solved
 // together by substructuring -- each thread reduces its chunk of M rows to

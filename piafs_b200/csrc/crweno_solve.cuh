@@ -1,5 +1,5 @@
 // The CRWENO5 line solve of one (line, component, field) as a device
-// function of a whole CTA (crweno_line.cu, hyp_line.cu); the method is
+// function of a whole CTA (crweno_line.cu); the method is
 // described in crweno_line.cu.
 #pragma once
 #include <type_traits>

@@ -1,15 +1,17 @@
 // Hot-path kernels of the PIAFS GPU path (sm_100a).
 //
 // Per RK stage the host enqueues, for each direction d:
-//   k_flux          cell-centred flux F_d(U) at every point (FFunction)
+//   k_flux          cell-centred flux F_d(U) at every point (FFunction);
+//                   for the y pass of 2D Navier-Stokes k_transpose_flux_y
+//                   (transposed state and its y flux)
 //   k_weno5 or      interface values uL,uR,fL,fR (InterpolateInterfacesHyp
-//   k_crweno_pair     with the weights of SetInterpLimiterVar fused in;
-//                     crweno.cu)
-//   k_upwind_div    upwind flux at interfaces + conservative difference,
-//                   accumulated into the stage derivative (Upwind +
-//                   HyperbolicFunction's dxinv*(fI[j+1]-fI[j]))
+//   k_crw_line        with the weights of SetInterpLimiterVar fused in;
+//                     crweno_line.cu, crweno.cu)
+//   k_upwind_div2d  upwind flux at the interfaces of both directions +
+//   (k_upwind_div   conservative difference into the stage derivative
+//    in 1D)         (Upwind + HyperbolicFunction's dxinv*(fI[j+1]-fI[j]))
 // then k_visc_source (ParabolicFunction + SourceFunction) and the RK
-// kernels k_stage / k_update (TimeRK).  All state is FP64.
+// kernels k_stage / k_update2 (TimeRK).  All state is FP64.
 #include <cstdio>
 #include <type_traits>
 #include "kernels.h"
