@@ -254,6 +254,12 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
   if (k == 0) { bnd[0] = make_double2(d[0], d[1]); bnd[1] = make_double2(e[0], e[1]); bnd[2] = make_double2(f[0], f[1]); }
   if (k == Pt - 1) { bnd[3] = make_double2(d[0], d[1]); bnd[4] = make_double2(e[0], e[1]); bnd[5] = make_double2(f[0], f[1]); }
   cl.sync();
+  // the cluster's boundary rows gathered by 6 ncta threads at once (one
+  // round trip of distributed shared memory) into this CTA's cell staging,
+  // free between the chunk phase and the recovery
+  double2* gath = (double2*)cs;
+  if (k < 6 * ncta) gath[k] = cl.map_shared_rank(bnd, k / 6)[k % 6];
+  __syncthreads();
   if (k == 0) {
     // unknowns F_c (first separator of CTA c) = z[2c], G_c (last) = z[2c+1]:
     //   F_c + e0_c G_{c-1} + f0_c F_{c+1} = d0_c,  G_c + el_c G_{c-1} + fl_c F_{c+1} = dl_c
@@ -264,7 +270,7 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
     double A[2][2 * MAXC][2 * MAXC], z[2][2 * MAXC];
     const int n = 2 * ncta;
     for (int c = 0; c < ncta; c++) {
-      const double2* rb2 = cl.map_shared_rank(bnd, c);
+      const double2* rb2 = gath + 6 * c;
       const double2 d0 = rb2[0], e0 = rb2[1], f0 = rb2[2], dl2 = rb2[3], el = rb2[4], fl = rb2[5];
       const double d0q[2] = {d0.x, d0.y}, e0q[2] = {e0.x, e0.y}, f0q[2] = {f0.x, f0.y};
       const double dlq[2] = {dl2.x, dl2.y}, elq[2] = {el.x, el.y}, flq[2] = {fl.x, fl.y};
