@@ -260,52 +260,38 @@ __global__ void __launch_bounds__(line_threads_max(), 1)
   double2* gath = (double2*)cs;
   if (k < 6 * ncta) gath[k] = cl.map_shared_rank(bnd, k / 6)[k % 6];
   __syncthreads();
-  if (k == 0) {
-    // unknowns F_c (first separator of CTA c) = z[2c], G_c (last) = z[2c+1]:
-    //   F_c + e0_c G_{c-1} + f0_c F_{c+1} = d0_c,  G_c + el_c G_{c-1} + fl_c F_{c+1} = dl_c
-    // (no G_{-1}, no F_{ncta}: those columns are zero), banded elimination
-    // without pivoting (the off-diagonal columns are what the local PCR left
-    // of single couplings, below one in magnitude)
+  if (k < 2) {
+    // bias q = k.  Unknowns F_c (first separator of CTA c) and G_c (last):
+    //   F_c = d0_c - e0_c G_{c-1} - f0_c F_{c+1},  G_c = dl_c - el_c G_{c-1} - fl_c F_{c+1}
+    // (no G_{-1}, no F_{ncta}).  Forward: G_c = al_c + be_c F_{c+1} and
+    // F_c = ga_c + de_c F_{c+1}; backward from F_{ncta} = 0.  This CTA needs
+    // L = G_{rank-1} and R = F_{rank+1}.
     constexpr int MAXC = 8;
-    double A[2][2 * MAXC][2 * MAXC], z[2][2 * MAXC];
-    const int n = 2 * ncta;
+    const int q = k;
+    double al[MAXC], be[MAXC], ga[MAXC], de[MAXC];
+    double alp = 0.0, bep = 0.0;
     for (int c = 0; c < ncta; c++) {
-      const double2* rb2 = gath + 6 * c;
-      const double2 d0 = rb2[0], e0 = rb2[1], f0 = rb2[2], dl2 = rb2[3], el = rb2[4], fl = rb2[5];
-      const double d0q[2] = {d0.x, d0.y}, e0q[2] = {e0.x, e0.y}, f0q[2] = {f0.x, f0.y};
-      const double dlq[2] = {dl2.x, dl2.y}, elq[2] = {el.x, el.y}, flq[2] = {fl.x, fl.y};
-      for (int q = 0; q < 2; q++) {
-        for (int j = 0; j < n; j++) { A[q][2 * c][j] = 0.0; A[q][2 * c + 1][j] = 0.0; }
-        A[q][2 * c][2 * c] = 1.0;
-        A[q][2 * c + 1][2 * c + 1] = 1.0;
-        if (c > 0) { A[q][2 * c][2 * c - 1] = e0q[q]; A[q][2 * c + 1][2 * c - 1] = elq[q]; }
-        if (c + 1 < ncta) { A[q][2 * c][2 * c + 2] = f0q[q]; A[q][2 * c + 1][2 * c + 2] = flq[q]; }
-        z[q][2 * c] = d0q[q];
-        z[q][2 * c + 1] = dlq[q];
-      }
+      const double* g6 = (const double*)(gath + 6 * c);   // (d0, e0, f0, dl, el, fl), two biases each
+      const double d0 = g6[0 + q], e0 = g6[2 + q], f0 = g6[4 + q];
+      const double dl = g6[6 + q], el = g6[8 + q], fl = g6[10 + q];
+      const double den = 1.0 + e0 * bep;
+      bad |= (den == 0.0);
+      const double rd = rcp_nr(den);
+      ga[c] = (d0 - e0 * alp) * rd;
+      de[c] = -f0 * rd;
+      al[c] = dl - el * (alp + bep * ga[c]);
+      be[c] = -(el * bep * de[c] + fl);
+      alp = al[c];
+      bep = be[c];
     }
-    for (int q = 0; q < 2; q++) {
-      for (int i = 0; i < n; i++) {
-        const double piv = A[q][i][i];
-        bad |= (piv == 0.0);
-        const double ip = 1.0 / piv;
-        for (int r = i + 1; r < n && r <= i + 3; r++) {
-          const double m = A[q][r][i] * ip;
-          if (m == 0.0) continue;
-          for (int j = i; j < n && j <= i + 3; j++) A[q][r][j] -= m * A[q][i][j];
-          z[q][r] -= m * z[q][i];
-        }
-      }
-      for (int i = n - 1; i >= 0; i--) {
-        double t = z[q][i];
-        for (int j = i + 1; j < n && j <= i + 3; j++) t -= A[q][i][j] * z[q][j];
-        z[q][i] = t / A[q][i][i];
-      }
+    double Fn = 0.0, Lv = 0.0, Rv = 0.0;   // Fn: F_{c+1}
+    for (int c = ncta - 1; c >= 0; c--) {
+      if (c == rank + 1) Rv = ga[c] + de[c] * Fn;
+      if (c == rank - 1) Lv = al[c] + be[c] * Fn;
+      Fn = ga[c] + de[c] * Fn;
     }
-    const double L0 = rank > 0 ? z[0][2 * rank - 1] : 0.0, L1 = rank > 0 ? z[1][2 * rank - 1] : 0.0;
-    const double R0 = rank + 1 < ncta ? z[0][2 * rank + 2] : 0.0, R1 = rank + 1 < ncta ? z[1][2 * rank + 2] : 0.0;
-    bnd[6] = make_double2(L0, L1);
-    bnd[7] = make_double2(R0, R1);
+    ((double*)(bnd + 6))[q] = Lv;
+    ((double*)(bnd + 7))[q] = Rv;
   }
   cl.sync();   // every CTA's reads of the others' shared memory are done
   const double2 Lv = bnd[6], Rv = bnd[7];
